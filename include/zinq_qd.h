@@ -1,0 +1,265 @@
+/*
+ * zinq_qd.h -- C-ABI of the B200-native split-operator wavepacket propagator.
+ *
+ * Drop-in for Zinq's grid quantum-dynamics path (tjira/zinq).  Every entry
+ * point below names the reference interface it replaces.  Plain C99: no CUDA,
+ * torch or C++ types cross this boundary; device memory is owned by the
+ * library.  A Zig host imports it the way src/cimport.zig:3-8 imports FFTW
+ * and ExprTk: `@cImport(@cInclude("zinq_qd.h"))`.
+ *
+ * Status codes: 0 is success, negative values mirror the reference's Zig
+ * error set (error.InvalidInput, error.OutOfMemory, error.PlanCreationFailed,
+ * error.LapackError, ExprTk's null return) plus device-side conditions.
+ */
+#ifndef ZINQ_QD_H
+#define ZINQ_QD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZQD_ABI_VERSION 1
+#define ZQD_MAX_NDIM 3
+#define ZQD_MAX_NSTATE 4
+
+typedef enum {
+    ZQD_OK = 0,
+    ZQD_ERR_INVALID_INPUT = -1, /* error.InvalidInput, src/quantum_dynamics.zig:606-710 */
+    ZQD_ERR_OUT_OF_MEMORY = -2, /* error.OutOfMemory (host allocation) */
+    ZQD_ERR_DEVICE_OOM = -3,    /* device allocation refused / not enough free HBM */
+    ZQD_ERR_PLAN_FAILED = -4,   /* error.PlanCreationFailed, src/fourier_transform.zig:22 */
+    ZQD_ERR_EIGEN_FAILED = -5,  /* error.LapackError, src/linear_algebra.zig:69 */
+    ZQD_ERR_EXPRESSION = -6,    /* exprtk_init returned null, src/exprtk.cpp:21-23 */
+    ZQD_ERR_UNSUPPORTED = -7,   /* valid for the reference, outside this build's limits */
+    ZQD_ERR_DEVICE = -8,        /* CUDA runtime error */
+    ZQD_ERR_TIMEOUT = -9,       /* a bounded device or host wait ran out */
+    ZQD_ERR_CANCELLED = -10,    /* job cancelled through the server */
+    ZQD_ERR_NOT_FOUND = -11,    /* unknown job id or result index */
+    ZQD_ERR_NO_DEVICE = -12     /* no CUDA device with sm_100 */
+} zqd_status;
+
+/* Human-readable text of a status code; the last failing call's detail
+   (e.g. "MASS MUST BE GREATER THAN 0") is available from zqd_last_error(). */
+const char* zqd_status_string(int status);
+const char* zqd_last_error(void);
+
+/* ------------------------------------------------------------------ options
+ * zqd_options mirrors `Options` (src/quantum_dynamics.zig:25-67),
+ * `InitialConditions` (src/wavepacket.zig:16-23) and the potential `Options`
+ * union (src/potential.zig:19-60).  Arrays are pointer + implied length
+ * (ndim, nstate); the library deep-copies everything it keeps.
+ */
+typedef enum {
+    ZQD_POT_HARMONIC = 0,    /* src/potential.zig:143-175 */
+    ZQD_POT_TIME_LINEAR = 1, /* :178-215 */
+    ZQD_POT_TULLY_1 = 2,     /* :218-261 */
+    ZQD_POT_TULLY_2 = 3,     /* :264-314 */
+    ZQD_POT_TULLY_3 = 4,     /* :317-361 */
+    ZQD_POT_CUSTOM = 5,      /* :364-451, expressions as in src/exprtk.cpp:10-40 */
+    ZQD_POT_LVC = 6,         /* :493-575 */
+    ZQD_POT_FILE = 7         /* :454-490, table as read by src/read_write.zig:24-56 */
+} zqd_potential_kind;
+
+typedef struct {
+    zqd_potential_kind kind;
+    /* harmonic: k[ndim] (default {1}) */
+    const double* harmonic_k;
+    uint32_t harmonic_ndim;
+    /* time_linear: a (10), g (2); tully_1: A B C D; tully_2: A B C D E0; tully_3: A B C */
+    double p[5];
+    /* custom: nstate x nstate NUL-terminated expressions, row-major */
+    const char* const* custom_matrix;
+    uint32_t custom_nstate;
+    uint32_t custom_ndim;
+    int custom_time_dependent;
+    /* lvc: frequencies[nmode] cm^-1, excitation_energies[nstate] eV,
+       kappa[nstate][nmode], lambda[nstate][nstate][nmode] */
+    const double* lvc_frequencies;
+    uint32_t lvc_nmode;
+    const double* lvc_excitation_energies;
+    uint32_t lvc_nstate;
+    const double* lvc_kappa;
+    const double* lvc_lambda;
+    /* file: nrow x ncol row-major table; the first file_ndim columns are coordinates */
+    const double* file_table;
+    uint32_t file_nrow;
+    uint32_t file_ncol;
+    uint32_t file_ndim;
+} zqd_potential;
+
+/* bits of zqd_options.write_mask: which time series are recorded (Write, src/quantum_dynamics.zig:86-96) */
+enum {
+    ZQD_WRITE_ACF = 1u << 0,
+    ZQD_WRITE_KINETIC_ENERGY = 1u << 1,
+    ZQD_WRITE_MOMENTUM = 1u << 2,
+    ZQD_WRITE_NORM = 1u << 3,
+    ZQD_WRITE_POPULATION = 1u << 4,
+    ZQD_WRITE_POSITION = 1u << 5,
+    ZQD_WRITE_POTENTIAL_ENERGY = 1u << 6,
+    ZQD_WRITE_TOTAL_ENERGY = 1u << 7,
+    ZQD_WRITE_WAVEFUNCTION = 1u << 8
+};
+
+typedef enum {
+    ZQD_FP64 = 0,      /* plain form: complex FP64 throughout */
+    ZQD_FP32_MIXED = 1 /* FP32 state, butterflies and phases; FP64 tables, eigh and reductions */
+} zqd_precision;
+
+typedef struct {
+    uint32_t struct_size; /* sizeof(zqd_options); set by zqd_options_init */
+    /* grid */
+    uint32_t ndim;
+    uint32_t npoint;
+    const double* grid_bounds; /* [ndim][2] */
+    /* initial_conditions */
+    const double* ic_position; /* [ndim] */
+    const double* ic_momentum; /* [ndim] */
+    const double* ic_gamma;    /* [ndim] */
+    uint32_t ic_state;
+    int ic_adiabatic;
+    /* potential */
+    zqd_potential potential;
+    /* propagation */
+    double time_step;
+    uint32_t iterations;
+    const double* mass; /* [ndim] */
+    uint32_t write_mask;
+    int adiabatic;
+    uint32_t log_interval;
+    /* absorbing_potential (optional) */
+    int has_absorbing_potential;
+    int cap_track_population;
+    const double* cap_bounds; /* [ndim][2] */
+    double cap_exponent;      /* default 0.001 */
+    int cap_has_stop_norm;
+    double cap_stop_norm;
+    /* fft.plan: accepted for schema compatibility; planning effort has no effect here */
+    int fft_plan;
+    /* imaginary (optional): number of relaxed states, 0 for real-time propagation */
+    uint32_t imaginary_nstate;
+    /* spectrum (optional) */
+    int has_spectrum;
+    uint32_t spectrum_padding;
+    double spectrum_threshold; /* default 1e-6 */
+    /* this build */
+    zqd_precision precision;
+    int log; /* compute every observable on log steps, like run(..., log=true) */
+} zqd_options;
+
+/* Fills the reference's field defaults (log_interval 1, cap exponent 0.001,
+   spectrum threshold 1e-6, fft.plan measure, FP64, harmonic potential). */
+void zqd_options_init(zqd_options* opt);
+/* Sets a potential's kind and the reference's default constants for it
+   (src/potential.zig:24-48: harmonic k {1}; time_linear a 10 g 2; Tully 1/2/3). */
+void zqd_potential_init(zqd_potential* pot, zqd_potential_kind kind);
+
+/* ------------------------------------------------------------------ results
+ * zqd_result mirrors Result(T) (src/quantum_dynamics.zig:70-83): one
+ * Observables entry per imaginary-time state (or one for real time), plus the
+ * recorded time series (History, :99-279).  Owned by the library until
+ * zqd_result_destroy (the reference's Result.deinit).
+ */
+typedef struct zqd_result zqd_result;
+
+typedef enum {
+    ZQD_SERIES_POSITION = 0, /* rows x ndim */
+    ZQD_SERIES_MOMENTUM = 1, /* rows x ndim */
+    ZQD_SERIES_POPULATION = 2,
+    ZQD_SERIES_POTENTIAL_ENERGY = 3,
+    ZQD_SERIES_KINETIC_ENERGY = 4,
+    ZQD_SERIES_TOTAL_ENERGY = 5,
+    ZQD_SERIES_NORM = 6,
+    ZQD_SERIES_ACF = 7 /* rows x 2 (re, im) */
+} zqd_series;
+
+typedef struct {
+    uint32_t ndim, nstate;
+    double pos[ZQD_MAX_NDIM];
+    double mom[ZQD_MAX_NDIM];
+    double pop[ZQD_MAX_NSTATE];
+    double epot, ekin, norm;
+    double acf_re, acf_im; /* NaN unless the autocorrelation is recorded */
+} zqd_observables;
+
+uint32_t zqd_result_nsolve(const zqd_result* res);
+/* final Observables of solve s (Observables.init with log=true, src/quantum_dynamics.zig:949) */
+int zqd_result_final(const zqd_result* res, uint32_t solve, zqd_observables* out);
+/* one recorded time series; *rows = iterations+1 unless stop_norm ended the solve early */
+int zqd_result_series(const zqd_result* res, uint32_t solve, zqd_series which, const double** data, size_t* rows,
+                      size_t* cols);
+/* final wavefunction of solve s, nstate x npoint^ndim complex (re, im interleaved), state-major */
+int zqd_result_wavefunction(const zqd_result* res, uint32_t solve, double* host_out, size_t capacity_doubles);
+/* spectrum of solve s (calcSpectrum, src/spectral_analysis.zig:13-44) */
+int zqd_result_spectrum(const zqd_result* res, uint32_t solve, const double** acf_padded, size_t* nacf,
+                        const double** sigma, size_t* nsigma);
+/* GPU time of the propagation kernels of the whole run, milliseconds (CUDA events) */
+double zqd_result_device_ms(const zqd_result* res);
+void zqd_result_destroy(zqd_result* res);
+
+/* --------------------------------------------------------------- method API
+ * zqd_run replaces `quantum_dynamics.run(comptime T, io, opt, log, gpa)`
+ * (src/quantum_dynamics.zig:567-603): validation identical to
+ * checkInvalidInput (:606-710), setup (:713-749), one solve per
+ * imaginary-time state (:582-598) on the GPU.
+ */
+int zqd_run(const zqd_options* opt, zqd_result** out);
+
+/* Staged form of zqd_run: create (validate, upload, build the potential and
+   phase tables on the device), solve, fetch.  A job handle is used by one
+   host thread at a time. */
+typedef struct zqd_job zqd_job;
+int zqd_job_create(const zqd_options* opt, zqd_job** out);
+int zqd_job_run(zqd_job* job);                           /* every solve, device-resident, no host copies */
+int zqd_job_result(zqd_job* job, zqd_result** out);      /* device -> host copy of observables */
+int zqd_job_info(const zqd_job* job, uint32_t* ndim, uint32_t* nstate, uint64_t* npoint_total,
+                 uint32_t* cluster_ctas, size_t* device_bytes);
+/* device time (ms, CUDA events on the job's stream) of the last zqd_job_run */
+double zqd_job_device_ms(const zqd_job* job);
+void zqd_job_destroy(zqd_job* job);
+
+/* Several independent jobs advanced together on the device (the batched
+   form): one launch per group of jobs with equal shape and precision.
+   results[i] receives the result of opts[i]. */
+int zqd_run_batch(const zqd_options* const* opts, uint32_t njobs, zqd_result** results);
+
+/* ------------------------------------------------------------ FFT seam
+ * Replaces FftPlan(T) (src/fourier_transform.zig:8-49: fftw_plan_dft,
+ * fftw_execute_dft, fftw_destroy_plan): in-place N-D complex transform of a
+ * device buffer, sign -1 unnormalised forward, +1 inverse followed by 1/N.
+ * Square grids n^ndim with n a power of two from 2 to 8192.
+ */
+typedef struct zqd_fft zqd_fft;
+int zqd_fft_plan_create(uint32_t ndim, const int* shape, int sign, zqd_precision precision, zqd_fft** out);
+int zqd_fft_execute(zqd_fft* plan, void* device_inout, void* cuda_stream);
+void zqd_fft_destroy(zqd_fft* plan);
+
+/* --------------------------------------------------------- expression seam
+ * Replaces exprtk_init / exprtk_evaluate_d0 / exprtk_deinit
+ * (src/exprtk.h:1-10, src/exprtk.cpp:10-40): compiles an expression over
+ * r1..r<nvar> and t into device bytecode.  A parse error returns
+ * ZQD_ERR_EXPRESSION where ExprTk returned null.
+ */
+typedef struct zqd_expr zqd_expr;
+int zqd_expr_compile(const char* text, size_t len, size_t nvar, zqd_expr** out);
+/* evaluates on the device for npts coordinate rows (host arrays r[npts][nvar]) */
+int zqd_expr_eval_points(const zqd_expr* e, const double* host_r, size_t npts, double t, double* host_out);
+void zqd_expr_destroy(zqd_expr* e);
+
+/* ------------------------------------------------------------ eigen seam
+ * Replaces eighBatch (src/linear_algebra.zig:28-42, LAPACKE_dsyevd row-major
+ * 'V','U' at :67) with the device FP64 solver; exposed for parity tests.
+ * W ascending, U[k*n+m] = component k of eigenvector m.
+ */
+int zqd_eigh_batch(uint32_t n, size_t count, const double* host_V, double* host_W, double* host_U);
+
+/* ------------------------------------------------------------------ device */
+int zqd_device_count(void);
+int zqd_set_device(int device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZINQ_QD_H */

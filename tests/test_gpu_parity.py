@@ -1,0 +1,196 @@
+"""GPU parity of the propagator against the oracle and the reference's goldens.
+
+Bars (FP64 plain form): relative L2 of the final wavefunction <= 1e-10 and
+every population sample within 1e-12 absolute of the oracle; the reference's
+own known answers (test/quantum_dynamics.zig:8-282) within their 1e-8.
+FP32 form: every population sample within 1e-5 of the FP64 oracle.
+All calls go through the C-ABI (libzinq_qd.so).
+"""
+import copy
+import os
+
+import numpy as np
+import pytest
+
+from oracle import qd_ref
+from zinq_b200 import quantum_dynamics as qd
+
+pytestmark = pytest.mark.gpu
+
+PSI_TOL = 1e-10
+POP_TOL = 1e-12
+FP32_POP_TOL = 1e-5
+
+ORACLE_NAMES = {"position": "pos", "momentum": "mom", "population": "pop", "potential_energy": "epot",
+                "kinetic_energy": "ekin", "total_energy": "etot", "norm": "norm", "acf": "acf"}
+
+
+def psi_rel(g, r):
+    return float(np.linalg.norm(g - r) / np.linalg.norm(r))
+
+
+def compare(opt, precision="fp64", pop_tol=POP_TOL, psi_tol=PSI_TOL, obs_tol=1e-10, sign_free=False):
+    gpu = qd.run(opt, precision=precision)
+    ref = qd_ref.run(opt)
+    assert len(gpu.observables) == len(ref)
+    worst = {}
+    for g, r in zip(gpu.observables, ref):
+        for name, series in g.history.items():
+            rs = r.history[ORACLE_NAMES[name]]
+            assert series.shape[0] == rs.shape[0], name
+            tol = pop_tol if name == "population" else obs_tol
+            err = float(np.max(np.abs(series - rs)))
+            worst[name] = max(worst.get(name, 0.0), err)
+            assert err <= tol, (name, err)
+        for name in ("pos", "mom", "pop"):
+            err = float(np.max(np.abs(getattr(g, name) - getattr(r, name))))
+            assert err <= (pop_tol if name == "pop" else obs_tol), (name, err)
+        for name in ("epot", "ekin", "norm"):
+            assert abs(getattr(g, name) - getattr(r, name)) <= obs_tol, name
+        if precision == "fp64":
+            gw, rw = g.wavefunction, r.wavefunction
+            if sign_free:  # eigenvector sign conventions may differ by a global per-state sign
+                for s in range(gw.shape[0]):
+                    if np.vdot(gw[s], rw[s]).real < 0:
+                        gw[s] = -gw[s]
+            rel = psi_rel(gw, rw)
+            assert rel <= psi_tol, rel
+            worst["psi_rel_l2"] = max(worst.get("psi_rel_l2", 0.0), rel)
+    return gpu, ref, worst
+
+
+def tully(pot, adia, npoint=512, iters=3000):
+    return {"grid": {"bounds": [[-24, 32]], "npoint": npoint},
+            "initial_conditions": {"momentum": [15], "position": [-10], "state": 0, "gamma": [2], "adiabatic": adia},
+            "potential": {pot: {}}, "mass": [2000], "iterations": iters, "time_step": 1, "adiabatic": adia,
+            "write": {"population": "P", "position": "X", "momentum": "K", "total_energy": "E", "norm": "N"}}
+
+
+# ---------------------------------------------------------------- goldens
+@pytest.mark.parametrize("case", range(10))
+def test_gpu_reproduces_reference_known_answers(known_answers, case):
+    t = known_answers["tests"][case]
+    res = qd.run(t["options"], want_wavefunction=False)
+    for e in t["expect"]:
+        v = getattr(res.observables[e["solve"]], e["field"])
+        got = float(v[e["index"]]) if e["index"] is not None else float(v)
+        assert abs(got - e["value"]) <= known_answers["tolerance"], (t["name"], e, got)
+
+
+@pytest.mark.parametrize("case", range(10))
+def test_gpu_matches_oracle_on_golden_inputs(known_answers, case):
+    opt = copy.deepcopy(known_answers["tests"][case]["options"])
+    opt["write"] = {"population": "P", "position": "X", "total_energy": "E", "norm": "N"}
+    compare(opt)
+
+
+# ---------------------------------------------------------------- 1-D paths
+@pytest.mark.parametrize("pot", ["tully_1", "tully_2", "tully_3"])
+def test_adiabatic_initial_state_signs_match_lapack(pot):
+    # wavefunction compared without any sign freedom: eigenvector signs follow dsyevd
+    compare(tully(pot, True, iters=300))
+
+
+@pytest.mark.parametrize("cluster", ["1", "2", "4", "8", "16"])
+def test_cluster_sizes_agree_with_oracle(cluster, monkeypatch):
+    monkeypatch.setenv("ZQD_LINE_CLUSTER", cluster)
+    opt = tully("tully_1", True, npoint=1024, iters=400)
+    compare(opt)
+
+
+def test_custom_expression_potential_matches_builtin():
+    # example/input/quantum_dynamics_custom_real.json writes Tully 1 as expressions
+    expr = {"custom": {"ndim": 1, "matrix": [
+        ["+sgn(r1) * 0.01 * (1.0 - exp(-1.6 * abs(r1)))", "0.005 * exp(-r1^2)"],
+        ["0.005 * exp(-r1^2)", "-sgn(r1) * 0.01 * (1.0 - exp(-1.6 * abs(r1)))"]]}}
+    opt = tully("tully_1", True, npoint=1024, iters=500)
+    opt["potential"] = expr
+    g, _, _ = compare(opt)
+    b = qd.run(tully("tully_1", True, npoint=1024, iters=500))
+    assert np.max(np.abs(g.observables[0].history["population"] - b.observables[0].history["population"])) < 1e-12
+
+
+def test_time_dependent_custom_potential():
+    opt = {"grid": {"bounds": [[-16, 16]], "npoint": 256},
+           "initial_conditions": {"momentum": [0], "position": [0], "state": 1, "gamma": [2], "adiabatic": True},
+           "potential": {"custom": {"ndim": 1, "time_dependent": True,
+                                    "matrix": [["(t - 10) * 10", "2"], ["2", "-(t - 10) * 10"]]}},
+           "mass": [1], "iterations": 500, "time_step": 0.01, "adiabatic": True,
+           "write": {"population": "P", "potential_energy": "V"}}
+    compare(opt)
+
+
+def test_absorbing_potential_tracking_and_stop_norm():
+    opt = tully("tully_1", False, npoint=512, iters=3000)
+    # the packet (x0 = -10, v = 15/2000) crosses x = 5 near step 2000 and is absorbed beyond it
+    opt["absorbing_potential"] = {"bounds": [[-20, 5]], "exponent": 0.05, "track_population": True,
+                                  "stop_norm": 0.5}
+    g, r, _ = compare(opt)
+    rows = g.observables[0].history["population"].shape[0]
+    assert rows < 3001  # stopped early, like the oracle
+
+
+def test_autocorrelation_and_three_states():
+    opt = {"grid": {"bounds": [[-12, 12]], "npoint": 2048},
+           "initial_conditions": {"momentum": [1], "position": [-2], "state": 0, "gamma": [1]},
+           "potential": {"custom": {"ndim": 1, "matrix": [
+               ["0.5*r1^2 + 0.3*r1", "0.05*exp(-r1^2/2)", "0.02"],
+               ["0.05*exp(-r1^2/2)", "0.5*r1^2 - 0.2*r1 + 0.1", "0.05*exp(-r1^2/2)"],
+               ["0.02", "0.05*exp(-r1^2/2)", "0.5*r1^2 + 0.15"]]}},
+           "mass": [1], "iterations": 400, "time_step": 0.05,
+           "write": {"population": "P", "acf": "A", "total_energy": "E"}}
+    compare(opt)
+
+
+def test_imaginary_time_three_states_orthogonalised():
+    opt = {"grid": {"bounds": [[-8, 8]], "npoint": 256},
+           "initial_conditions": {"momentum": [0.3], "position": [1], "gamma": [2]},
+           "potential": {"harmonic": {}}, "imaginary": {"nstate": 3}, "mass": [1], "iterations": 600,
+           "time_step": 0.01, "write": {"total_energy": "E", "norm": "N"}}
+    compare(opt)
+
+
+# ---------------------------------------------------------------- workloads
+def config1():
+    return {"grid": {"bounds": [[-16, 16]], "npoint": 1024},
+            "initial_conditions": {"position": [1], "momentum": [0], "gamma": [1], "state": 0},
+            "potential": {"harmonic": {"k": [1]}}, "mass": [1], "iterations": 1000, "time_step": 0.1,
+            "write": {"norm": "N", "total_energy": "E", "position": "X"}}
+
+
+def config2(p0, iters=4000):
+    return {"grid": {"bounds": [[-24, 24]], "npoint": 8192},
+            "initial_conditions": {"position": [-10], "momentum": [p0], "gamma": [p0 * p0 / 400.0], "state": 0,
+                                   "adiabatic": True},
+            "potential": {"custom": {"ndim": 1, "matrix": [["0.01*tanh(1.6*r1)", "0.005*exp(-r1^2)"],
+                                                           ["0.005*exp(-r1^2)", "-0.01*tanh(1.6*r1)"]]}},
+            "mass": [2000], "iterations": iters, "time_step": 1, "adiabatic": True,
+            "write": {"population": "P"}}
+
+
+def test_config1_harmonic_1024():
+    compare(config1())
+
+
+def test_config2_tanh_crossing_fp64():
+    compare(config2(20.0, iters=1500))
+
+
+@pytest.mark.parametrize("p0", [10.0, 30.0])
+def test_config2_fp32_populations_within_1e5(p0):
+    compare(config2(p0, iters=1500), precision="fp32", pop_tol=FP32_POP_TOL, obs_tol=1e-4)
+
+
+def test_batched_jobs_equal_single_jobs():
+    opts = [config2(p, iters=300) for p in (10.0, 15.0, 20.0, 25.0, 30.0)]
+    batch = qd.run_batch(opts)
+    for o, b in zip(opts, batch):
+        s = qd.run(o, want_wavefunction=False)
+        np.testing.assert_array_equal(b.observables[0].history["population"], s.observables[0].history["population"])
+
+
+def test_runs_are_bitwise_deterministic():
+    a = qd.run(config1())
+    b = qd.run(config1())
+    np.testing.assert_array_equal(a.observables[0].wavefunction, b.observables[0].wavefunction)
+    np.testing.assert_array_equal(a.observables[0].history["total_energy"], b.observables[0].history["total_energy"])

@@ -1,0 +1,89 @@
+// internal.h -- host-side state shared by the C-ABI implementation files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/zinq_qd.h"
+#include "expr.h"
+#include "physics.cuh"
+
+namespace zqd {
+
+void set_error(const std::string& msg);
+int fail(int status, const std::string& msg);
+
+#define ZQD_CUDA(call)                                                                                             \
+    do {                                                                                                           \
+        cudaError_t e__ = (call);                                                                                  \
+        if (e__ != cudaSuccess)                                                                                    \
+            return ::zqd::fail(e__ == cudaErrorMemoryAllocation ? ZQD_ERR_DEVICE_OOM : ZQD_ERR_DEVICE,             \
+                               std::string(#call) + ": " + cudaGetErrorString(e__));                               \
+    } while (0)
+
+// Deep copy of zqd_options (the caller's memory is only borrowed during a call).
+struct Opts {
+    uint32_t ndim = 0, npoint = 0;
+    std::vector<double> bounds, pos, mom, gamma, mass, cap_bounds;
+    uint32_t ic_state = 0;
+    bool ic_adiabatic = false;
+    double time_step = 0;
+    uint32_t iterations = 0, write_mask = 0, log_interval = 1, imag_nstate = 0, spectrum_padding = 0;
+    bool adiabatic = false, has_cap = false, cap_track = false, cap_has_stop = false, has_spectrum = false, log = false;
+    double cap_exponent = 0.001, cap_stop_norm = 0, spectrum_threshold = 1e-6;
+    zqd_precision precision = ZQD_FP64;
+    // potential
+    int pkind = 0;
+    std::vector<double> harmonic_k;
+    double p[5] = {0, 0, 0, 0, 0};
+    std::vector<std::string> custom;
+    uint32_t custom_ns = 0, custom_nd = 0;
+    bool custom_td = false;
+    std::vector<double> lvc_freq, lvc_exc, lvc_kappa, lvc_lambda;
+    std::vector<double> file_table;
+    uint32_t file_nrow = 0, file_ncol = 0, file_nd = 0;
+    // derived
+    int pot_nd = 0, pot_ns = 0;
+    bool pot_td = false;
+};
+
+int copy_options(const zqd_options* in, Opts& o);
+int validate(const Opts& o);
+
+// Device resident potential description + its storage.
+struct PotStore {
+    PotDev dev{};
+    uint32_t* d_code = nullptr;
+    double* d_consts = nullptr;
+    double* d_lvc = nullptr;
+    double* d_file = nullptr;
+    ~PotStore();
+};
+int build_potential(const Opts& o, PotStore& ps);
+
+// Twiddle tables exp(-2 pi i t / n), t < n, generated in long double and rounded.
+std::vector<double> twiddles_f64(int n);
+
+struct SolveOut {
+    size_t rows = 0;
+    std::vector<double> hist; // rows x HC
+    std::vector<double> fin;  // HC
+    std::vector<double> psi;  // S x N complex, natural order
+    std::vector<double> acfpad, sigma;
+};
+
+} // namespace zqd
+
+struct zqd_result {
+    uint32_t ndim = 0, nstate = 0;
+    uint64_t npoint_total = 0;
+    std::vector<zqd::SolveOut> solves;
+    std::vector<std::vector<double>> series_cache; // per (solve, series)
+    double device_ms = 0;
+    uint32_t write_mask = 0;
+    int hc = 0;
+};

@@ -1,0 +1,580 @@
+// job.cu -- job lifecycle behind the C-ABI: create (init, src/quantum_dynamics.zig:713-749),
+// run (run/solve, :567-603 and :860-950) and result download.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "internal.h"
+#include "line_kernel.cuh"
+
+namespace zqd {
+
+// ------------------------------------------------------------------ setup
+template <typename T> struct LineTablesArgs {
+    int n, m, C, q;
+    double lo, hi, mass, dt_re, dt_im;
+    int has_cap;
+    double cap_lo, cap_hi, cap_exp;
+    PotDev pot;
+    cx<T>* R;
+    double* V;
+    double* U;
+    double* capw;
+    cx<T>* expk;
+};
+
+// Hamiltonian.init/update at t = 0 (wavepacket.zig:96-143) and Propagator.init/update
+// (quantum_dynamics.zig:387-468) for every grid point, written in the cluster-permuted layout.
+template <typename T, int S> __global__ void line_tables_kernel(LineTablesArgs<T> a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const int c = p / a.m, j = p - c * a.m;
+    const int x = c + a.C * j;
+    double r = __dadd_rn(a.lo, __dmul_rn((double)x, a.hi - a.lo) / (double)a.n);
+    double V[S * S], Vu[S * S], W[S], U[S * S];
+    pot_eval(a.pot, &r, 0.0, V);
+    for (int i = 0; i < S; ++i)
+        for (int k = 0; k < S; ++k) Vu[i * S + k] = V[(i < k ? i : k) * S + (i < k ? k : i)];
+    eigh_dev<S>(Vu, W, U);
+    for (int e = 0; e < S * S; ++e) a.V[(size_t)e * a.n + p] = V[e];
+    if (S > 1)
+        for (int e = 0; e < S * S; ++e) a.U[(size_t)e * a.n + p] = U[e];
+    double cap_sum = 0;
+    if (a.has_cap) {
+        double dist = fmax(0.0, fmax(a.cap_lo - r, r - a.cap_hi));
+        if (dist > 0) cap_sum = __dadd_rn(cap_sum, exp(__dmul_rn(a.cap_exp, dist)) - 1);
+    }
+    double decay = exp(__dmul_rn(__dmul_rn(-0.5, cap_sum), hypot(a.dt_re, a.dt_im)));
+    if (a.capw) a.capw[p] = 1 - decay * decay;
+    int idx = 0;
+    for (int k = 0; k < S; ++k)
+        for (int jj = k; jj < S; ++jj) {
+            double re, im;
+            propagator_entry<S>(W, U, a.dt_re, a.dt_im, decay, k, jj, re, im);
+            a.R[(size_t)idx * a.n + p] = mk<T>((T)re, (T)im);
+            ++idx;
+        }
+    // kinetic phase exp(-i K dt) at the wavenumber this slot holds after the forward transform
+    {
+        const int e = j, k2 = e / a.q, u = e - k2 * a.q;
+        const int kidx = c * a.q + u + a.m * k2;
+        double nn = (double)kidx;
+        double kv = __dmul_rn(kidx < a.n / 2 ? nn : __dsub_rn(nn, (double)a.n), 6.283185307179586476925286766559 / (a.hi - a.lo));
+        double K = __dmul_rn(__dmul_rn(0.5, kv), kv) / a.mass;
+        // Complex(0, -K) * dt
+        double zre = __dsub_rn(__dmul_rn(0.0, a.dt_re), __dmul_rn(-K, a.dt_im));
+        double zim = __dadd_rn(__dmul_rn(0.0, a.dt_im), __dmul_rn(-K, a.dt_re));
+        double ore, oim;
+        cexp_dev(zre, zim, ore, oim);
+        a.expk[p] = mk<T>((T)ore, (T)oim);
+    }
+}
+
+// 1-D eigenvector sign continuity (wavepacket.zig:145-155): eigenvector j at
+// point x is flipped when its overlap with the (already fixed) vector at x-1
+// is negative.  s_x = s_{x-1} for a positive raw overlap, -s_{x-1} for a
+// negative one, +1 for zero; a single CTA scans these maps in grid order.
+template <int S> __global__ void sign_scan_kernel(double* U, int n, int m, int C, signed char* code) {
+    __shared__ int sm_m[1024], sm_c[1024];
+    const int nt = blockDim.x, t = threadIdx.x;
+    const int chunk = (n + nt - 1) / nt;
+    auto pos = [&](int x) { return (x % C) * m + x / C; };
+    for (int jcol = 0; jcol < S; ++jcol) {
+        // phase 1: per-point maps from raw overlaps, and this thread's composed map
+        int M = 1, Cc = 0; // s -> M*s + Cc
+        int x0 = t * chunk, x1 = min(n, x0 + chunk);
+        for (int x = max(x0, 1); x < x1; ++x) {
+            double ov = 0;
+            for (int k = 0; k < S; ++k)
+                ov += U[(size_t)(k * S + jcol) * n + pos(x)] * U[(size_t)(k * S + jcol) * n + pos(x - 1)];
+            int cd = ov > 0 ? 0 : (ov < 0 ? 1 : 2);
+            code[x] = (signed char)cd;
+            if (cd == 1) {
+                M = -M;
+                Cc = -Cc;
+            } else if (cd == 2) {
+                M = 0;
+                Cc = 1;
+            }
+        }
+        sm_m[t] = M;
+        sm_c[t] = Cc;
+        __syncthreads();
+        if (t == 0) { // sequential exclusive scan of the per-thread maps applied to s_0 = +1
+            int s = 1;
+            for (int i = 0; i < nt; ++i) {
+                int mi = sm_m[i], ci = sm_c[i];
+                sm_m[i] = s; // sign entering chunk i
+                s = mi * s + ci;
+            }
+        }
+        __syncthreads();
+        int s = sm_m[t];
+        // phase 2: walk the chunk and flip
+        for (int x = x0; x < x1; ++x) {
+            if (x > 0) {
+                int cd = code[x];
+                s = cd == 0 ? s : (cd == 1 ? -s : 1);
+            }
+            if (s < 0)
+                for (int k = 0; k < S; ++k) {
+                    double* u = &U[(size_t)(k * S + jcol) * n + pos(x)];
+                    *u = -*u;
+                }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ job state
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(size_t b) {
+        bytes = b;
+        if (b == 0) return ZQD_OK;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(ZQD_ERR_DEVICE_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
+        }
+        return ZQD_OK;
+    }
+    template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
+};
+
+} // namespace zqd
+
+using namespace zqd;
+
+struct zqd_job {
+    Opts o;
+    int S = 1, d = 1, n = 0;
+    size_t N = 0;
+    int C = 1, m = 0, q = 0, E = 8, threads = 32;
+    size_t smem = 0;
+    bool fp32 = false;
+    int nsolve = 1, hc = 0;
+    PotStore pot;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
+    float last_ms = 0;
+    size_t device_bytes = 0;
+    ~zqd_job() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace zqd {
+
+template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
+
+static int choose_line_shape(zqd_job* J) {
+    const size_t csz = J->fp32 ? sizeof(float2) : sizeof(double2);
+    const size_t budget = 200 * 1024; // dynamic shared memory per CTA
+    int forced = 0;
+    if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
+    for (int C = 1; C <= 16; C <<= 1) {
+        if (forced && C != forced) continue;
+        if (J->n % C) continue;
+        int m = J->n / C;
+        if (m < 4 || m / C < 1 || (C > 1 && m < C)) continue;
+        size_t ld = J->fp32 ? (size_t)padded_len<float>(m) : (size_t)padded_len<double>(m);
+        size_t smem = (C > 1 ? 2 : 1) * (size_t)J->S * ld * csz;
+        if (smem > budget) continue;
+        int elems = J->S * m;
+        int E = J->fp32 ? ElemsOf<float>::E : ElemsOf<double>::E;
+        int threads = (elems + E - 1) / E;
+        if (threads > 512) continue;
+        threads = std::max(32, (threads + 31) / 32 * 32);
+        J->C = C;
+        J->m = m;
+        J->q = m / C;
+        J->E = E;
+        J->threads = threads;
+        J->smem = smem;
+        return ZQD_OK;
+    }
+    return fail(ZQD_ERR_UNSUPPORTED, "1-D GRID TOO LARGE FOR THE RESIDENT CLUSTER KERNEL");
+}
+
+using LineKernelFn = void (*)(const void*);
+
+// launchers compiled in line_inst.cu, one translation unit per (precision, states)
+int launch_line_d1(const LaunchShape*, const void*, int);
+int launch_line_d2(const LaunchShape*, const void*, int);
+int launch_line_d3(const LaunchShape*, const void*, int);
+int launch_line_d4(const LaunchShape*, const void*, int);
+int launch_line_f1(const LaunchShape*, const void*, int);
+int launch_line_f2(const LaunchShape*, const void*, int);
+int launch_line_f3(const LaunchShape*, const void*, int);
+int launch_line_f4(const LaunchShape*, const void*, int);
+
+template <typename T> static int launch_line_s(const LaunchShape* J, const void* dj, int nj) {
+    static int (*const dtab[4])(const LaunchShape*, const void*, int) = {launch_line_d1, launch_line_d2, launch_line_d3,
+                                                                          launch_line_d4};
+    static int (*const ftab[4])(const LaunchShape*, const void*, int) = {launch_line_f1, launch_line_f2, launch_line_f3,
+                                                                          launch_line_f4};
+    if (J->S < 1 || J->S > 4) return fail(ZQD_ERR_UNSUPPORTED, "STATE COUNT MUST BE 1..4");
+    return std::is_same<T, double>::value ? dtab[J->S - 1](J, dj, nj) : ftab[J->S - 1](J, dj, nj);
+}
+
+template <typename T, int S> static int run_tables(zqd_job* J) {
+    LineTablesArgs<T> a{};
+    a.n = J->n;
+    a.m = J->m;
+    a.C = J->C;
+    a.q = J->q;
+    a.lo = J->o.bounds[0];
+    a.hi = J->o.bounds[1];
+    a.mass = J->o.mass[0];
+    a.dt_re = J->o.imag_nstate ? 0.0 : J->o.time_step;
+    a.dt_im = J->o.imag_nstate ? -J->o.time_step : 0.0;
+    a.has_cap = J->o.has_cap;
+    if (J->o.has_cap) {
+        a.cap_lo = J->o.cap_bounds[0];
+        a.cap_hi = J->o.cap_bounds[1];
+        a.cap_exp = J->o.cap_exponent;
+    }
+    a.pot = J->pot.dev;
+    a.R = J->R.as<cx<T>>();
+    a.V = J->V.as<double>();
+    a.U = J->U.as<double>();
+    a.capw = J->capw.as<double>();
+    a.expk = J->expk.as<cx<T>>();
+    int threads = 128, blocks = (J->n + threads - 1) / threads;
+    line_tables_kernel<T, S><<<blocks, threads, 0, J->stream>>>(a);
+    ZQD_CUDA(cudaGetLastError());
+    if (S > 1) {
+        sign_scan_kernel<S><<<1, 1024, 0, J->stream>>>(J->U.as<double>(), J->n, J->m, J->C, J->scratch.as<signed char>());
+        ZQD_CUDA(cudaGetLastError());
+    }
+    return ZQD_OK;
+}
+
+template <typename T> static int run_tables_s(zqd_job* J) {
+    switch (J->S) {
+    case 1: return run_tables<T, 1>(J);
+    case 2: return run_tables<T, 2>(J);
+    case 3: return run_tables<T, 3>(J);
+    default: return run_tables<T, 4>(J);
+    }
+}
+
+template <typename T> static int create_line(zqd_job* J) {
+    const size_t n = J->n, S = J->S, nsym = S * (S + 1) / 2;
+    const size_t c = sizeof(cx<T>);
+    int rc;
+    if ((rc = J->R.alloc(nsym * n * c))) return rc;
+    if ((rc = J->expk.alloc(n * c))) return rc;
+    if ((rc = J->V.alloc(S * S * n * sizeof(double)))) return rc;
+    if (S > 1 && (rc = J->U.alloc(S * S * n * sizeof(double)))) return rc;
+    if (J->o.has_cap && (rc = J->capw.alloc(n * sizeof(double)))) return rc;
+    if ((rc = J->tw.alloc(n * c))) return rc;
+    if ((rc = J->psi_save.alloc(S * n * c))) return rc;
+    bool acf = J->o.has_spectrum || (J->o.write_mask & ZQD_WRITE_ACF);
+    if (acf && (rc = J->psi0.alloc(S * n * c))) return rc;
+    if (J->o.imag_nstate > 1 && (rc = J->orth.alloc((size_t)(J->o.imag_nstate - 1) * S * n * c))) return rc;
+    size_t rows = (size_t)J->o.iterations + 1;
+    if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double)))) return rc;
+    if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double)))) return rc;
+    if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
+    if ((rc = J->jobs.alloc((size_t)J->nsolve * sizeof(LineJob<T>)))) return rc;
+    if ((rc = J->scratch.alloc(n + 16))) return rc;
+    J->device_bytes = J->R.bytes + J->expk.bytes + J->V.bytes + J->U.bytes + J->capw.bytes + J->tw.bytes +
+                      J->psi_save.bytes + J->psi0.bytes + J->orth.bytes + J->hist.bytes;
+    // twiddles
+    std::vector<double> tw = twiddles_f64(J->n);
+    if (std::is_same<T, double>::value) {
+        ZQD_CUDA(cudaMemcpyAsync(J->tw.p, tw.data(), n * c, cudaMemcpyHostToDevice, J->stream));
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    } else {
+        std::vector<float> twf(tw.begin(), tw.end());
+        ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twf.data(), n * c, cudaMemcpyHostToDevice, J->stream));
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    }
+    if ((rc = run_tables_s<T>(J))) return rc;
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    return ZQD_OK;
+}
+
+template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
+    LineJob<T> L{};
+    const Opts& o = J->o;
+    L.n = J->n;
+    L.m = J->m;
+    L.logm = 0;
+    while ((1 << L.logm) < J->m) ++L.logm;
+    L.q = J->q;
+    L.lo = o.bounds[0];
+    L.hi = o.bounds[1];
+    L.dr = (o.bounds[1] - o.bounds[0]) / (double)o.npoint;
+    L.dk = L.dr / (double)J->N;
+    L.mass = o.mass[0];
+    L.iters = (int)o.iterations;
+    L.dt_re = o.imag_nstate ? 0.0 : o.time_step;
+    L.dt_im = o.imag_nstate ? -o.time_step : 0.0;
+    L.tstep = o.time_step;
+    L.itp = o.imag_nstate > 0;
+    L.ic_state = (int)o.ic_state;
+    L.ic_adia = o.ic_adiabatic;
+    L.x0 = o.pos[0];
+    L.p0 = o.mom[0];
+    L.gamma = o.gamma[0];
+    L.wmask = o.write_mask;
+    L.log = o.log;
+    L.log_interval = (int)o.log_interval;
+    L.adiabatic = o.adiabatic;
+    L.calc_acf = o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF);
+    L.track = o.has_cap && o.cap_track;
+    L.has_stop = o.has_cap && o.cap_has_stop;
+    L.stop_norm = o.cap_stop_norm;
+    L.td = o.pot_td;
+    L.has_cap = o.has_cap;
+    if (o.has_cap) {
+        L.cap_lo = o.cap_bounds[0];
+        L.cap_hi = o.cap_bounds[1];
+        L.cap_exp = o.cap_exponent;
+    }
+    L.R = J->R.as<cx<T>>();
+    L.expk = J->expk.as<cx<T>>();
+    L.V = J->V.as<double>();
+    L.U = J->U.as<double>();
+    L.capw = J->capw.as<double>();
+    L.tw = J->tw.as<cx<T>>();
+    L.psi_save = J->psi_save.as<cx<T>>();
+    L.psi0 = J->psi0.as<cx<T>>();
+    L.orth = J->orth.as<cx<T>>();
+    L.northo = s;
+    size_t rows = (size_t)o.iterations + 1;
+    L.hist = J->hist.as<double>() + (size_t)s * rows * J->hc;
+    L.fin = J->fin.as<double>() + (size_t)s * J->hc;
+    L.rows = J->rows.as<int>() + s;
+    L.pot = J->pot.dev;
+    return L;
+}
+
+template <typename T> static int run_line(zqd_job* J) {
+    const size_t SN = (size_t)J->S * J->n * sizeof(cx<T>);
+    std::vector<LineJob<T>> descs;
+    for (int s = 0; s < J->nsolve; ++s) descs.push_back(line_job_desc<T>(J, s));
+    ZQD_CUDA(cudaMemcpyAsync(J->jobs.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, J->stream));
+    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+    LaunchShape sh{J->S, J->C, J->E, J->threads, J->smem, J->stream};
+    for (int s = 0; s < J->nsolve; ++s) {
+        int rc = launch_line_s<T>(&sh, J->jobs.as<LineJob<T>>() + s, 1);
+        if (rc) return rc;
+        if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)
+            ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice, J->stream));
+    }
+    ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
+    return ZQD_OK;
+}
+
+template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
+    size_t rows = (size_t)J->o.iterations + 1;
+    std::vector<double> hist((size_t)J->nsolve * rows * J->hc), fin((size_t)J->nsolve * J->hc);
+    std::vector<int> nrows(J->nsolve);
+    ZQD_CUDA(cudaMemcpyAsync(hist.data(), J->hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaMemcpyAsync(fin.data(), J->fin.p, fin.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaMemcpyAsync(nrows.data(), J->rows.p, nrows.size() * sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    const size_t SN = (size_t)J->S * J->n;
+    std::vector<cx<T>> save(SN), orth;
+    ZQD_CUDA(cudaMemcpyAsync(save.data(), J->psi_save.p, SN * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
+    if (J->nsolve > 1) {
+        orth.resize((size_t)(J->nsolve - 1) * SN);
+        ZQD_CUDA(cudaMemcpyAsync(orth.data(), J->orth.p, orth.size() * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
+    }
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    R->ndim = 1;
+    R->nstate = J->S;
+    R->npoint_total = J->n;
+    R->hc = J->hc;
+    R->write_mask = J->o.write_mask;
+    R->device_ms = J->last_ms;
+    R->solves.resize(J->nsolve);
+    for (int s = 0; s < J->nsolve; ++s) {
+        SolveOut& so = R->solves[s];
+        so.rows = (size_t)nrows[s];
+        so.hist.assign(hist.begin() + (size_t)s * rows * J->hc, hist.begin() + ((size_t)s * rows + so.rows) * J->hc);
+        so.fin.assign(fin.begin() + (size_t)s * J->hc, fin.begin() + (size_t)(s + 1) * J->hc);
+        const cx<T>* src = (s + 1 < J->nsolve) ? orth.data() + (size_t)s * SN : save.data();
+        so.psi.resize(2 * SN);
+        for (int st = 0; st < J->S; ++st)
+            for (int p = 0; p < J->n; ++p) { // un-permute: position p = c*m + j holds grid index c + C*j
+                int c = p / J->m, j = p - c * J->m, x = c + J->C * j;
+                cx<T> z = src[(size_t)st * J->n + p];
+                so.psi[2 * ((size_t)st * J->n + x)] = (double)z.x;
+                so.psi[2 * ((size_t)st * J->n + x) + 1] = (double)z.y;
+            }
+    }
+    return ZQD_OK;
+}
+
+} // namespace zqd
+
+// ------------------------------------------------------------------ C-ABI
+extern "C" int zqd_job_create(const zqd_options* opt, zqd_job** out) {
+    if (!out) return fail(ZQD_ERR_INVALID_INPUT, "NULL OUTPUT HANDLE");
+    *out = nullptr;
+    std::unique_ptr<zqd_job> J(new (std::nothrow) zqd_job());
+    if (!J) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    int rc = copy_options(opt, J->o);
+    if (rc) return rc;
+    if ((rc = validate(J->o))) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ZQD_ERR_NO_DEVICE, "no CUDA device");
+    J->S = J->o.pot_ns;
+    J->d = (int)J->o.ndim;
+    J->n = (int)J->o.npoint;
+    J->N = 1;
+    for (int i = 0; i < J->d; ++i) J->N *= (size_t)J->n;
+    J->fp32 = J->o.precision == ZQD_FP32_MIXED;
+    J->nsolve = J->o.imag_nstate ? (int)J->o.imag_nstate : 1;
+    J->hc = RowLayout{J->d, J->S}.width();
+    if (J->d != 1) return fail(ZQD_ERR_UNSUPPORTED, "MULTI-DIMENSIONAL GRIDS ARE NOT AVAILABLE IN THIS BUILD YET");
+    if ((rc = choose_line_shape(J.get()))) return rc;
+    ZQD_CUDA(cudaStreamCreateWithFlags(&J->stream, cudaStreamNonBlocking));
+    ZQD_CUDA(cudaEventCreate(&J->ev0));
+    ZQD_CUDA(cudaEventCreate(&J->ev1));
+    if ((rc = build_potential(J->o, J->pot))) return rc;
+    rc = J->fp32 ? create_line<float>(J.get()) : create_line<double>(J.get());
+    if (rc) return rc;
+    *out = J.release();
+    return ZQD_OK;
+}
+
+extern "C" int zqd_job_run(zqd_job* J) {
+    if (!J) return fail(ZQD_ERR_INVALID_INPUT, "NULL JOB");
+    return J->fp32 ? run_line<float>(J) : run_line<double>(J);
+}
+
+extern "C" int zqd_job_result(zqd_job* J, zqd_result** out) {
+    if (!J || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    std::unique_ptr<zqd_result> R(new (std::nothrow) zqd_result());
+    if (!R) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
+    int rc = J->fp32 ? fetch_line<float>(J, R.get()) : fetch_line<double>(J, R.get());
+    if (rc) return rc;
+    *out = R.release();
+    return ZQD_OK;
+}
+
+extern "C" int zqd_job_info(const zqd_job* J, uint32_t* ndim, uint32_t* nstate, uint64_t* npoint_total,
+                            uint32_t* cluster_ctas, size_t* device_bytes) {
+    if (!J) return fail(ZQD_ERR_INVALID_INPUT, "NULL JOB");
+    if (ndim) *ndim = (uint32_t)J->d;
+    if (nstate) *nstate = (uint32_t)J->S;
+    if (npoint_total) *npoint_total = J->N;
+    if (cluster_ctas) *cluster_ctas = (uint32_t)J->C;
+    if (device_bytes) *device_bytes = J->device_bytes;
+    return ZQD_OK;
+}
+
+extern "C" double zqd_job_device_ms(const zqd_job* J) { return J ? (double)J->last_ms : 0.0; }
+
+extern "C" void zqd_job_destroy(zqd_job* J) { delete J; }
+
+extern "C" int zqd_run(const zqd_options* opt, zqd_result** out) {
+    if (!out) return fail(ZQD_ERR_INVALID_INPUT, "NULL OUTPUT HANDLE");
+    *out = nullptr;
+    zqd_job* J = nullptr;
+    int rc = zqd_job_create(opt, &J);
+    if (rc) return rc;
+    rc = zqd_job_run(J);
+    if (!rc) rc = zqd_job_result(J, out);
+    zqd_job_destroy(J);
+    return rc;
+}
+
+namespace zqd {
+// One launch advances every job of a group: cluster i of the grid runs job i.
+template <typename T> static int run_group(std::vector<zqd_job*>& grp, float* ms) {
+    zqd_job* lead = grp[0];
+    std::vector<LineJob<T>> descs;
+    LaunchShape sh{lead->S, lead->C, lead->E, 0, 0, lead->stream};
+    for (zqd_job* J : grp) {
+        descs.push_back(line_job_desc<T>(J, 0));
+        sh.threads = std::max(sh.threads, J->threads);
+        sh.smem = std::max(sh.smem, J->smem);
+    }
+    DevBuf d;
+    int rc = d.alloc(descs.size() * sizeof(LineJob<T>));
+    if (rc) return rc;
+    ZQD_CUDA(cudaMemcpyAsync(d.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, lead->stream));
+    ZQD_CUDA(cudaEventRecord(lead->ev0, lead->stream));
+    if ((rc = launch_line_s<T>(&sh, d.p, (int)grp.size()))) return rc;
+    ZQD_CUDA(cudaEventRecord(lead->ev1, lead->stream));
+    ZQD_CUDA(cudaStreamSynchronize(lead->stream));
+    ZQD_CUDA(cudaEventElapsedTime(ms, lead->ev0, lead->ev1));
+    for (zqd_job* J : grp) J->last_ms = *ms;
+    return ZQD_OK;
+}
+} // namespace zqd
+
+extern "C" int zqd_run_batch(const zqd_options* const* opts, uint32_t njobs, zqd_result** results) {
+    if (!opts || !results) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    for (uint32_t i = 0; i < njobs; ++i) results[i] = nullptr;
+    std::vector<std::unique_ptr<zqd_job, void (*)(zqd_job*)>> jobs;
+    for (uint32_t i = 0; i < njobs; ++i) {
+        zqd_job* J = nullptr;
+        int rc = zqd_job_create(opts[i], &J);
+        if (rc) return rc;
+        jobs.emplace_back(J, zqd_job_destroy);
+    }
+    // group single-solve jobs by kernel instantiation; multi-solve (ITP) jobs run alone
+    std::vector<bool> done(njobs, false);
+    for (uint32_t i = 0; i < njobs; ++i) {
+        if (done[i]) continue;
+        zqd_job* a = jobs[i].get();
+        if (a->nsolve > 1) {
+            int rc = zqd_job_run(a);
+            if (rc) return rc;
+            done[i] = true;
+            continue;
+        }
+        std::vector<zqd_job*> grp{a};
+        done[i] = true;
+        for (uint32_t k = i + 1; k < njobs; ++k) {
+            zqd_job* b = jobs[k].get();
+            if (!done[k] && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C && b->E == a->E) {
+                grp.push_back(b);
+                done[k] = true;
+            }
+        }
+        float ms = 0;
+        int rc = a->fp32 ? run_group<float>(grp, &ms) : run_group<double>(grp, &ms);
+        if (rc) return rc;
+    }
+    for (uint32_t i = 0; i < njobs; ++i) {
+        int rc = zqd_job_result(jobs[i].get(), &results[i]);
+        if (rc) {
+            for (uint32_t k = 0; k < i; ++k) {
+                zqd_result_destroy(results[k]);
+                results[k] = nullptr;
+            }
+            return rc;
+        }
+    }
+    return ZQD_OK;
+}
+
+extern "C" int zqd_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+extern "C" int zqd_set_device(int dev) {
+    ZQD_CUDA(cudaSetDevice(dev));
+    return ZQD_OK;
+}

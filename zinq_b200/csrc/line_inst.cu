@@ -1,0 +1,53 @@
+// line_inst.cu -- instantiations of the resident line kernel for one
+// (precision, state count) pair.  The build compiles this file once per pair
+// with -DZQD_T=<double|float> -DZQD_S=<1..4> -DZQD_LAUNCH=<symbol>, so the
+// heavy template instantiations spread over parallel nvcc processes.
+#include <mutex>
+
+#include "internal.h"
+#include "line_kernel.cuh"
+
+#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_LAUNCH)
+#error "line_inst.cu needs -DZQD_T, -DZQD_S and -DZQD_LAUNCH"
+#endif
+
+namespace zqd {
+
+template <int C> static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
+    auto kern = line_solve_kernel<ZQD_T, ZQD_S, C>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [&] {
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+        if (attr_err == cudaSuccess && C > 8)
+            attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
+    ZQD_CUDA(attr_err);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * njobs, 1, 1);
+    cfg.blockDim = dim3(J->threads, 1, 1);
+    cfg.dynamicSmemBytes = J->smem;
+    cfg.stream = J->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ZQD_CUDA(cudaLaunchKernelEx(&cfg, kern, reinterpret_cast<const LineJob<ZQD_T>*>(d_jobs)));
+    return ZQD_OK;
+}
+
+int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
+    switch (J->C) {
+    case 1: return launch_one<1>(J, dj, nj);
+    case 2: return launch_one<2>(J, dj, nj);
+    case 4: return launch_one<4>(J, dj, nj);
+    case 8: return launch_one<8>(J, dj, nj);
+    case 16: return launch_one<16>(J, dj, nj);
+    default: return fail(ZQD_ERR_UNSUPPORTED, "CLUSTER SIZE MUST BE 1, 2, 4, 8 OR 16");
+    }
+}
+
+} // namespace zqd

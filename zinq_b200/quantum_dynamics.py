@@ -1,0 +1,299 @@
+"""Host-side mirror of Zinq's `quantum_dynamics` method over the C-ABI.
+
+`run(options)` takes a ``quantum_dynamics`` options object in the reference's
+JSON schema (src/quantum_dynamics.zig:25-67, src/wavepacket.zig:16-23,
+src/potential.zig:19-60) and returns a `Result` whose ``observables`` list
+holds one `Observables` per imaginary-time state, like
+``quantum_dynamics.run(f64, io, opt, log, gpa)`` (:567-603).  Invalid input
+raises `ZqdError` with the reference's message (checkInvalidInput, :606-710).
+All arithmetic runs on the GPU through libzinq_qd.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import ZqdError, check
+
+POT_DEFAULTS = {  # src/potential.zig:24-48
+    "harmonic": {"k": [1.0]},
+    "time_linear": {"a": 10.0, "g": 2.0},
+    "tully_1": {"A": 0.010, "B": 1.600, "C": 0.005, "D": 1.000},
+    "tully_2": {"A": 0.10, "B": 0.28, "C": 0.015, "D": 0.06, "E0": 0.05},
+    "tully_3": {"A": 6.0e-4, "B": 0.10, "C": 0.90},
+}
+PARAM_ORDER = {"time_linear": ["a", "g"], "tully_1": ["A", "B", "C", "D"], "tully_2": ["A", "B", "C", "D", "E0"],
+               "tully_3": ["A", "B", "C"]}
+
+
+@dataclass
+class Observables:
+    """Final expectation values of one solve (Observables, quantum_dynamics.zig:282-375)."""
+    pos: np.ndarray
+    mom: np.ndarray
+    pop: np.ndarray
+    epot: float
+    ekin: float
+    norm: float
+    acf: complex | None
+    history: dict = field(default_factory=dict)
+    wavefunction: np.ndarray | None = None
+
+
+@dataclass
+class Result:
+    """Result(T) (quantum_dynamics.zig:70-83) plus the device time of the propagation."""
+    observables: list
+    device_ms: float = 0.0
+
+
+def read_matrix(path):
+    """readMatrix (src/read_write.zig:24-56): a "rows cols" header, then whitespace-separated values."""
+    with open(path) as f:
+        hdr = f.readline().split()
+        nrow, ncol = int(hdr[0]), int(hdr[1])
+        data = np.array(f.read().split(), dtype=np.float64)
+    return data[: nrow * ncol].reshape(nrow, ncol)
+
+
+class _Keep:
+    """Owns the ctypes buffers an options struct points at."""
+
+    def __init__(self):
+        self.refs = []
+
+    def arr(self, x):
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+        self.refs.append(a)
+        return a.ctypes.data_as(_abi.DP)
+
+
+def to_struct(opt: dict, precision: str = "fp64", log: bool = False):
+    """Translate a reference-schema options dict into zqd_options; returns (struct, keepalive)."""
+    L = _abi.load()
+    keep = _Keep()
+    o = _abi.ZqdOptions()
+    L.zqd_options_init(C.byref(o))
+    g = opt["grid"]
+    bounds = [list(b) for b in g["bounds"]]
+    o.ndim = len(bounds)
+    o.npoint = int(g["npoint"])
+    o.grid_bounds = keep.arr(bounds)
+    ic = opt["initial_conditions"]
+    o.ic_position, o.ic_momentum, o.ic_gamma = keep.arr(ic["position"]), keep.arr(ic["momentum"]), keep.arr(ic["gamma"])
+    # the C struct carries one length (ndim) for these arrays; mismatches are reported with the reference's messages
+    if len(opt["mass"]) != len(ic["position"]):
+        raise ZqdError(-1, "MASS VECTOR MUST HAVE THE SAME LENGTH AS POSITION VECTOR")
+    if len(ic["momentum"]) != len(ic["position"]):
+        raise ZqdError(-1, "INITIAL MOMENTUM AND POSITION VECTORS MUST HAVE THE SAME LENGTH")
+    if len(ic["gamma"]) != len(ic["position"]):
+        raise ZqdError(-1, "INITIAL GAMMA VECTOR MUST HAVE THE SAME LENGTH AS POSITION VECTOR")
+    if len(ic["position"]) == 0:
+        raise ZqdError(-1, "INITIAL POSITION VECTOR MUST NOT BE EMPTY")
+    if len(ic["position"]) != len(bounds):
+        raise ZqdError(-1, "INITIAL CONDITIONS DIMENSION DOES NOT MATCH GRID DIMENSION")
+    o.ic_state = int(ic.get("state", 0))
+    o.ic_adiabatic = int(bool(ic.get("adiabatic", False)))
+    o.time_step = float(opt["time_step"])
+    o.iterations = int(opt["iterations"])
+    o.mass = keep.arr(opt["mass"])
+    wm = 0
+    for k, v in (opt.get("write") or {}).items():
+        if v is not None:
+            wm |= _abi.WRITE[k]
+    o.write_mask = wm
+    o.adiabatic = int(bool(opt.get("adiabatic", False)))
+    o.log_interval = int(opt.get("log_interval", 1))
+    cap = opt.get("absorbing_potential")
+    if cap is not None:
+        if len(cap["bounds"]) != len(bounds):
+            raise ZqdError(-1, "ABSORBING POTENTIAL BOUNDS DIMENSION DOES NOT MATCH GRID DIMENSION")
+        o.has_absorbing_potential = 1
+        o.cap_track_population = int(bool(cap.get("track_population", False)))
+        o.cap_bounds = keep.arr(cap["bounds"])
+        o.cap_exponent = float(cap.get("exponent", 0.001))
+        if cap.get("stop_norm") is not None:
+            o.cap_has_stop_norm = 1
+            o.cap_stop_norm = float(cap["stop_norm"])
+    o.fft_plan = _abi.FFT_PLAN[(opt.get("fft") or {}).get("plan", "measure")]
+    imag = opt.get("imaginary")
+    if imag is not None:
+        o.imaginary_nstate = int(imag.get("nstate", 1))
+        if o.imaginary_nstate == 0:
+            raise ZqdError(-1, "ITP TARGET STATE COUNT MUST BE GREATER THAN 0")
+    spec = opt.get("spectrum")
+    if spec is not None:
+        o.has_spectrum = 1
+        o.spectrum_padding = int(spec.get("padding", 0))
+        o.spectrum_threshold = float(spec.get("threshold", 1e-6))
+    o.precision = _abi.PRECISION[precision]
+    o.log = int(bool(log))
+
+    (pname, pval), = opt["potential"].items()
+    pval = dict(POT_DEFAULTS.get(pname, {}), **(pval or {}))
+    p = o.potential
+    L.zqd_potential_init(C.byref(p), _abi.POT[pname])
+    if pname == "harmonic":
+        p.harmonic_k = keep.arr(pval["k"])
+        p.harmonic_ndim = len(pval["k"])
+    elif pname in PARAM_ORDER:
+        for i, k in enumerate(PARAM_ORDER[pname]):
+            p.p[i] = float(pval[k])
+    elif pname == "custom":
+        mat = pval["matrix"]
+        ns = len(mat)
+        if any(len(row) != ns for row in mat):
+            raise ZqdError(-1, "NonSquareMatrix")
+        strs = [s.encode() for row in mat for s in row]
+        arr = (C.c_char_p * len(strs))(*strs)
+        keep.refs.append(arr)
+        p.custom_matrix = C.cast(arr, C.POINTER(C.c_char_p))
+        p.custom_nstate = ns
+        p.custom_ndim = int(pval["ndim"])
+        p.custom_time_dependent = int(bool(pval.get("time_dependent", False)))
+    elif pname == "lvc":
+        freq = np.asarray(pval["frequencies"], float)
+        exc = np.asarray(pval["excitation_energies"], float)
+        p.lvc_frequencies, p.lvc_nmode = keep.arr(freq), len(freq)
+        p.lvc_excitation_energies, p.lvc_nstate = keep.arr(exc), len(exc)
+        p.lvc_kappa = keep.arr(np.asarray(pval["kappa"], float))
+        p.lvc_lambda = keep.arr(np.asarray(pval["lambda"], float))
+    elif pname == "file":
+        table = pval["data"] if "data" in pval else read_matrix(pval["path"])
+        table = np.ascontiguousarray(table, dtype=np.float64)
+        p.file_table = keep.arr(table)
+        p.file_nrow, p.file_ncol = table.shape
+        p.file_ndim = int(pval["ndim"])
+    else:
+        raise ZqdError(-1, f"UNKNOWN POTENTIAL {pname}")
+    return o, keep
+
+
+def _collect(res_ptr):
+    L = _abi.load()
+    out = []
+    for s in range(L.zqd_result_nsolve(res_ptr)):
+        ob = _abi.ZqdObservables()
+        check(L.zqd_result_final(res_ptr, s, C.byref(ob)))
+        d, S = ob.ndim, ob.nstate
+        hist = {}
+        for name, code in _abi.SERIES.items():
+            ptr, rows, cols = _abi.DP(), C.c_size_t(), C.c_size_t()
+            if L.zqd_result_series(res_ptr, s, code, C.byref(ptr), C.byref(rows), C.byref(cols)) == 0:
+                a = np.ctypeslib.as_array(ptr, shape=(rows.value * cols.value,)).copy().reshape(rows.value, cols.value)
+                hist[name] = a[:, 0] + 1j * a[:, 1] if name == "acf" else a
+        acf = None if np.isnan(ob.acf_re) else complex(ob.acf_re, ob.acf_im)
+        out.append(Observables(pos=np.array(ob.pos[:d]), mom=np.array(ob.mom[:d]), pop=np.array(ob.pop[:S]),
+                               epot=ob.epot, ekin=ob.ekin, norm=ob.norm, acf=acf, history=hist))
+    return out
+
+
+def _attach_wavefunctions(res_ptr, obs, npoint_total, nstate):
+    L = _abi.load()
+    for s, ob in enumerate(obs):
+        buf = np.zeros(2 * nstate * npoint_total)
+        check(L.zqd_result_wavefunction(res_ptr, s, buf.ctypes.data_as(_abi.DP), buf.size))
+        ob.wavefunction = (buf[0::2] + 1j * buf[1::2]).reshape(nstate, npoint_total)
+
+
+def _shape(opt):
+    g = opt["grid"]
+    return int(g["npoint"]) ** len(g["bounds"])
+
+
+def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction: bool = True) -> Result:
+    """quantum_dynamics.run on the GPU (src/quantum_dynamics.zig:567-603)."""
+    L = _abi.load()
+    o, keep = to_struct(opt, precision, log)
+    res = C.c_void_p()
+    check(L.zqd_run(C.byref(o), C.byref(res)))
+    try:
+        obs = _collect(res)
+        if want_wavefunction and obs:
+            S = len(obs[0].pop)
+            _attach_wavefunctions(res, obs, _shape(opt), S)
+        return Result(observables=obs, device_ms=L.zqd_result_device_ms(res))
+    finally:
+        L.zqd_result_destroy(res)
+
+
+def run_batch(opts: list, precision: str = "fp64", want_wavefunction: bool = False) -> list:
+    """Several independent jobs advanced together (zqd_run_batch); one Result per options dict."""
+    L = _abi.load()
+    structs = [to_struct(o, precision) for o in opts]
+    arr = (C.POINTER(_abi.ZqdOptions) * len(opts))(*[C.pointer(s) for s, _ in structs])
+    res = (C.c_void_p * len(opts))()
+    check(L.zqd_run_batch(arr, len(opts), res))
+    out = []
+    try:
+        for i, r in enumerate(res):
+            obs = _collect(r)
+            if want_wavefunction and obs:
+                _attach_wavefunctions(r, obs, _shape(opts[i]), len(obs[0].pop))
+            out.append(Result(observables=obs, device_ms=L.zqd_result_device_ms(r)))
+    finally:
+        for r in res:
+            if r:
+                L.zqd_result_destroy(r)
+    return out
+
+
+class Job:
+    """Staged form: device tables built at construction, `run()` propagates with no host copies."""
+
+    def __init__(self, opt: dict, precision: str = "fp64"):
+        self._L = _abi.load()
+        self.opt = opt
+        self._o, self._keep = to_struct(opt, precision)
+        self._h = C.c_void_p()
+        check(self._L.zqd_job_create(C.byref(self._o), C.byref(self._h)))
+
+    def info(self):
+        d, s, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        n, b = C.c_uint64(), C.c_size_t()
+        check(self._L.zqd_job_info(self._h, C.byref(d), C.byref(s), C.byref(n), C.byref(c), C.byref(b)))
+        return {"ndim": d.value, "nstate": s.value, "npoint_total": n.value, "cluster_ctas": c.value,
+                "device_bytes": b.value}
+
+    def run(self) -> float:
+        check(self._L.zqd_job_run(self._h))
+        return self._L.zqd_job_device_ms(self._h)
+
+    def result(self, want_wavefunction=True) -> Result:
+        res = C.c_void_p()
+        check(self._L.zqd_job_result(self._h, C.byref(res)))
+        try:
+            obs = _collect(res)
+            if want_wavefunction and obs:
+                _attach_wavefunctions(res, obs, _shape(self.opt), len(obs[0].pop))
+            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res))
+        finally:
+            self._L.zqd_result_destroy(res)
+
+    def close(self):
+        if self._h:
+            self._L.zqd_job_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_file(path: str, precision: str = "fp64"):
+    """Runs every quantum_dynamics job of a Zinq input file ({"zinq": [...]}, src/main.zig:63-73,122-135)."""
+    with open(path) as f:
+        doc = json.load(f)
+    out = []
+    for entry in doc["zinq"]:
+        for tag, opt in entry.items():
+            if tag != "quantum_dynamics":
+                raise ZqdError(-7, f"method {tag!r} is outside this library")
+            out.append(run(opt, precision, log=True))
+    return out
