@@ -1,0 +1,316 @@
+"""Benchmark: grid-pt*state*steps/s of the split-operator propagator on B200.
+
+Workload (the reference configuration the headline metric is quoted on): the
+1-D two-state avoided crossing, V11 = 0.01 tanh(1.6x) = -V22,
+V12 = 0.005 exp(-x^2), mass 2000, 8192 points on [-24, 24], Gaussians at
+x0 = -10 with sigma = 20/p0 for p0 in {10, 15, 20, 25, 30} (5 jobs), dt = 1,
+4000 steps, adiabatic populations recorded every step.  One bench step is one
+full propagation of the 5-job batch (5 x 8192 x 2 x 4000 grid-pt*state*steps).
+Inputs are synthetic (generated here), no dataset is involved.
+
+Legs printed in one JSON line:
+  value      FP32 batched form, tables resident on the device, device time
+             (CUDA events on the library's stream), L2 flushed between steps;
+  fp64       the plain FP64 form on the same batch;
+  e2e        zqd_run_batch through the public API from host options to host
+             results (table setup, H2D, D2H inside the timed region);
+  roofline   the resident line kernel against the measured HBM copy bandwidth;
+  cpu_baseline  the oracle port, single thread, on a bounded sample.
+`--impl reference` times the CPU restatement of the reference path (the
+oracle) with all host threads on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt*state*steps/s (FP32-batched vs FP64, 1 B200)"
+UNIT = "grid-pt*state*steps/s"
+MOMENTA = (10.0, 15.0, 20.0, 25.0, 30.0)
+NPOINT, NSTATE, ITERS = 8192, 2, 4000
+# algorithmic bytes per grid-pt*state*step of a 1-D two-state step:
+# psi read+write once (2*S*c per point) plus two reads of the complex R table (2*S^2*c), over S
+BYTES_PER_UNIT = {"fp64": (2 * 1 * NSTATE * 16 + 2 * NSTATE**2 * 16) / NSTATE,
+                  "fp32": (2 * 1 * NSTATE * 8 + 2 * NSTATE**2 * 8) / NSTATE}
+
+
+def workload(iters=ITERS):
+    opts = []
+    for p0 in MOMENTA:
+        opts.append({
+            "grid": {"bounds": [[-24, 24]], "npoint": NPOINT},
+            "initial_conditions": {"position": [-10.0], "momentum": [p0], "gamma": [p0 * p0 / 400.0], "state": 0,
+                                   "adiabatic": True},
+            "potential": {"custom": {"ndim": 1, "matrix": [["0.01*tanh(1.6*r1)", "0.005*exp(-r1^2)"],
+                                                           ["0.005*exp(-r1^2)", "-0.01*tanh(1.6*r1)"]]}},
+            "mass": [2000.0], "iterations": iters, "time_step": 1.0, "adiabatic": True,
+            "write": {"population": "POP.mat"},
+        })
+    return opts
+
+
+def units(opts):
+    return sum(o["grid"]["npoint"] ** len(o["grid"]["bounds"]) * NSTATE * o["iterations"] for o in opts)
+
+
+def config(extra=None):
+    c = {"workload": "1-D two-state tanh crossing, 8192 pts x 2 states, 5 momenta, 4000 steps, dt 1",
+         "jobs": len(MOMENTA), "npoint": NPOINT, "nstate": NSTATE, "iterations": ITERS,
+         "l2": "flushed between timed steps (512 MiB write)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- CPU legs
+def oracle_sample(opts, threads):
+    from oracle import qd_ref
+
+    t0 = time.perf_counter()
+    if threads == 1:
+        res = [qd_ref.run(o, want_wavefunction=False) for o in opts]
+    else:
+        with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+            res = list(ex.map(lambda o: qd_ref.run(o, want_wavefunction=False), opts))
+    return time.perf_counter() - t0, res
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    sample_iters = 1000  # bounded sample per step: 5 jobs x 1000 steps, all jobs in parallel threads
+    opts = workload(sample_iters)
+    threads = min(len(opts), os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        oracle_sample(opts, threads)
+    tot = 0.0
+    for _ in range(args.steps):
+        dt, _ = oracle_sample(opts, threads)
+        tot += dt
+    value = units(opts) * args.steps / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config({"sample": f"{len(opts)} jobs x {sample_iters} steps per bench step"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{len(opts)} jobs x {sample_iters} steps, one thread per job"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU legs
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu_index, path):
+        self.path = path
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = None
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(gpu_index), "-lms", "50"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_traffic(kernel, precision):
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        p = line.split()
+        if len(p) >= 3 and p[0] == kernel and p[1] == precision:
+            return float(p[2])
+    return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="zinq_b200", choices=["zinq_b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
+                    help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
+    args = ap.parse_args()
+
+    if args.profile_case:
+        from zinq_b200 import quantum_dynamics as qd
+
+        b = qd.Batch(workload(200)[2:3], args.profile_case)
+        for _ in range(2):
+            ms = b.run()
+        print(json.dumps({"profile_case": args.profile_case, "ms": ms, "launches": b.launches}))
+        return
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import datetime
+
+    import numpy as np
+    import torch
+
+    from zinq_b200 import _abi
+    from zinq_b200 import quantum_dynamics as qd
+
+    torch.cuda.set_device(local)
+    _abi.check(_abi.load().zqd_set_device(local))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    opts = workload()
+    U = units(opts)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(batch, steps, warm):
+        for _ in range(warm):
+            batch.run()
+        barrier()
+        times = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            times.append(batch.run())
+        barrier()
+        return times
+
+    fp64 = qd.Batch(opts, "fp64")
+    fp32 = qd.Batch(opts, "fp32")
+    clk = Clocks(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                     f"bench_clocks_rank{rank}.csv"))
+    t32 = timed(fp32, args.steps, args.warmup)
+    t64 = timed(fp64, args.steps, args.warmup)
+    clocks = clk.stop()
+    launches32 = fp32.launches * args.steps
+    launches64 = fp64.launches * args.steps
+
+    # accuracy of the FP32 form against the FP64 form (itself parity-tested against the oracle)
+    pop_err = 0.0
+    for i in range(len(opts)):
+        a = fp32.result(i).observables[0].history["population"]
+        b = fp64.result(i).observables[0].history["population"]
+        pop_err = max(pop_err, float(np.max(np.abs(a - b))))
+
+    # end to end through the public API, host options -> host results
+    for _ in range(args.warmup):
+        qd.run_batch_e2e(opts, "fp32")
+    barrier()
+    e2e_times, h2d, d2h = [], 0, 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, h2d, d2h = qd.run_batch_e2e(opts, "fp32")
+        e2e_times.append(time.perf_counter() - t0)
+    barrier()
+
+    def maxall(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    s32 = maxall(sum(t32) / 1e3)
+    s64 = maxall(sum(t64) / 1e3)
+    se2e = maxall(sum(e2e_times))
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    value = world * U * args.steps / s32
+    v64 = world * U * args.steps / s64
+    peak, peak_kind = measured_peak()
+    per_launch = statistics.mean(t32) / 1e3  # one grouped launch runs the whole batch
+    achieved = BYTES_PER_UNIT["fp32"] * U / per_launch / 1e9
+    traffic = read_traffic("line_solve_kernel", "fp32")
+    lat = sorted(t32)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * s32 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config({"precision": "FP32 state/butterflies/phases, FP64 tables split hi+lo, FP64 reductions",
+                          "parallelism": f"replicas x{world}"}),
+        "fp64": {"value": v64, "unit": UNIT, "ms_per_step": 1e3 * s64 / args.steps, "dtype": "f64",
+                 "gpu_launches": launches64},
+        "fp32_over_fp64": value / v64,
+        "pop_err_fp32_vs_fp64": pop_err, "pop_err_ok": pop_err <= 1e-5,
+        "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                       "note": "per job; the 5 jobs of a step complete together in one launch"},
+        "e2e": {"value": world * U * args.steps / se2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": launches32,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "note": "algorithmic bytes per grid-pt*state*step (psi r+w once, R read twice); the resident "
+                             "kernel keeps psi in shared memory across steps, so frac > 1 is on-chip residency"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu:
+        sample = workload(ITERS)[2:4]
+        dt, _ = oracle_sample(sample, 1)
+        line["cpu_baseline"] = {"value": units(sample) / dt, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"2 of the 5 jobs (p0 = 20, 25) x {ITERS} steps, single thread"}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -221,9 +221,26 @@ double zqd_job_device_ms(const zqd_job* job);
 void zqd_job_destroy(zqd_job* job);
 
 /* Several independent jobs advanced together on the device (the batched
-   form): one launch per group of jobs with equal shape and precision.
-   results[i] receives the result of opts[i]. */
+   form): one launch per group of jobs with equal kernel shape and precision,
+   cluster i of the grid running job i.  results[i] receives the result of
+   opts[i].  Replaces a loop of quantum_dynamics.run calls. */
 int zqd_run_batch(const zqd_options* const* opts, uint32_t njobs, zqd_result** results);
+
+/* Staged form of zqd_run_batch: tables of every job built once at create;
+   each zqd_batch_run propagates all jobs again from their initial state with
+   no host copies.  zqd_batch_launches reports the kernel launches of the last
+   run. */
+typedef struct zqd_batch zqd_batch;
+int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, zqd_batch** out);
+int zqd_batch_run(zqd_batch* batch);
+int zqd_batch_result(zqd_batch* batch, uint32_t index, zqd_result** out);
+double zqd_batch_device_ms(const zqd_batch* batch);
+uint32_t zqd_batch_launches(const zqd_batch* batch);
+void zqd_batch_destroy(zqd_batch* batch);
+
+/* Bytes the library copied host->device and device->host for this result
+   (options, tables and descriptors in; observables and wavefunctions out). */
+int zqd_result_transfer_bytes(const zqd_result* res, uint64_t* h2d, uint64_t* d2h);
 
 /* ------------------------------------------------------------ FFT seam
  * Replaces FftPlan(T) (src/fourier_transform.zig:8-49: fftw_plan_dft,

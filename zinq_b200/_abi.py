@@ -97,6 +97,13 @@ SIGNATURES = [
     ("zqd_job_device_ms", C.c_double, [VP]),
     ("zqd_job_destroy", None, [VP]),
     ("zqd_run_batch", C.c_int, [C.POINTER(C.POINTER(ZqdOptions)), C.c_uint32, C.POINTER(VP)]),
+    ("zqd_batch_create", C.c_int, [C.POINTER(C.POINTER(ZqdOptions)), C.c_uint32, C.POINTER(VP)]),
+    ("zqd_batch_run", C.c_int, [VP]),
+    ("zqd_batch_result", C.c_int, [VP, C.c_uint32, C.POINTER(VP)]),
+    ("zqd_batch_device_ms", C.c_double, [VP]),
+    ("zqd_batch_launches", C.c_uint32, [VP]),
+    ("zqd_batch_destroy", None, [VP]),
+    ("zqd_result_transfer_bytes", C.c_int, [VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("zqd_fft_plan_create", C.c_int, [C.c_uint32, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(VP)]),
     ("zqd_fft_execute", C.c_int, [VP, VP, VP]),
     ("zqd_fft_destroy", None, [VP]),

@@ -22,7 +22,7 @@ struct zqd_fft {
 
 template <typename T, int SIGN>
 __global__ void __launch_bounds__(512) fft_axis_kernel(cx<T>* data, int n, int logn, size_t stride, size_t N,
-                                                       const cx<T>* tw) {
+                                                       const Tab<T>* tw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* buf = reinterpret_cast<cx<T>*>(smem_raw);
     const size_t line = blockIdx.x; // line index among N / n
@@ -58,9 +58,10 @@ extern "C" int zqd_fft_plan_create(uint32_t ndim, const int* shape, int sign, zq
     p->fp32 = precision == ZQD_FP32_MIXED;
     std::vector<double> tw = twiddles_f64(n);
     if (p->fp32) {
-        std::vector<float> f(tw.begin(), tw.end());
-        ZQD_CUDA(cudaMalloc(&p->tw, f.size() * sizeof(float)));
-        ZQD_CUDA(cudaMemcpy(p->tw, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+        std::vector<float4> f(n);
+        for (int t = 0; t < n; ++t) f[t] = mktab<float>(tw[2 * t], tw[2 * t + 1]);
+        ZQD_CUDA(cudaMalloc(&p->tw, f.size() * sizeof(float4)));
+        ZQD_CUDA(cudaMemcpy(p->tw, f.data(), f.size() * sizeof(float4), cudaMemcpyHostToDevice));
     } else {
         ZQD_CUDA(cudaMalloc(&p->tw, tw.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(p->tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -80,9 +81,9 @@ template <typename T> static int fft_exec(zqd_fft* p, void* data, cudaStream_t s
     for (int a = p->ndim - 1; a >= 0; --a) {
         unsigned lines = (unsigned)(p->N / p->n);
         if (p->sign < 0)
-            kf<<<lines, threads, smem, st>>>((cx<T>*)data, p->n, p->logn, stride, p->N, (const cx<T>*)p->tw);
+            kf<<<lines, threads, smem, st>>>((cx<T>*)data, p->n, p->logn, stride, p->N, (const Tab<T>*)p->tw);
         else
-            ki<<<lines, threads, smem, st>>>((cx<T>*)data, p->n, p->logn, stride, p->N, (const cx<T>*)p->tw);
+            ki<<<lines, threads, smem, st>>>((cx<T>*)data, p->n, p->logn, stride, p->N, (const Tab<T>*)p->tw);
         ZQD_CUDA(cudaGetLastError());
         stride *= (size_t)p->n;
     }

@@ -61,6 +61,7 @@ struct PotStore {
     double* d_consts = nullptr;
     double* d_lvc = nullptr;
     double* d_file = nullptr;
+    size_t bytes = 0; // uploaded to the device
     ~PotStore();
 };
 int build_potential(const Opts& o, PotStore& ps);
@@ -86,4 +87,5 @@ struct zqd_result {
     double device_ms = 0;
     uint32_t write_mask = 0;
     int hc = 0;
+    uint64_t h2d = 0, d2h = 0;
 };

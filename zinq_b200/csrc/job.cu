@@ -7,7 +7,7 @@
 #include <mutex>
 
 #include "internal.h"
-#include "line_kernel.cuh"
+#include "line_solve.cuh"
 
 namespace zqd {
 
@@ -18,11 +18,11 @@ template <typename T> struct LineTablesArgs {
     int has_cap;
     double cap_lo, cap_hi, cap_exp;
     PotDev pot;
-    cx<T>* R;
+    Tab<T>* R;
     double* V;
     double* U;
     double* capw;
-    cx<T>* expk;
+    Tab<T>* expk;
 };
 
 // Hamiltonian.init/update at t = 0 (wavepacket.zig:96-143) and Propagator.init/update
@@ -53,7 +53,7 @@ template <typename T, int S> __global__ void line_tables_kernel(LineTablesArgs<T
         for (int jj = k; jj < S; ++jj) {
             double re, im;
             propagator_entry<S>(W, U, a.dt_re, a.dt_im, decay, k, jj, re, im);
-            a.R[(size_t)idx * a.n + p] = mk<T>((T)re, (T)im);
+            a.R[(size_t)idx * a.n + p] = mktab<T>(re, im);
             ++idx;
         }
     // kinetic phase exp(-i K dt) at the wavenumber this slot holds after the forward transform
@@ -68,7 +68,7 @@ template <typename T, int S> __global__ void line_tables_kernel(LineTablesArgs<T
         double zim = __dadd_rn(__dmul_rn(0.0, a.dt_im), __dmul_rn(-K, a.dt_re));
         double ore, oim;
         cexp_dev(zre, zim, ore, oim);
-        a.expk[p] = mk<T>((T)ore, (T)oim);
+        a.expk[p] = mktab<T>(ore, oim);
     }
 }
 
@@ -166,6 +166,7 @@ struct zqd_job {
     DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
     float last_ms = 0;
     size_t device_bytes = 0;
+    uint64_t h2d = 0, d2h = 0; // bytes copied by this job
     ~zqd_job() {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -177,33 +178,41 @@ namespace zqd {
 
 template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
 
+// Cluster shape of a 1-D job: C CTAs of m = n/C points each, m/8 threads per
+// CTA (one radix-8 butterfly of every state per thread).  The default is the
+// smallest C whose CTA fits in shared memory and holds at most `target`
+// points; ZQD_LINE_CLUSTER forces C (used by the tuning sweeps).
 static int choose_line_shape(zqd_job* J) {
-    const size_t csz = J->fp32 ? sizeof(float2) : sizeof(double2);
-    const size_t budget = 200 * 1024; // dynamic shared memory per CTA
+    const size_t budget = 205 * 1024; // dynamic shared memory per CTA
     int forced = 0;
     if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
-    for (int C = 1; C <= 16; C <<= 1) {
-        if (forced && C != forced) continue;
-        if (J->n % C) continue;
-        int m = J->n / C;
-        if (m < 4 || m / C < 1 || (C > 1 && m < C)) continue;
-        size_t ld = J->fp32 ? (size_t)padded_len<float>(m) : (size_t)padded_len<double>(m);
-        size_t smem = (C > 1 ? 2 : 1) * (size_t)J->S * ld * csz;
-        if (smem > budget) continue;
-        int elems = J->S * m;
-        int E = J->fp32 ? ElemsOf<float>::E : ElemsOf<double>::E;
-        int threads = (elems + E - 1) / E;
-        if (threads > 512) continue;
-        threads = std::max(32, (threads + 31) / 32 * 32);
-        J->C = C;
-        J->m = m;
-        J->q = m / C;
-        J->E = E;
-        J->threads = threads;
-        J->smem = smem;
-        return ZQD_OK;
+    const int target = J->fp32 ? 4096 : 2048;
+    int fallback = -1;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int C = 1; C <= 16; C <<= 1) {
+            if (forced && C != forced) continue;
+            if (J->n % C) continue;
+            const int m = J->n / C;
+            if (m < 8 || m / C < 1) continue;
+            const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m) : line_smem_bytes<double>(J->S, C, m);
+            if (smem > budget) continue;
+            const int threads = std::max(32, (m / 8 + 31) / 32 * 32);
+            if (threads > (J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value)) continue;
+            if (pass == 0 && !forced && m > target) {
+                if (fallback < 0) fallback = C;
+                continue;
+            }
+            J->C = C;
+            J->m = m;
+            J->q = m / C;
+            J->E = 8 * J->S;
+            J->threads = threads;
+            J->smem = smem;
+            return ZQD_OK;
+        }
+        if (forced) break;
     }
-    return fail(ZQD_ERR_UNSUPPORTED, "1-D GRID TOO LARGE FOR THE RESIDENT CLUSTER KERNEL");
+    return fail(ZQD_ERR_UNSUPPORTED, "1-D GRID DOES NOT FIT THE RESIDENT CLUSTER KERNEL (at most 16 CTAs of 4096 points)");
 }
 
 using LineKernelFn = void (*)(const void*);
@@ -245,11 +254,11 @@ template <typename T, int S> static int run_tables(zqd_job* J) {
         a.cap_exp = J->o.cap_exponent;
     }
     a.pot = J->pot.dev;
-    a.R = J->R.as<cx<T>>();
+    a.R = J->R.as<Tab<T>>();
     a.V = J->V.as<double>();
     a.U = J->U.as<double>();
     a.capw = J->capw.as<double>();
-    a.expk = J->expk.as<cx<T>>();
+    a.expk = J->expk.as<Tab<T>>();
     int threads = 128, blocks = (J->n + threads - 1) / threads;
     line_tables_kernel<T, S><<<blocks, threads, 0, J->stream>>>(a);
     ZQD_CUDA(cudaGetLastError());
@@ -273,12 +282,13 @@ template <typename T> static int create_line(zqd_job* J) {
     const size_t n = J->n, S = J->S, nsym = S * (S + 1) / 2;
     const size_t c = sizeof(cx<T>);
     int rc;
-    if ((rc = J->R.alloc(nsym * n * c))) return rc;
-    if ((rc = J->expk.alloc(n * c))) return rc;
+    const size_t tb = sizeof(Tab<T>);
+    if ((rc = J->R.alloc(nsym * n * tb))) return rc;
+    if ((rc = J->expk.alloc(n * tb))) return rc;
     if ((rc = J->V.alloc(S * S * n * sizeof(double)))) return rc;
     if (S > 1 && (rc = J->U.alloc(S * S * n * sizeof(double)))) return rc;
     if (J->o.has_cap && (rc = J->capw.alloc(n * sizeof(double)))) return rc;
-    if ((rc = J->tw.alloc(n * c))) return rc;
+    if ((rc = J->tw.alloc(n * tb))) return rc;
     if ((rc = J->psi_save.alloc(S * n * c))) return rc;
     bool acf = J->o.has_spectrum || (J->o.write_mask & ZQD_WRITE_ACF);
     if (acf && (rc = J->psi0.alloc(S * n * c))) return rc;
@@ -293,14 +303,11 @@ template <typename T> static int create_line(zqd_job* J) {
                       J->psi_save.bytes + J->psi0.bytes + J->orth.bytes + J->hist.bytes;
     // twiddles
     std::vector<double> tw = twiddles_f64(J->n);
-    if (std::is_same<T, double>::value) {
-        ZQD_CUDA(cudaMemcpyAsync(J->tw.p, tw.data(), n * c, cudaMemcpyHostToDevice, J->stream));
-        ZQD_CUDA(cudaStreamSynchronize(J->stream));
-    } else {
-        std::vector<float> twf(tw.begin(), tw.end());
-        ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twf.data(), n * c, cudaMemcpyHostToDevice, J->stream));
-        ZQD_CUDA(cudaStreamSynchronize(J->stream));
-    }
+    std::vector<Tab<T>> twt(n);
+    for (size_t t = 0; t < n; ++t) twt[t] = mktab<T>(tw[2 * t], tw[2 * t + 1]);
+    ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twt.data(), n * tb, cudaMemcpyHostToDevice, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->h2d += n * tb + J->pot.bytes;
     if ((rc = run_tables_s<T>(J))) return rc;
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     return ZQD_OK;
@@ -344,12 +351,12 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
         L.cap_hi = o.cap_bounds[1];
         L.cap_exp = o.cap_exponent;
     }
-    L.R = J->R.as<cx<T>>();
-    L.expk = J->expk.as<cx<T>>();
+    L.R = J->R.as<Tab<T>>();
+    L.expk = J->expk.as<Tab<T>>();
     L.V = J->V.as<double>();
     L.U = J->U.as<double>();
     L.capw = J->capw.as<double>();
-    L.tw = J->tw.as<cx<T>>();
+    L.tw = J->tw.as<Tab<T>>();
     L.psi_save = J->psi_save.as<cx<T>>();
     L.psi0 = J->psi0.as<cx<T>>();
     L.orth = J->orth.as<cx<T>>();
@@ -367,6 +374,7 @@ template <typename T> static int run_line(zqd_job* J) {
     std::vector<LineJob<T>> descs;
     for (int s = 0; s < J->nsolve; ++s) descs.push_back(line_job_desc<T>(J, s));
     ZQD_CUDA(cudaMemcpyAsync(J->jobs.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, J->stream));
+    J->h2d += descs.size() * sizeof(LineJob<T>);
     ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
     LaunchShape sh{J->S, J->C, J->E, J->threads, J->smem, J->stream};
     for (int s = 0; s < J->nsolve; ++s) {
@@ -396,6 +404,10 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
         ZQD_CUDA(cudaMemcpyAsync(orth.data(), J->orth.p, orth.size() * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
     }
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->d2h += (hist.size() + fin.size()) * sizeof(double) + nrows.size() * sizeof(int) +
+              (save.size() + orth.size()) * sizeof(cx<T>);
+    R->h2d = J->h2d;
+    R->d2h = J->d2h;
     R->ndim = 1;
     R->nstate = J->S;
     R->npoint_total = J->n;
@@ -496,68 +508,133 @@ extern "C" int zqd_run(const zqd_options* opt, zqd_result** out) {
     return rc;
 }
 
-namespace zqd {
-// One launch advances every job of a group: cluster i of the grid runs job i.
-template <typename T> static int run_group(std::vector<zqd_job*>& grp, float* ms) {
-    zqd_job* lead = grp[0];
-    std::vector<LineJob<T>> descs;
-    LaunchShape sh{lead->S, lead->C, lead->E, 0, 0, lead->stream};
-    for (zqd_job* J : grp) {
-        descs.push_back(line_job_desc<T>(J, 0));
-        sh.threads = std::max(sh.threads, J->threads);
-        sh.smem = std::max(sh.smem, J->smem);
+struct zqd_batch {
+    std::vector<std::unique_ptr<zqd_job, void (*)(zqd_job*)>> jobs;
+    struct Group {
+        std::vector<zqd_job*> members;
+        LaunchShape shape{};
+        DevBuf descs; // LineJob array, one per member (solve 0)
+        bool fp32 = false;
+    };
+    std::vector<std::unique_ptr<Group>> groups;
+    std::vector<zqd_job*> solo; // multi-solve (imaginary-time) jobs run on their own
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0;
+    uint32_t launches = 0;
+    ~zqd_batch() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
     }
-    DevBuf d;
-    int rc = d.alloc(descs.size() * sizeof(LineJob<T>));
+};
+
+namespace zqd {
+template <typename T> static int upload_group(zqd_batch* B, zqd_batch::Group* g) {
+    std::vector<LineJob<T>> descs;
+    for (zqd_job* J : g->members) {
+        descs.push_back(line_job_desc<T>(J, 0));
+        g->shape.threads = std::max(g->shape.threads, J->threads);
+        g->shape.smem = std::max(g->shape.smem, J->smem);
+        J->h2d += sizeof(LineJob<T>);
+    }
+    int rc = g->descs.alloc(descs.size() * sizeof(LineJob<T>));
     if (rc) return rc;
-    ZQD_CUDA(cudaMemcpyAsync(d.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, lead->stream));
-    ZQD_CUDA(cudaEventRecord(lead->ev0, lead->stream));
-    if ((rc = launch_line_s<T>(&sh, d.p, (int)grp.size()))) return rc;
-    ZQD_CUDA(cudaEventRecord(lead->ev1, lead->stream));
-    ZQD_CUDA(cudaStreamSynchronize(lead->stream));
-    ZQD_CUDA(cudaEventElapsedTime(ms, lead->ev0, lead->ev1));
-    for (zqd_job* J : grp) J->last_ms = *ms;
+    ZQD_CUDA(cudaMemcpyAsync(g->descs.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, B->stream));
+    ZQD_CUDA(cudaStreamSynchronize(B->stream));
     return ZQD_OK;
 }
 } // namespace zqd
 
-extern "C" int zqd_run_batch(const zqd_options* const* opts, uint32_t njobs, zqd_result** results) {
-    if (!opts || !results) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
-    for (uint32_t i = 0; i < njobs; ++i) results[i] = nullptr;
-    std::vector<std::unique_ptr<zqd_job, void (*)(zqd_job*)>> jobs;
+extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, zqd_batch** out) {
+    if (!opts || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    *out = nullptr;
+    std::unique_ptr<zqd_batch> B(new (std::nothrow) zqd_batch());
+    if (!B) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
     for (uint32_t i = 0; i < njobs; ++i) {
         zqd_job* J = nullptr;
         int rc = zqd_job_create(opts[i], &J);
         if (rc) return rc;
-        jobs.emplace_back(J, zqd_job_destroy);
+        B->jobs.emplace_back(J, zqd_job_destroy);
     }
-    // group single-solve jobs by kernel instantiation; multi-solve (ITP) jobs run alone
+    ZQD_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+    ZQD_CUDA(cudaEventCreate(&B->ev0));
+    ZQD_CUDA(cudaEventCreate(&B->ev1));
+    // group single-solve jobs by kernel instantiation (precision, states, cluster size)
     std::vector<bool> done(njobs, false);
     for (uint32_t i = 0; i < njobs; ++i) {
         if (done[i]) continue;
-        zqd_job* a = jobs[i].get();
+        zqd_job* a = B->jobs[i].get();
+        done[i] = true;
         if (a->nsolve > 1) {
-            int rc = zqd_job_run(a);
-            if (rc) return rc;
-            done[i] = true;
+            B->solo.push_back(a);
             continue;
         }
-        std::vector<zqd_job*> grp{a};
-        done[i] = true;
+        std::unique_ptr<zqd_batch::Group> g(new zqd_batch::Group());
+        g->members.push_back(a);
+        g->fp32 = a->fp32;
+        g->shape = LaunchShape{a->S, a->C, a->E, 0, 0, B->stream};
         for (uint32_t k = i + 1; k < njobs; ++k) {
-            zqd_job* b = jobs[k].get();
-            if (!done[k] && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C && b->E == a->E) {
-                grp.push_back(b);
+            zqd_job* b = B->jobs[k].get();
+            if (!done[k] && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C) {
+                g->members.push_back(b);
                 done[k] = true;
             }
         }
-        float ms = 0;
-        int rc = a->fp32 ? run_group<float>(grp, &ms) : run_group<double>(grp, &ms);
+        int rc = g->fp32 ? upload_group<float>(B.get(), g.get()) : upload_group<double>(B.get(), g.get());
         if (rc) return rc;
+        B->groups.push_back(std::move(g));
     }
+    *out = B.release();
+    return ZQD_OK;
+}
+
+extern "C" int zqd_batch_run(zqd_batch* B) {
+    if (!B) return fail(ZQD_ERR_INVALID_INPUT, "NULL BATCH");
+    B->launches = 0;
+    ZQD_CUDA(cudaEventRecord(B->ev0, B->stream));
+    for (auto& g : B->groups) {
+        int rc = g->fp32 ? launch_line_s<float>(&g->shape, g->descs.p, (int)g->members.size())
+                         : launch_line_s<double>(&g->shape, g->descs.p, (int)g->members.size());
+        if (rc) return rc;
+        ++B->launches;
+    }
+    ZQD_CUDA(cudaEventRecord(B->ev1, B->stream));
+    for (zqd_job* J : B->solo) { // runs on its own stream, overlapping the grouped launches
+        int rc = zqd_job_run(J);
+        if (rc) return rc;
+        B->launches += (uint32_t)J->nsolve;
+    }
+    ZQD_CUDA(cudaStreamSynchronize(B->stream));
+    float ms = 0;
+    ZQD_CUDA(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+    for (zqd_job* J : B->solo) ms = std::max(ms, J->last_ms);
+    B->last_ms = ms;
+    for (auto& g : B->groups)
+        for (zqd_job* J : g->members) J->last_ms = ms;
+    return ZQD_OK;
+}
+
+extern "C" int zqd_batch_result(zqd_batch* B, uint32_t i, zqd_result** out) {
+    if (!B || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    if (i >= B->jobs.size()) return fail(ZQD_ERR_NOT_FOUND, "JOB INDEX OUT OF RANGE");
+    return zqd_job_result(B->jobs[i].get(), out);
+}
+
+extern "C" double zqd_batch_device_ms(const zqd_batch* B) { return B ? (double)B->last_ms : 0.0; }
+extern "C" uint32_t zqd_batch_launches(const zqd_batch* B) { return B ? B->launches : 0; }
+extern "C" void zqd_batch_destroy(zqd_batch* B) { delete B; }
+
+extern "C" int zqd_run_batch(const zqd_options* const* opts, uint32_t njobs, zqd_result** results) {
+    if (!opts || !results) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    for (uint32_t i = 0; i < njobs; ++i) results[i] = nullptr;
+    zqd_batch* B = nullptr;
+    int rc = zqd_batch_create(opts, njobs, &B);
+    if (rc) return rc;
+    std::unique_ptr<zqd_batch, void (*)(zqd_batch*)> guard(B, zqd_batch_destroy);
+    if ((rc = zqd_batch_run(B))) return rc;
     for (uint32_t i = 0; i < njobs; ++i) {
-        int rc = zqd_job_result(jobs[i].get(), &results[i]);
-        if (rc) {
+        if ((rc = zqd_batch_result(B, i, &results[i]))) {
             for (uint32_t k = 0; k < i; ++k) {
                 zqd_result_destroy(results[k]);
                 results[k] = nullptr;

@@ -5,7 +5,7 @@
 #include <mutex>
 
 #include "internal.h"
-#include "line_kernel.cuh"
+#include "line_solve.cuh"
 
 #if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_LAUNCH)
 #error "line_inst.cu needs -DZQD_T, -DZQD_S and -DZQD_LAUNCH"
@@ -18,7 +18,7 @@ template <int C> static int launch_one(const LaunchShape* J, const void* d_jobs,
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024);
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 215 * 1024);
         if (attr_err == cudaSuccess && C > 8)
             attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     });

@@ -1,0 +1,685 @@
+// line_solve.cuh -- the fused resident 1-D solve (src/quantum_dynamics.zig:860-950).
+//
+// Shared memory of a CTA holds two wavefunction buffers (the Stockham passes
+// ping-pong between them, one barrier per pass), the twiddles exp(-2 pi i t/m),
+// the cluster twiddles exp(-2 pi i c k1/n), the potential propagator R at the
+// CTA's grid points and the kinetic phase at its wavenumbers.  One time step
+// (Propagator.step, :417-427) is
+//   forward FFT   first pass: [accumAbsorbed], psi <- R psi, butterflies
+//                 last pass : butterflies, cluster twiddle (C > 1) or kinetic phase (C = 1)
+//   exchange      C-point DFTs across the cluster with the kinetic phase between them (C > 1)
+//   inverse FFT   first pass: remote gather of the exchanged values (C > 1), butterflies
+//                 last pass : butterflies, 1/N, [accumAbsorbed], psi <- R psi, observables
+// followed by one cluster reduction of every observable of the step.
+#pragma once
+
+#include "line_kernel.cuh"
+
+namespace zqd {
+
+// dynamic shared memory of one CTA
+template <typename T> __host__ __device__ inline size_t line_smem_bytes(int S, int C, int m) {
+    const size_t ld = (size_t)padded_len<T>(m), nsym = (size_t)S * (S + 1) / 2;
+    return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 2 : 1) + nsym + 1) * (size_t)m * sizeof(Tab<T>);
+}
+
+// reduction slots of a step
+enum : int { A_NORM = 0, A_POS, A_EPOT, A_ACFR, A_ACFI, A_MOM, A_EKIN, A_POP };
+template <int S> struct NAcc { static constexpr int value = A_POP + 2 * S; }; // pop[S] then absorbed[S]
+
+struct ObsFlags {
+    bool norm, pos, epot, acf, pop, mom, ekin, adia, track;
+};
+
+template <typename T> __device__ __forceinline__ const cx<T>* remote(const cx<T>* p, int rank) {
+    return cg::this_cluster().map_shared_rank(p, rank);
+}
+
+template <int C> __device__ __forceinline__ double grid_r(double lo, double span, int n, int cta, int j) {
+    // grid coordinate of local point j: min + x (max - min) / n (Grid.init, wavepacket.zig:66)
+    return __dadd_rn(lo, __dmul_rn((double)(cta + C * j), span) / (double)n);
+}
+
+template <typename T> __device__ __forceinline__ double capdecay(const LineJob<T>& J, double r) {
+    // quantum_dynamics.zig:434-449
+    double cap_sum = 0;
+    if (J.has_cap) {
+        double dist = fmax(0.0, fmax(J.cap_lo - r, r - J.cap_hi));
+        if (dist > 0) cap_sum = __dadd_rn(cap_sum, exp(__dmul_rn(J.cap_exp, dist)) - 1);
+    }
+    return exp(__dmul_rn(__dmul_rn(-0.5, cap_sum), hypot(J.dt_re, J.dt_im)));
+}
+
+// psi_i <- sum_k R_ik psi_k at one point (applyR, quantum_dynamics.zig:515-534)
+template <typename T, int S>
+__device__ __forceinline__ void apply_r_point(cx<T>* x, const Tab<T>* __restrict__ Rs, int m, int j) {
+    constexpr int NSYM = S * (S + 1) / 2;
+    Tab<T> r[NSYM];
+#pragma unroll
+    for (int c = 0; c < NSYM; ++c) r[c] = Rs[c * m + j];
+    cx<T> y[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        cx<T> acc = mk<T>(0, 0);
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            const int a = i < k ? i : k, b = i < k ? k : i;
+            acc = add<T>(acc, tmul<-1>(x[k], r[a * S - a * (a - 1) / 2 + (b - a)]));
+        }
+        y[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < S; ++i) x[i] = y[i];
+}
+
+// cap_weight-weighted populations at one point (accumAbsorbed, quantum_dynamics.zig:471-499)
+template <typename T, int S>
+__device__ __forceinline__ void absorbed_point(Acc* acc, const cx<T>* x, double w, const double* __restrict__ U, int n,
+                                               int j, bool adia) {
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        if (adia && S > 1) {
+            double are = 0, aim = 0;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const double u = U[(size_t)(k * S + i) * n + j];
+                are += (double)x[k].x * u;
+                aim += (double)x[k].y * u;
+            }
+            acc[A_POP + S + i].add(w * (are * are + aim * aim));
+        } else {
+            acc[A_POP + S + i].add(w * ((double)x[i].x * (double)x[i].x + (double)x[i].y * (double)x[i].y));
+        }
+    }
+}
+
+// position-space observables of one point (wavepacket.zig:235-352, Observables.init :321-345)
+template <typename T, int S>
+__device__ __forceinline__ void observe_point(Acc* acc, const cx<T>* x, double r, const LineJob<T>& J, size_t gidx,
+                                              const ObsFlags& f) {
+    double m2 = 0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const double w = (double)x[s].x * (double)x[s].x + (double)x[s].y * (double)x[s].y;
+        m2 += w;
+        if (f.pop && !(f.adia && S > 1)) acc[A_POP + s].add(w);
+    }
+    if (f.norm) acc[A_NORM].add(m2);
+    if (f.pos) acc[A_POS].add(m2 * r);
+    if (f.epot) {
+        double e = 0;
+#pragma unroll
+        for (int i = 0; i < S; ++i)
+#pragma unroll
+            for (int k = 0; k < S; ++k)
+                e += ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) *
+                     J.V[(size_t)(i * S + k) * J.n + gidx];
+        acc[A_EPOT].add(e);
+    }
+    if (f.acf) {
+        double re = 0, im = 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const cx<T> z0 = J.psi0[(size_t)s * J.n + gidx];
+            re += (double)z0.x * (double)x[s].x + (double)z0.y * (double)x[s].y;
+            im += (double)z0.x * (double)x[s].y - (double)z0.y * (double)x[s].x;
+        }
+        acc[A_ACFR].add(re);
+        acc[A_ACFI].add(im);
+    }
+    if (f.pop && f.adia && S > 1) {
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            double are = 0, aim = 0;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const double u = J.U[(size_t)(k * S + i) * J.n + gidx];
+                are += (double)x[k].x * u;
+                aim += (double)x[k].y * u;
+            }
+            acc[A_POP + i].add(are * are + aim * aim);
+        }
+    }
+}
+
+// momentum-space observables of one wavenumber slot (wavepacket.zig:224-232, 258-268)
+template <typename T, int S>
+__device__ __forceinline__ void observe_k(Acc* acc, const cx<T>* z, int kidx, int n, double dkunit, double mass,
+                                          const ObsFlags& f) {
+    double w = 0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) w += (double)z[s].x * (double)z[s].x + (double)z[s].y * (double)z[s].y;
+    const double nn = (double)kidx;
+    const double kv = __dmul_rn(kidx < n / 2 ? nn : __dsub_rn(nn, (double)n), dkunit); // wavepacket.zig:68-70
+    if (f.mom) acc[A_MOM].add(w * kv);
+    if (f.ekin) acc[A_EKIN].add(w * (0.5 * kv * kv / mass));
+}
+
+// ------------------------------------------------------------ rare phases
+// (initial state, imaginary time, time-dependent updates): out of line
+template <typename T> struct LineCtx {
+    const LineJob<T>* J;
+    cx<T>* psi; // current wavefunction buffer
+    cx<T>* spare;
+    RedSmem* rs;
+    int m, n, logm, q, ldp, cta;
+    size_t base;
+};
+
+// psi <- psi / sqrt(norm) as std.math.Complex.div by (s, 0) (wavepacket.zig:282-284)
+template <typename T, int S, int C> __device__ __noinline__ void line_normalize(const LineCtx<T>& X) {
+    const int m = X.m, ldp = X.ldp;
+    cx<T>* __restrict__ psi = X.psi;
+    Acc a[1];
+    for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+        const int s = e / m, j = e - s * m;
+        const cx<T> z = psi[s * ldp + padx<T>(j)];
+        a[0].add((double)z.x * (double)z.x + (double)z.y * (double)z.y);
+    }
+    double o[1];
+    cluster_sum<1, C>(a, o, X.rs);
+    const double sq = sqrt(o[0] * X.J->dr), den = sq * sq;
+    for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+        const int s = e / m, j = e - s * m;
+        cx<T>& z = psi[s * ldp + padx<T>(j)];
+        z = mk<T>((T)((double)z.x * sq / den), (T)((double)z.y * sq / den));
+    }
+    __syncthreads();
+}
+
+// imaginary-time Gram-Schmidt against the relaxed states (quantum_dynamics.zig:898-904)
+template <typename T, int S, int C> __device__ __noinline__ void line_orthogonalize(const LineCtx<T>& X) {
+    const int m = X.m, ldp = X.ldp, n = X.n, northo = X.J->northo;
+    cx<T>* __restrict__ psi = X.psi;
+    const double dr = X.J->dr;
+    for (int o = 0; o < northo; ++o) {
+        const cx<T>* __restrict__ ph = X.J->orth + (size_t)o * S * n + X.base;
+        Acc a[2];
+        for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+            const int s = e / m, j = e - s * m;
+            const cx<T> p = ph[(size_t)s * n + j], z = psi[s * ldp + padx<T>(j)];
+            a[0].add((double)p.x * (double)z.x + (double)p.y * (double)z.y);
+            a[1].add((double)p.x * (double)z.y - (double)p.y * (double)z.x);
+        }
+        double ov[2];
+        cluster_sum<2, C>(a, ov, X.rs);
+        const double ore = ov[0] * dr, oim = ov[1] * dr;
+        for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+            const int s = e / m, j = e - s * m;
+            const cx<T> p = ph[(size_t)s * n + j];
+            cx<T>& z = psi[s * ldp + padx<T>(j)];
+            const double re = (double)z.x - (ore * (double)p.x - oim * (double)p.y);
+            const double im = (double)z.y - (ore * (double)p.y + oim * (double)p.x);
+            z = mk<T>((T)re, (T)im);
+        }
+        __syncthreads();
+    }
+}
+
+// time-dependent Hamiltonian.update (wavepacket.zig:137-143) and, with_R,
+// Propagator.update into the shared-memory R table
+template <typename T, int S, int C>
+__device__ __noinline__ void line_ham_update(const LineCtx<T>& X, double t, bool with_R, Tab<T>* Rs, double lo,
+                                             double span) {
+    const LineJob<T>& J = *X.J;
+    for (int j = threadIdx.x; j < X.m; j += blockDim.x) {
+        const double r = grid_r<C>(lo, span, X.n, X.cta, j);
+        td_point_update<T, S>(J.pot, r, t, with_R, J.dt_re, J.dt_im, with_R ? capdecay(J, r) : 1.0, J.V, J.U,
+                              (size_t)X.n, X.base + j, Rs, (size_t)X.m, (size_t)j);
+    }
+    __syncthreads();
+}
+
+// setGaussian (wavepacket.zig:355-371), toDia (:398-419), autocorrelation reference
+template <typename T, int S, int C>
+__device__ __noinline__ void line_initial_state(const LineCtx<T>& X, double lo, double span) {
+    const LineJob<T>& J = *X.J;
+    const int m = X.m, ldp = X.ldp, n = X.n;
+    cx<T>* __restrict__ psi = X.psi;
+    for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+        const int s = e / m, j = e - s * m;
+        cx<T> z = mk<T>(0, 0);
+        if (s == J.ic_state) {
+            const double dx = __dsub_rn(grid_r<C>(lo, span, n, X.cta, j), J.x0);
+            const double ere = __dmul_rn(__dmul_rn(__dmul_rn(-0.5, J.gamma), dx), dx);
+            const double eim = __dmul_rn(J.p0, dx);
+            double zr, zi;
+            cexp_dev(ere, eim, zr, zi);
+            z = mk<T>((T)zr, (T)zi);
+        }
+        psi[s * ldp + padx<T>(j)] = z;
+    }
+    __syncthreads();
+    line_normalize<T, S, C>(X);
+    if (J.ic_adia && S > 1) {
+        const double* __restrict__ U = J.U + X.base;
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = psi[s * ldp + padx<T>(j)];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                double re = 0, im = 0;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const double u = U[(size_t)(i * S + k) * n + j];
+                    re += (double)x[k].x * u;
+                    im += (double)x[k].y * u;
+                }
+                psi[i * ldp + padx<T>(j)] = mk<T>((T)re, (T)im);
+            }
+        }
+        __syncthreads();
+    }
+    if (J.calc_acf) {
+        cx<T>* __restrict__ psi0 = J.psi0 + X.base;
+        for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+            const int s = e / m, j = e - s * m;
+            psi0[(size_t)s * n + j] = psi[s * ldp + padx<T>(j)];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ the kernel
+// threads per CTA: m/8; FP64 CTAs are capped at 256 threads (m <= 2048) so a
+// thread may use up to 255 registers for the S x 8 complex values of a butterfly
+template <typename T> struct LineMaxThreads { static constexpr int value = 512; };
+template <> struct LineMaxThreads<double> { static constexpr int value = 256; };
+
+enum PassKind : int { FWD_FIRST = 1, FWD_LAST = 2, INV_FIRST = 4, INV_LAST = 8 };
+
+// All state of one CTA's solve.  Every member function is force-inlined into
+// the kernel, so the members stay in registers (no closure objects, no stack).
+template <typename T, int S, int C> struct LineSolver {
+    static constexpr int NSYM = S * (S + 1) / 2;
+    static constexpr int NV = NAcc<S>::value;
+
+    const LineJob<T>* J; // shared-memory copy of the job
+    RedSmem* rs;
+    cx<T>* bufA;
+    cx<T>* bufB;
+    cx<T>* cur; // holds psi between steps
+    const Tab<T>* twm;
+    const Tab<T>* twc;
+    const Tab<T>* Rs;
+    const Tab<T>* eks;
+    const double* capw; // this CTA's slice of the global tables
+    const double* Ug;
+    const double* Vg;
+    const cx<T>* psi0;
+    int m, n, logm, q, ldp, cta;
+    size_t base;
+    double lo, span, dr, dk, dkunit, mass;
+    T inv_n;
+    bool prop;     // propagation step (true) or momentum-observation round trip (false)
+    bool fuse_obs; // accumulate the position-space observables in the last inverse pass
+    ObsFlags f;
+    Acc acc[NV];
+    double pop_abs[S];
+
+    // ---------------------------------------------------------------- hooks
+    // forward, first pass: accumAbsorbed before the first applyR, then R
+    template <int R> __device__ __forceinline__ void fwd_first(int i, int mr, cx<T> (&v)[S][R]) {
+        if (!prop) return;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = i + r * mr;
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = v[s][r];
+            if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
+            apply_r_point<T, S>(x, Rs, m, j);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][r] = x[s];
+        }
+    }
+    // forward, last pass: cluster twiddle (C > 1) or, for C = 1, kinetic phase / k-space observables
+    template <int R> __device__ __forceinline__ void fwd_last(int o0, int p, cx<T> (&v)[S][R]) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int k = o0 + r * p;
+            if constexpr (C > 1) {
+                if (cta > 0) {
+                    const Tab<T> w = twc[k];
+#pragma unroll
+                    for (int s = 0; s < S; ++s) v[s][r] = tmul<-1>(v[s][r], w);
+                }
+            } else if (prop) {
+                const Tab<T> w = eks[k];
+#pragma unroll
+                for (int s = 0; s < S; ++s) v[s][r] = tmul<-1>(v[s][r], w);
+            } else {
+                cx<T> z[S];
+#pragma unroll
+                for (int s = 0; s < S; ++s) z[s] = v[s][r];
+                observe_k<T, S>(acc, z, k, n, dkunit, mass, f);
+            }
+        }
+    }
+    // inverse, first pass (C > 1): gather the exchanged values from their owners
+    template <int R> __device__ __forceinline__ void inv_first(int i, int mr, cx<T> (&v)[S][R], const cx<T>* xbuf) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int k1 = i + r * mr, owner = k1 / q, u = k1 - owner * q;
+            const cx<T>* src = remote<T>(xbuf, owner);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][r] = src[s * ldp + padx<T>(cta * q + u)];
+            if (cta > 0) {
+                const Tab<T> w = twc[k1];
+#pragma unroll
+                for (int s = 0; s < S; ++s) v[s][r] = tmul<1>(v[s][r], w);
+            }
+        }
+    }
+    // inverse, last pass: 1/N, accumAbsorbed, R and the observables of the step
+    template <int R> __device__ __forceinline__ void inv_last(int o0, int p, cx<T> (&v)[S][R]) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = o0 + r * p;
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = scale<T>(v[s][r], inv_n);
+            if (prop) {
+                if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
+                apply_r_point<T, S>(x, Rs, m, j);
+                if (fuse_obs) observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f);
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][r] = x[s];
+        }
+    }
+
+    // One radix-R Stockham pass over S lines of m points, `in` -> `out`.  Thread t
+    // handles the butterflies i = t, t + nt, ... of every state, so all S states of
+    // a grid point meet in one thread.  KIND selects the hooks of first/last passes.
+    template <int R, int SIGN, int KIND>
+    __device__ __forceinline__ void pass(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int p, int logp,
+                                         const cx<T>* xbuf) {
+        constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
+        const int logmr = logm - LR, mr = 1 << logmr, nt = blockDim.x;
+        const int tshift = logm - logp - LR;
+        for (int i = threadIdx.x; i < mr; i += nt) {
+            cx<T> v[S][R];
+            if constexpr ((KIND & INV_FIRST) && C > 1) {
+                inv_first<R>(i, mr, v, xbuf);
+            } else {
+#pragma unroll
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[s][r] = in[s * ldp + padx<T>(i + r * mr)];
+            }
+            if constexpr (KIND & FWD_FIRST) fwd_first<R>(i, mr, v);
+            const int kk = i & (p - 1);
+            if (p > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const Tab<T> w = twm[(r * kk) << tshift];
+#pragma unroll
+                    for (int s = 0; s < S; ++s) v[s][r] = tmul<SIGN>(v[s][r], w);
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) dft<R, SIGN, T>(v[s]);
+            const int o0 = ((i - kk) << LR) + kk;
+            if constexpr (KIND & FWD_LAST) fwd_last<R>(o0, p, v);
+            if constexpr (KIND & INV_LAST) inv_last<R>(o0, p, v);
+#pragma unroll
+            for (int s = 0; s < S; ++s)
+#pragma unroll
+                for (int r = 0; r < R; ++r) out[s * ldp + padx<T>(o0 + r * p)] = v[s][r];
+        }
+        __syncthreads();
+    }
+
+    // local m-point transform ping-ponging between a (input) and b; returns the result buffer
+    template <int SIGN> __device__ __forceinline__ cx<T>* local_fft(cx<T>* a, cx<T>* b, const cx<T>* xbuf) {
+        constexpr int KF = SIGN < 0 ? FWD_FIRST : INV_FIRST, KL = SIGN < 0 ? FWD_LAST : INV_LAST;
+        int p = 1, logp = 0, rem = logm;
+        bool first = true;
+        cx<T>* in = a;
+        cx<T>* out = b;
+        while (rem > 0) {
+            const int LR = rem >= 3 ? 3 : rem;
+            const bool last = rem == LR;
+            if (LR == 3) {
+                if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
+                else if (first) pass<8, SIGN, KF>(in, out, p, logp, xbuf);
+                else if (last) pass<8, SIGN, KL>(in, out, p, logp, xbuf);
+                else pass<8, SIGN, 0>(in, out, p, logp, xbuf);
+            } else if (LR == 2) {
+                if (first) pass<4, SIGN, KF | KL>(in, out, p, logp, xbuf);
+                else pass<4, SIGN, KL>(in, out, p, logp, xbuf);
+            } else {
+                if (first) pass<2, SIGN, KF | KL>(in, out, p, logp, xbuf);
+                else pass<2, SIGN, KL>(in, out, p, logp, xbuf);
+            }
+            // the inverse's first pass read other CTAs' exchange buffers: none may be
+            // overwritten before every CTA of the cluster has finished that gather
+            if (C > 1 && SIGN > 0 && first) cg::this_cluster().sync();
+            cx<T>* t = in;
+            in = out;
+            out = t;
+            p <<= LR;
+            logp += LR;
+            rem -= LR;
+            first = false;
+        }
+        return in;
+    }
+
+    __device__ __forceinline__ cx<T>* other(const cx<T>* b) const { return b == bufA ? bufB : bufA; }
+
+    // forward transform of cur; returns the buffer the inverse starts from
+    __device__ __forceinline__ cx<T>* forward() {
+        cx<T>* res = local_fft<-1>(cur, other(cur), nullptr);
+        if constexpr (C > 1) { // C-point DFTs across the cluster, kinetic phase in between
+            cx<T>* xb = other(res);
+            cg::cluster_group cl = cg::this_cluster();
+            cl.sync();
+            for (int u = threadIdx.x; u < q; u += blockDim.x) {
+                cx<T> w[S][C];
+#pragma unroll
+                for (int cc = 0; cc < C; ++cc) {
+                    const cx<T>* src = remote<T>(res, cc);
+#pragma unroll
+                    for (int s = 0; s < S; ++s) w[s][cc] = src[s * ldp + padx<T>(cta * q + u)];
+                }
+#pragma unroll
+                for (int s = 0; s < S; ++s) dft<C, -1, T>(w[s]);
+#pragma unroll
+                for (int k2 = 0; k2 < C; ++k2) {
+                    if (prop) {
+                        const Tab<T> ph = eks[k2 * q + u];
+#pragma unroll
+                        for (int s = 0; s < S; ++s) w[s][k2] = tmul<-1>(w[s][k2], ph);
+                    } else {
+                        cx<T> z[S];
+#pragma unroll
+                        for (int s = 0; s < S; ++s) z[s] = w[s][k2];
+                        observe_k<T, S>(acc, z, cta * q + u + m * k2, n, dkunit, mass, f);
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < S; ++s) dft<C, 1, T>(w[s]);
+#pragma unroll
+                for (int cc = 0; cc < C; ++cc)
+#pragma unroll
+                    for (int s = 0; s < S; ++s) xb[s * ldp + padx<T>(cc * q + u)] = w[s][cc];
+            }
+            cl.sync();
+            return xb;
+        }
+        return res;
+    }
+    // inverse transform (from forward's buffer) into cur
+    __device__ __forceinline__ void inverse(cx<T>* kb) {
+        if constexpr (C > 1) cur = local_fft<1>(kb, other(kb), kb); // first pass gathers remote kb, writes the other buffer
+        else cur = local_fft<1>(kb, other(kb), nullptr);
+    }
+
+    __device__ __forceinline__ void zero_acc() {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = Acc();
+    }
+    // position-space observables of cur in a pass of their own
+    __device__ __forceinline__ void observe_x() {
+        for (int j = threadIdx.x; j < m; j += blockDim.x) {
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = cur[s * ldp + padx<T>(j)];
+            observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f);
+        }
+    }
+    // momentum-space round trip (quantum_dynamics.zig:347-363): psi <- IFFT(FFT(psi)) as in the reference
+    __device__ __forceinline__ void roundtrip() {
+        prop = false;
+        inverse(forward());
+        prop = true;
+    }
+    __device__ __forceinline__ void set_flags(uint32_t mask) {
+        f.pos = mask & WM_POS;
+        f.mom = mask & WM_MOM;
+        f.pop = mask & WM_POP;
+        f.ekin = (mask & WM_EKIN) || (mask & WM_ETOT);
+        f.epot = (mask & WM_EPOT) || (mask & WM_ETOT);
+        f.norm = (mask & WM_NORM) || J->has_stop;
+        f.acf = J->calc_acf != 0;
+        f.adia = J->adiabatic != 0;
+        f.track = J->track != 0;
+    }
+    // reduce the step's accumulators; the row is written by one thread of the cluster
+    __device__ __forceinline__ double finish_row(double* dst) {
+        double out[NV];
+        cluster_sum<NV, C>(acc, out, rs);
+#pragma unroll
+        for (int s = 0; s < S; ++s) pop_abs[s] += out[A_POP + S + s] * dr;
+        const double norm = out[A_NORM] * dr;
+        if (cta == 0 && threadIdx.x == 0) {
+            constexpr RowLayout L{1, S};
+            dst[L.norm()] = f.norm ? norm : nan("");
+            dst[L.pos()] = f.pos ? out[A_POS] * dr : nan("");
+            dst[L.epot()] = f.epot ? out[A_EPOT] * dr : nan("");
+            dst[L.acf()] = f.acf ? out[A_ACFR] * dr : nan("");
+            dst[L.acf() + 1] = f.acf ? out[A_ACFI] * dr : nan("");
+            dst[L.mom()] = f.mom ? out[A_MOM] * dk : nan("");
+            dst[L.ekin()] = f.ekin ? out[A_EKIN] * dk : nan("");
+#pragma unroll
+            for (int s = 0; s < S; ++s) dst[L.pop() + s] = f.pop ? out[A_POP + s] * dr + pop_abs[s] : nan("");
+        }
+        return norm;
+    }
+};
+
+template <typename T, int S, int C>
+__global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel(const LineJob<T>* __restrict__ jobs) {
+    using Solver = LineSolver<T, S, C>;
+    constexpr int NSYM = Solver::NSYM;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ LineJob<T> J;
+    __shared__ RedSmem rs;
+
+    const int cta = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    if (threadIdx.x == 0) {
+        J = jobs[blockIdx.x / C];
+        rs.slot_idx = 0;
+    }
+    __syncthreads();
+
+    Solver X;
+    X.J = &J;
+    X.rs = &rs;
+    X.m = J.m;
+    X.n = J.n;
+    X.logm = J.logm;
+    X.q = J.q;
+    X.ldp = padded_len<T>(J.m);
+    X.cta = cta;
+    X.base = (size_t)cta * J.m;
+    X.lo = J.lo;
+    X.span = J.hi - J.lo;
+    X.dr = J.dr;
+    X.dk = J.dk;
+    X.dkunit = 6.283185307179586476925286766559 / X.span;
+    X.mass = J.mass;
+    X.inv_n = (T)(1.0 / (double)J.n);
+    X.bufA = reinterpret_cast<cx<T>*>(smem_raw);
+    X.bufB = X.bufA + S * X.ldp;
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(X.bufB + S * X.ldp);
+    Tab<T>* twc = twm + X.m;
+    Tab<T>* Rs = twc + (C > 1 ? X.m : 0);
+    Tab<T>* eks = Rs + NSYM * X.m;
+    X.twm = twm;
+    X.twc = twc;
+    X.Rs = Rs;
+    X.eks = eks;
+    X.capw = J.capw ? J.capw + X.base : nullptr;
+    X.Ug = J.U ? J.U + X.base : nullptr;
+    X.Vg = J.V + X.base;
+    X.psi0 = J.psi0 ? J.psi0 + X.base : nullptr;
+    X.cur = X.bufA;
+    X.prop = true;
+    X.fuse_obs = false;
+#pragma unroll
+    for (int s = 0; s < S; ++s) X.pop_abs[s] = 0;
+
+    // stage the time-independent tables
+    const int m = X.m, n = X.n;
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+        twm[t] = J.tw[t * C]; // exp(-2 pi i t/m)
+        if (C > 1) twc[t] = J.tw[cta * t];
+        eks[t] = J.expk[X.base + t];
+    }
+    for (int e = threadIdx.x; e < NSYM * m; e += blockDim.x) {
+        const int c = e / m, j = e - c * m;
+        Rs[e] = J.R[(size_t)c * n + X.base + j];
+    }
+    __syncthreads();
+
+    LineCtx<T> ctx{&J, X.cur, nullptr, &rs, m, n, X.logm, X.q, X.ldp, cta, X.base};
+    line_initial_state<T, S, C>(ctx, X.lo, X.span);
+    constexpr int HC = RowLayout{1, S}.width();
+    const int iters = J.iters;
+    int rows = iters + 1;
+    for (int i = 0; i <= iters; ++i) {
+        const bool logstep = J.log && ((i % J.log_interval == 0) || (i == iters));
+        X.set_flags(J.wmask | (logstep ? (uint32_t)WM_ALL_OBS : 0u));
+        X.zero_acc();
+        X.fuse_obs = i > 0 && !J.itp && !J.td;
+        if (i > 0) { // Propagator.step (quantum_dynamics.zig:417-427)
+            if (J.td) line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.lo, X.span);
+            X.prop = true;
+            X.inverse(X.forward());
+            ctx.psi = X.cur;
+        }
+        if (J.itp) { // quantum_dynamics.zig:898-906
+            line_orthogonalize<T, S, C>(ctx);
+            line_normalize<T, S, C>(ctx);
+        }
+        if (J.td) line_ham_update<T, S, C>(ctx, (double)i * J.tstep, false, Rs, X.lo, X.span);
+        if (!X.fuse_obs) X.observe_x();
+        if (X.f.mom || X.f.ekin) {
+            X.roundtrip();
+            ctx.psi = X.cur;
+        }
+        const double nrm = X.finish_row(J.hist + (size_t)i * HC);
+        if (J.has_stop && nrm < J.stop_norm) { // stop_norm (quantum_dynamics.zig:933-944)
+            rows = i + 1;
+            break;
+        }
+    }
+    // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
+    X.set_flags(WM_ALL_OBS);
+    X.zero_acc();
+    X.observe_x();
+    X.roundtrip();
+    X.finish_row(J.fin);
+    if (cta == 0 && threadIdx.x == 0) *J.rows = rows;
+    for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+        const int s = e / m, j = e - s * m;
+        J.psi_save[(size_t)s * n + X.base + j] = X.cur[s * X.ldp + padx<T>(j)];
+    }
+    if constexpr (C > 1) cg::this_cluster().sync(); // keep shared memory alive for remote readers
+}
+
+} // namespace zqd

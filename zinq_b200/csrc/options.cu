@@ -218,6 +218,7 @@ int build_potential(const Opts& o, PotStore& ps) {
         ZQD_CUDA(cudaMemcpy(ps.d_consts, consts.data(), consts.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.code = ps.d_code;
         P.consts = ps.d_consts;
+        ps.bytes += code.size() * sizeof(uint32_t) + consts.size() * sizeof(double);
         break;
     }
     case ZQD_POT_LVC: {
@@ -229,6 +230,7 @@ int build_potential(const Opts& o, PotStore& ps) {
         ZQD_CUDA(cudaMalloc(&ps.d_lvc, packed.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(ps.d_lvc, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.lvc = ps.d_lvc;
+        ps.bytes += packed.size() * sizeof(double);
         P.lvc_nm = (int)o.lvc_freq.size();
         break;
     }
@@ -236,6 +238,7 @@ int build_potential(const Opts& o, PotStore& ps) {
         ZQD_CUDA(cudaMalloc(&ps.d_file, o.file_table.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(ps.d_file, o.file_table.data(), o.file_table.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.file = ps.d_file;
+        ps.bytes += o.file_table.size() * sizeof(double);
         P.file_nrow = (int)o.file_nrow;
         P.file_ncol = (int)o.file_ncol;
         P.file_size = (int)std::llround(std::pow((double)o.file_nrow, 1.0 / (double)o.file_nd));

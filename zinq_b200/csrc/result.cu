@@ -93,6 +93,13 @@ extern "C" int zqd_result_spectrum(const zqd_result* r, uint32_t s, const double
 }
 
 extern "C" double zqd_result_device_ms(const zqd_result* r) { return r ? r->device_ms : 0.0; }
+
+extern "C" int zqd_result_transfer_bytes(const zqd_result* r, uint64_t* h2d, uint64_t* d2h) {
+    if (!r) return fail(ZQD_ERR_INVALID_INPUT, "NULL RESULT");
+    if (h2d) *h2d = r->h2d;
+    if (d2h) *d2h = r->d2h;
+    return ZQD_OK;
+}
 extern "C" void zqd_result_destroy(zqd_result* r) { delete r; }
 
 // ------------------------------------------------------------ expression seam

@@ -286,6 +286,78 @@ class Job:
             pass
 
 
+class Batch:
+    """Staged batch: every job's tables resident on the device; run() re-propagates all jobs."""
+
+    def __init__(self, opts: list, precision: str = "fp64"):
+        self._L = _abi.load()
+        self.opts = opts
+        self._structs = [to_struct(o, precision) for o in opts]
+        arr = (C.POINTER(_abi.ZqdOptions) * len(opts))(*[C.pointer(s) for s, _ in self._structs])
+        self._h = C.c_void_p()
+        check(self._L.zqd_batch_create(arr, len(opts), C.byref(self._h)))
+
+    def run(self) -> float:
+        """Propagates every job once; returns the device time in ms (CUDA events)."""
+        check(self._L.zqd_batch_run(self._h))
+        return self._L.zqd_batch_device_ms(self._h)
+
+    @property
+    def launches(self) -> int:
+        return self._L.zqd_batch_launches(self._h)
+
+    def result(self, i: int, want_wavefunction=False) -> Result:
+        res = C.c_void_p()
+        check(self._L.zqd_batch_result(self._h, i, C.byref(res)))
+        try:
+            obs = _collect(res)
+            if want_wavefunction and obs:
+                _attach_wavefunctions(res, obs, _shape(self.opts[i]), len(obs[0].pop))
+            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res))
+        finally:
+            self._L.zqd_result_destroy(res)
+
+    def close(self):
+        if self._h:
+            self._L.zqd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def transfer_bytes(res_handle) -> tuple:
+    L = _abi.load()
+    h, d = C.c_uint64(), C.c_uint64()
+    check(L.zqd_result_transfer_bytes(res_handle, C.byref(h), C.byref(d)))
+    return h.value, d.value
+
+
+def run_batch_e2e(opts: list, precision: str = "fp64"):
+    """zqd_run_batch through the public API; returns (results, h2d bytes, d2h bytes)."""
+    L = _abi.load()
+    structs = [to_struct(o, precision) for o in opts]
+    arr = (C.POINTER(_abi.ZqdOptions) * len(opts))(*[C.pointer(s) for s, _ in structs])
+    res = (C.c_void_p * len(opts))()
+    check(L.zqd_run_batch(arr, len(opts), res))
+    h2d = d2h = 0
+    out = []
+    try:
+        for r in res:
+            h, d = transfer_bytes(r)
+            h2d += h
+            d2h += d
+            out.append(Result(observables=_collect(r), device_ms=L.zqd_result_device_ms(r)))
+    finally:
+        for r in res:
+            if r:
+                L.zqd_result_destroy(r)
+    return out, h2d, d2h
+
+
 def run_file(path: str, precision: str = "fp64"):
     """Runs every quantum_dynamics job of a Zinq input file ({"zinq": [...]}, src/main.zig:63-73,122-135)."""
     with open(path) as f:
