@@ -253,6 +253,19 @@ int zqd_fft_plan_create(uint32_t ndim, const int* shape, int sign, zqd_precision
 int zqd_fft_execute(zqd_fft* plan, void* device_inout, void* cuda_stream);
 void zqd_fft_destroy(zqd_fft* plan);
 
+/* No counterpart in the reference: the same transform as a plan's
+   zqd_fft_execute for callers that must not allocate device memory (code
+   running inside a framework's memory pool, or a host that owns one fixed
+   arena and forbids cudaMalloc/cudaFree).  The twiddle table lives in a
+   static 128 KiB device array of the library (held on every GPU that loads
+   it until exit), so n is at most 8192; larger n returns ZQD_ERR_UNSUPPORTED.
+   The first call on a device looks the array's address up once
+   (cudaGetSymbolAddress); make that first call before any stream capture.
+   Every call rewrites the shared table on `cuda_stream`, so calls that
+   overlap on the GPU race with one another.  Allocates nothing. */
+int zqd_fft_execute_noalloc(uint32_t ndim, const int* shape, int sign, zqd_precision precision, void* device_inout,
+                            void* cuda_stream);
+
 /* --------------------------------------------------------- expression seam
  * Replaces exprtk_init / exprtk_evaluate_d0 / exprtk_deinit
  * (src/exprtk.h:1-10, src/exprtk.cpp:10-40): compiles an expression over

@@ -107,6 +107,7 @@ SIGNATURES = [
     ("zqd_fft_plan_create", C.c_int, [C.c_uint32, C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(VP)]),
     ("zqd_fft_execute", C.c_int, [VP, VP, VP]),
     ("zqd_fft_destroy", None, [VP]),
+    ("zqd_fft_execute_noalloc", C.c_int, [C.c_uint32, C.POINTER(C.c_int), C.c_int, C.c_int, VP, VP]),
     ("zqd_expr_compile", C.c_int, [C.c_char_p, C.c_size_t, C.c_size_t, C.POINTER(VP)]),
     ("zqd_expr_eval_points", C.c_int, [VP, DP, C.c_size_t, C.c_double, DP]),
     ("zqd_expr_destroy", None, [VP]),
