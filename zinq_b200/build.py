@@ -23,6 +23,10 @@ SOURCES = ["options.cu", "expr.cpp", "job.cu", "result.cu", "fft_seam.cu"]
 # line_inst.cu is compiled once per (precision, number of electronic states)
 VARIANTS = [("line_inst.cu", f"line_{t[0]}{s}", [f"-DZQD_T={t}", f"-DZQD_S={s}", f"-DZQD_LAUNCH=launch_line_{t[0]}{s}"])
             for t in ("double", "float") for s in (1, 2, 3, 4)]
+# nd_inst.cu likewise: the 2-D / 3-D driver
+VARIANTS += [("nd_inst.cu", f"nd_{t[0]}{s}", [f"-DZQD_T={t}", f"-DZQD_S={s}", f"-DZQD_ND_CREATE=nd_create_{t[0]}{s}",
+                                               f"-DZQD_ND_RUN=nd_run_{t[0]}{s}"])
+             for t in ("double", "float") for s in (1, 2, 3, 4)]
 
 
 def _stale(target, deps):
@@ -32,16 +36,32 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def _headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    hs.append(os.path.join(os.path.dirname(HERE), "include", "zinq_qd.h"))
-    return hs
+def _headers(src):
+    """Local headers `src` includes, followed transitively (quoted includes only)."""
+    inc_dirs = [CSRC, os.path.join(os.path.dirname(HERE), "include")]
+    seen, todo = set(), [src]
+    while todo:
+        f = todo.pop()
+        with open(f) as fh:
+            for line in fh:
+                line = line.strip()
+                if not line.startswith("#include \""):
+                    continue
+                name = line.split('"')[1]
+                for d in [os.path.dirname(f)] + inc_dirs:
+                    h = os.path.join(d, name)
+                    if os.path.exists(h):
+                        if h not in seen:
+                            seen.add(h)
+                            todo.append(h)
+                        break
+    return sorted(seen)
 
 
 def _compile(item, verbose=False):
     src, stem, defines = item
     obj = os.path.join(BUILD, stem + ".o")
-    deps = [src] + _headers()
+    deps = [src] + _headers(src)
     if not _stale(obj, deps):
         return obj
     lang = ["-x", "cu"] if src.endswith(".cpp") else []

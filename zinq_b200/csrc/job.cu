@@ -7,6 +7,7 @@
 #include <mutex>
 
 #include "internal.h"
+#include "job.h"
 #include "line_solve.cuh"
 
 namespace zqd {
@@ -128,51 +129,11 @@ template <int S> __global__ void sign_scan_kernel(double* U, int n, int m, int C
     }
 }
 
-// ------------------------------------------------------------------ job state
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    int alloc(size_t b) {
-        bytes = b;
-        if (b == 0) return ZQD_OK;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail(ZQD_ERR_DEVICE_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
-        }
-        return ZQD_OK;
-    }
-    template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
-};
-
 } // namespace zqd
+
 
 using namespace zqd;
 
-struct zqd_job {
-    Opts o;
-    int S = 1, d = 1, n = 0;
-    size_t N = 0;
-    int C = 1, m = 0, q = 0, E = 8, threads = 32;
-    size_t smem = 0;
-    bool fp32 = false;
-    int nsolve = 1, hc = 0;
-    PotStore pot;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
-    float last_ms = 0;
-    size_t device_bytes = 0;
-    uint64_t h2d = 0, d2h = 0; // bytes copied by this job
-    ~zqd_job() {
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
 
 namespace zqd {
 
@@ -396,7 +357,7 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     ZQD_CUDA(cudaMemcpyAsync(hist.data(), J->hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
     ZQD_CUDA(cudaMemcpyAsync(fin.data(), J->fin.p, fin.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
     ZQD_CUDA(cudaMemcpyAsync(nrows.data(), J->rows.p, nrows.size() * sizeof(int), cudaMemcpyDeviceToHost, J->stream));
-    const size_t SN = (size_t)J->S * J->n;
+    const size_t SN = (size_t)J->S * J->N;
     std::vector<cx<T>> save(SN), orth;
     ZQD_CUDA(cudaMemcpyAsync(save.data(), J->psi_save.p, SN * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
     if (J->nsolve > 1) {
@@ -408,9 +369,9 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
               (save.size() + orth.size()) * sizeof(cx<T>);
     R->h2d = J->h2d;
     R->d2h = J->d2h;
-    R->ndim = 1;
+    R->ndim = (uint32_t)J->d;
     R->nstate = J->S;
-    R->npoint_total = J->n;
+    R->npoint_total = J->N;
     R->hc = J->hc;
     R->write_mask = J->o.write_mask;
     R->device_ms = J->last_ms;
@@ -422,15 +383,39 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
         so.fin.assign(fin.begin() + (size_t)s * J->hc, fin.begin() + (size_t)(s + 1) * J->hc);
         const cx<T>* src = (s + 1 < J->nsolve) ? orth.data() + (size_t)s * SN : save.data();
         so.psi.resize(2 * SN);
-        for (int st = 0; st < J->S; ++st)
-            for (int p = 0; p < J->n; ++p) { // un-permute: position p = c*m + j holds grid index c + C*j
-                int c = p / J->m, j = p - c * J->m, x = c + J->C * j;
-                cx<T> z = src[(size_t)st * J->n + p];
-                so.psi[2 * ((size_t)st * J->n + x)] = (double)z.x;
-                so.psi[2 * ((size_t)st * J->n + x) + 1] = (double)z.y;
+        if (J->d == 1) {
+            for (int st = 0; st < J->S; ++st)
+                for (int p = 0; p < J->n; ++p) { // un-permute: position p = c*m + j holds grid index c + C*j
+                    int c = p / J->m, j = p - c * J->m, x = c + J->C * j;
+                    cx<T> z = src[(size_t)st * J->n + p];
+                    so.psi[2 * ((size_t)st * J->n + x)] = (double)z.x;
+                    so.psi[2 * ((size_t)st * J->n + x) + 1] = (double)z.y;
+                }
+        } else {
+            for (size_t e = 0; e < SN; ++e) {
+                so.psi[2 * e] = (double)src[e].x;
+                so.psi[2 * e + 1] = (double)src[e].y;
             }
+        }
     }
     return ZQD_OK;
+}
+
+// N-D drivers compiled in nd_inst.cu, one translation unit per (precision, states)
+#define ZQD_ND_DECL(t, s) int nd_create_##t##s(zqd_job*); int nd_run_##t##s(zqd_job*);
+ZQD_ND_DECL(d, 1) ZQD_ND_DECL(d, 2) ZQD_ND_DECL(d, 3) ZQD_ND_DECL(d, 4)
+ZQD_ND_DECL(f, 1) ZQD_ND_DECL(f, 2) ZQD_ND_DECL(f, 3) ZQD_ND_DECL(f, 4)
+#undef ZQD_ND_DECL
+
+static int nd_create(zqd_job* J) {
+    static int (*const dt[4])(zqd_job*) = {nd_create_d1, nd_create_d2, nd_create_d3, nd_create_d4};
+    static int (*const ft[4])(zqd_job*) = {nd_create_f1, nd_create_f2, nd_create_f3, nd_create_f4};
+    return J->fp32 ? ft[J->S - 1](J) : dt[J->S - 1](J);
+}
+static int nd_run(zqd_job* J) {
+    static int (*const dt[4])(zqd_job*) = {nd_run_d1, nd_run_d2, nd_run_d3, nd_run_d4};
+    static int (*const ft[4])(zqd_job*) = {nd_run_f1, nd_run_f2, nd_run_f3, nd_run_f4};
+    return J->fp32 ? ft[J->S - 1](J) : dt[J->S - 1](J);
 }
 
 } // namespace zqd
@@ -454,13 +439,14 @@ extern "C" int zqd_job_create(const zqd_options* opt, zqd_job** out) {
     J->fp32 = J->o.precision == ZQD_FP32_MIXED;
     J->nsolve = J->o.imag_nstate ? (int)J->o.imag_nstate : 1;
     J->hc = RowLayout{J->d, J->S}.width();
-    if (J->d != 1) return fail(ZQD_ERR_UNSUPPORTED, "MULTI-DIMENSIONAL GRIDS ARE NOT AVAILABLE IN THIS BUILD YET");
-    if ((rc = choose_line_shape(J.get()))) return rc;
+    if (J->d == 1 && (rc = choose_line_shape(J.get()))) return rc;
+    if (J->d > 1 && J->n < 8) return fail(ZQD_ERR_UNSUPPORTED, "MULTI-DIMENSIONAL GRIDS NEED AT LEAST 8 POINTS PER AXIS");
     ZQD_CUDA(cudaStreamCreateWithFlags(&J->stream, cudaStreamNonBlocking));
     ZQD_CUDA(cudaEventCreate(&J->ev0));
     ZQD_CUDA(cudaEventCreate(&J->ev1));
     if ((rc = build_potential(J->o, J->pot))) return rc;
-    rc = J->fp32 ? create_line<float>(J.get()) : create_line<double>(J.get());
+    if (J->d == 1) rc = J->fp32 ? create_line<float>(J.get()) : create_line<double>(J.get());
+    else rc = nd_create(J.get());
     if (rc) return rc;
     *out = J.release();
     return ZQD_OK;
@@ -468,6 +454,7 @@ extern "C" int zqd_job_create(const zqd_options* opt, zqd_job** out) {
 
 extern "C" int zqd_job_run(zqd_job* J) {
     if (!J) return fail(ZQD_ERR_INVALID_INPUT, "NULL JOB");
+    if (J->d > 1) return nd_run(J);
     return J->fp32 ? run_line<float>(J) : run_line<double>(J);
 }
 
@@ -566,7 +553,7 @@ extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, 
         if (done[i]) continue;
         zqd_job* a = B->jobs[i].get();
         done[i] = true;
-        if (a->nsolve > 1) {
+        if (a->nsolve > 1 || a->d > 1) { // multi-solve and N-D jobs run on their own stream
             B->solo.push_back(a);
             continue;
         }

@@ -1,0 +1,56 @@
+// job.h -- the job handle behind the C-ABI, shared by the 1-D and N-D drivers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "internal.h"
+
+namespace zqd {
+
+// device allocation owned by a job
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    int alloc(size_t b) {
+        bytes = b;
+        if (b == 0) return ZQD_OK;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(ZQD_ERR_DEVICE_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
+        }
+        return ZQD_OK;
+    }
+    template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
+};
+
+} // namespace zqd
+
+struct zqd_job {
+    zqd::Opts o;
+    int S = 1, d = 1, n = 0;
+    size_t N = 0;
+    int C = 1, m = 0, q = 0, E = 8, threads = 32;
+    size_t smem = 0;
+    bool fp32 = false;
+    int nsolve = 1, hc = 0;
+    zqd::PotStore pot;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    zqd::DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
+    zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
+    int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
+    float last_ms = 0;
+    size_t device_bytes = 0;
+    uint64_t h2d = 0, d2h = 0; // bytes copied by this job
+    ~zqd_job() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};

@@ -1,0 +1,280 @@
+// nd_inst.cu -- the 2-D / 3-D driver for one (precision, state count) pair.
+// Compiled once per pair with -DZQD_T=<double|float> -DZQD_S=<1..4>
+// -DZQD_ND_CREATE=<symbol> -DZQD_ND_RUN=<symbol>.
+//
+// A solve (src/quantum_dynamics.zig:860-950) is a stream-ordered sequence of
+// axis passes (nd_kernels.cuh); nothing returns to the host until the end.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "job.h"
+#include "nd_kernels.cuh"
+
+#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_ND_CREATE) || !defined(ZQD_ND_RUN)
+#error "nd_inst.cu needs -DZQD_T, -DZQD_S, -DZQD_ND_CREATE and -DZQD_ND_RUN"
+#endif
+
+namespace zqd {
+namespace {
+
+using T = ZQD_T;
+constexpr int S = ZQD_S;
+constexpr int NSYM = S * (S + 1) / 2;
+
+NdJob<T> describe(zqd_job* J) {
+    NdJob<T> D{};
+    const Opts& o = J->o;
+    D.d = J->d;
+    D.n = J->n;
+    while ((1 << D.logn) < J->n) ++D.logn;
+    D.S = S;
+    D.N = J->N;
+    for (int j = 0; j < D.d; ++j) {
+        D.lo[j] = o.bounds[2 * j];
+        D.span[j] = o.bounds[2 * j + 1] - o.bounds[2 * j];
+        D.mass[j] = o.mass[j];
+        D.dkunit[j] = 6.283185307179586476925286766559 / D.span[j];
+        D.x0[j] = o.pos[j];
+        D.p0[j] = o.mom[j];
+        D.gamma[j] = o.gamma[j];
+        if (o.has_cap) {
+            D.cap_lo[j] = o.cap_bounds[2 * j];
+            D.cap_hi[j] = o.cap_bounds[2 * j + 1];
+        }
+    }
+    double dr = 1; // Grid.init (wavepacket.zig:44-53)
+    for (int j = 0; j < D.d; ++j) dr *= D.span[j] / (double)J->n;
+    D.dr = dr;
+    D.dk = dr / (double)J->N;
+    D.dt_re = o.imag_nstate ? 0.0 : o.time_step;
+    D.dt_im = o.imag_nstate ? -o.time_step : 0.0;
+    D.adiabatic = o.adiabatic;
+    D.track = o.has_cap && o.cap_track;
+    D.has_cap = o.has_cap;
+    D.cap_exp = o.cap_exponent;
+    D.ic_state = (int)o.ic_state;
+    D.ic_adia = o.ic_adiabatic;
+    D.psi = J->psi_save.as<cx<T>>();
+    D.phi = J->phi.as<cx<T>>();
+    D.psi0 = J->psi0.as<cx<T>>();
+    D.orth = J->orth.as<cx<T>>();
+    D.R = J->R.as<Tab<T>>();
+    D.V = J->V.as<double>();
+    D.U = J->U.as<double>();
+    D.capw = J->capw.as<double>();
+    D.tw = J->tw.as<Tab<T>>();
+    D.part = J->part.as<double>();
+    D.rows_per_cta = J->nd_rows;
+    D.tile = J->nd_tile;
+    D.stopped = J->flags.as<int>();
+    D.pot = J->pot.dev;
+    return D;
+}
+
+struct Launch {
+    zqd_job* J;
+    NdJob<T> D;
+    size_t nrow_blocks, ntile_blocks, ngrid;
+    // partial-sum regions (in blocks)
+    size_t R0, R1, R2, K, G;
+
+    int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false) {
+        NdJob<T> d = D;
+        if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
+        const int nbuf = (mode & RM_PHI) ? 3 : 2;
+        const size_t smem = nd_smem_bytes<T>(nbuf, S * J->nd_rows, J->n);
+        nd_row_kernel<T, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
+        ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
+    int tile(int axis, uint32_t mode, size_t region, bool nostop = false) {
+        NdJob<T> d = D;
+        if (nostop) d.stopped = J->flags.as<int>() + 1;
+        const size_t smem = nd_smem_bytes<T>(2, J->nd_tile, J->n);
+        nd_tile_kernel<T><<<dim3((unsigned)ntile_blocks, S), J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
+        ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
+    // forward along axes d-2..1, forward + kinetic phase + inverse along axis 0, inverse along 1..d-2
+    int step_tiles() {
+        int rc;
+        for (int a = D.d - 2; a >= 1; --a)
+            if ((rc = tile(a, TM_FWD, 0))) return rc;
+        if ((rc = tile(0, TM_FWD | TM_KPHASE | TM_INV, 0))) return rc;
+        for (int a = 1; a <= D.d - 2; ++a)
+            if ((rc = tile(a, TM_INV, 0))) return rc;
+        return ZQD_OK;
+    }
+    // momentum observables of phi (the forward transform along the last axis is already done)
+    int kobs(bool nostop = false) {
+        int rc;
+        for (int a = D.d - 2; a >= 1; --a)
+            if ((rc = tile(a, TM_FWD | TM_PHI, 0, nostop))) return rc;
+        return tile(0, TM_FWD | TM_KOBS | TM_PHI, K, nostop);
+    }
+};
+
+} // namespace
+
+int ZQD_ND_CREATE(zqd_job* J) {
+    const size_t N = J->N, c = sizeof(cx<T>), tb = sizeof(Tab<T>);
+    const Opts& o = J->o;
+    const int n = J->n;
+    // launch shapes: rows per CTA so a CTA has ~128 threads and fits in shared memory
+    const int budget = 200 * 1024;
+    const bool any_k = true; // the final observables always need the momentum-space round trip
+    J->nd_row_bufs = any_k ? 3 : 2;
+    int L = std::max(1, std::min<int>((int)(N / n), 1024 / n));
+    while (L > 1 && nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget) L >>= 1;
+    if (nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget)
+        return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS (npoint at most 1024 per axis)");
+    J->nd_rows = L;
+    J->nd_row_threads = std::max(32, std::min(512, (L * n / 8 + 31) / 32 * 32));
+    int Tn = std::min(n, (int)(128 / c)); // 128-byte rows of the tile
+    while (Tn > 1 && Tn * n / 8 > 512) Tn >>= 1;
+    while (Tn > 1 && nd_smem_bytes<T>(2, Tn, n) > (size_t)budget) Tn >>= 1;
+    J->nd_tile = Tn;
+    J->nd_tile_threads = std::max(32, std::min(512, (Tn * n / 8 + 31) / 32 * 32));
+    const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
+    const size_t nparts = 3 * nrow_blocks + S * ntile_blocks + 1024;
+    int rc;
+    if ((rc = J->psi_save.alloc((size_t)S * N * c))) return rc;
+    if ((rc = J->phi.alloc((size_t)S * N * c))) return rc;
+    if ((o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF)) && (rc = J->psi0.alloc((size_t)S * N * c))) return rc;
+    if (o.imag_nstate > 1 && (rc = J->orth.alloc((size_t)(o.imag_nstate - 1) * S * N * c))) return rc;
+    if ((rc = J->R.alloc((size_t)NSYM * N * tb))) return rc;
+    if ((rc = J->V.alloc((size_t)S * S * N * sizeof(double)))) return rc;
+    if (S > 1 && (rc = J->U.alloc((size_t)S * S * N * sizeof(double)))) return rc;
+    if (o.has_cap && (rc = J->capw.alloc(N * sizeof(double)))) return rc;
+    if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
+    if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
+    if ((rc = J->book.alloc(sizeof(NdBook)))) return rc;
+    if ((rc = J->flags.alloc(2 * sizeof(int)))) return rc;
+    const size_t rows = (size_t)o.iterations + 1;
+    if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double)))) return rc;
+    if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double)))) return rc;
+    if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
+    J->device_bytes = J->psi_save.bytes + J->phi.bytes + J->psi0.bytes + J->orth.bytes + J->R.bytes + J->V.bytes +
+                      J->U.bytes + J->capw.bytes + J->part.bytes + J->hist.bytes;
+    std::vector<double> tw = twiddles_f64(n);
+    std::vector<Tab<T>> twt(n);
+    for (int t = 0; t < n; ++t) twt[t] = mktab<T>(tw[2 * t], tw[2 * t + 1]);
+    ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twt.data(), (size_t)n * tb, cudaMemcpyHostToDevice, J->stream));
+    ZQD_CUDA(cudaMemsetAsync(J->flags.p, 0, 2 * sizeof(int), J->stream));
+    ZQD_CUDA(cudaMemsetAsync(J->hist.p, 0xff, J->hist.bytes, J->stream)); // NaN until written
+    J->h2d += (size_t)n * tb + J->pot.bytes;
+    NdJob<T> D = describe(J);
+    nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(D, 0.0, 1);
+    ZQD_CUDA(cudaGetLastError());
+    for (auto f : {nd_row_kernel<T, S>}) ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+    ZQD_CUDA(cudaFuncSetAttribute(nd_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    return ZQD_OK;
+}
+
+int ZQD_ND_RUN(zqd_job* J) {
+    const Opts& o = J->o;
+    Launch Lc{J, describe(J)};
+    const size_t N = J->N;
+    Lc.nrow_blocks = N / J->n / J->nd_rows;
+    Lc.ntile_blocks = N / J->n / J->nd_tile;
+    Lc.ngrid = std::min<size_t>(1024, (N + 255) / 256);
+    Lc.R0 = 0;
+    Lc.R1 = Lc.nrow_blocks;
+    Lc.R2 = 2 * Lc.nrow_blocks;
+    Lc.K = 3 * Lc.nrow_blocks;
+    Lc.G = Lc.K + S * Lc.ntile_blocks;
+    const bool split = o.imag_nstate > 0 || o.pot_td || (o.has_cap && o.cap_has_stop);
+    const bool acf = o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF);
+    const int iters = (int)o.iterations, HC = J->hc;
+    const size_t SN = (size_t)S * N * sizeof(cx<T>);
+    const unsigned ng = (unsigned)Lc.ngrid;
+    int rc;
+    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+    for (int s = 0; s < J->nsolve; ++s) {
+        Lc.D.orth = J->orth.as<cx<T>>();
+        double* hist = J->hist.as<double>() + (size_t)s * (iters + 1) * HC;
+        int* rows_out = J->rows.as<int>() + s;
+        ZQD_CUDA(cudaMemsetAsync(J->flags.p, 0, 2 * sizeof(int), J->stream));
+        ZQD_CUDA(cudaMemsetAsync(J->book.p, 0, sizeof(NdBook), J->stream));
+        // setGaussian, normalise, toDia, acf reference (quantum_dynamics.zig:867-882)
+        nd_gauss_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G);
+        ZQD_CUDA(cudaGetLastError());
+        nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G, Lc.G + ng, o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
+        ZQD_CUDA(cudaGetLastError());
+        auto finalize = [&](size_t x0, size_t x1, bool k, uint32_t mask, int i) -> int {
+            nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, x0, x1, Lc.K, k ? Lc.K + S * Lc.ntile_blocks : Lc.K, mask,
+                                                          hist + (size_t)i * HC, J->book.as<NdBook>(), rows_out, i,
+                                                          o.has_cap && o.cap_has_stop, o.cap_stop_norm, 0);
+            ZQD_CUDA(cudaGetLastError());
+            return ZQD_OK;
+        };
+        auto carry = [&](size_t r0, size_t r1) -> int { // absorbed sums of the next step's start
+            nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, r0, r1, Lc.K, Lc.K, 0, J->fin.as<double>() + (size_t)s * HC,
+                                                          J->book.as<NdBook>(), rows_out, 0, 0, 0.0, 2);
+            ZQD_CUDA(cudaGetLastError());
+            return ZQD_OK;
+        };
+        auto itp_ops = [&]() -> int { // quantum_dynamics.zig:898-906
+            for (int j = 0; j < s; ++j) {
+                nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G);
+                nd_orth_apply_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G, Lc.G + ng);
+            }
+            nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, -1, Lc.G);
+            nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G, Lc.G + ng, 0, 0);
+            ZQD_CUDA(cudaGetLastError());
+            return ZQD_OK;
+        };
+        for (int i = 0; i <= iters; ++i) {
+            const bool logstep = o.log && ((i % o.log_interval == 0) || (i == iters));
+            const uint32_t mask = o.write_mask | (logstep ? (uint32_t)WM_ALL_OBS : 0u) | (acf ? (uint32_t)WM_ACF : 0u);
+            const bool needk = mask & (WM_MOM | WM_EKIN | WM_ETOT);
+            const uint32_t obs = mask | ((o.has_cap && o.cap_has_stop) ? (uint32_t)WM_NORM : 0u);
+            if (i > 0 && (rc = Lc.step_tiles())) return rc;
+            if (!split) {
+                uint32_t mode = RM_OBS | RM_STORE | (needk ? RM_PHI : 0u);
+                if (i > 0) mode |= RM_INV | RM_REND;
+                if (i < iters) mode |= RM_RSTART | RM_FWD;
+                if ((rc = Lc.row(mode, obs, Lc.R0))) return rc;
+                if (needk && (rc = Lc.kobs())) return rc;
+                if ((rc = finalize(Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, i))) return rc;
+            } else {
+                if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
+                if (o.imag_nstate && (rc = itp_ops())) return rc; // every i, the initial state included
+                if (i == 0) ZQD_CUDA(cudaMemsetAsync(Lc.D.part, 0, Lc.nrow_blocks * NDV * 2 * sizeof(double), J->stream));
+                if (o.pot_td) {
+                    nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, (double)i * o.time_step, 0);
+                    ZQD_CUDA(cudaGetLastError());
+                }
+                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1))) return rc;
+                if (needk && (rc = Lc.kobs())) return rc;
+                if ((rc = finalize(Lc.R0, Lc.R1 + Lc.nrow_blocks, needk, mask, i))) return rc;
+                if (i < iters) {
+                    if (o.pot_td) {
+                        nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, ((double)i + 0.5) * o.time_step, 1);
+                        ZQD_CUDA(cudaGetLastError());
+                    }
+                    if ((rc = Lc.row(RM_RSTART | RM_FWD | RM_STORE, 0, Lc.R2))) return rc;
+                    if ((rc = carry(Lc.R2, Lc.R2 + Lc.nrow_blocks))) return rc;
+                }
+            }
+        }
+        // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
+        const uint32_t all = WM_ALL_OBS | (acf ? (uint32_t)WM_ACF : 0u);
+        if ((rc = Lc.row(RM_OBS | RM_PHI, all, Lc.R1, true))) return rc;
+        if ((rc = Lc.kobs(true))) return rc;
+        nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, Lc.R1, Lc.R1 + Lc.nrow_blocks, Lc.K, Lc.K + S * Lc.ntile_blocks,
+                                                      all, J->fin.as<double>() + (size_t)s * HC, J->book.as<NdBook>(),
+                                                      rows_out, 0, 0, 0.0, 1);
+        ZQD_CUDA(cudaGetLastError());
+        if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)
+            ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice, J->stream));
+    }
+    ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
+    return ZQD_OK;
+}
+
+} // namespace zqd

@@ -1,0 +1,692 @@
+// nd_kernels.cuh -- split-operator passes for 2-D and 3-D grids.
+//
+// The wavefunction (S x N complex, state-major, last axis fastest: the
+// reference's Matrix(Complex) layout, src/wavepacket.zig:182) stays in global
+// memory; a time step is a sequence of axis passes, each staging lines of one
+// axis in shared memory, running the Stockham FFT passes there and writing
+// them back:
+//   row pass   (last axis, contiguous; all S states of a row in one CTA)
+//              [inverse FFT, 1/N, accumAbsorbed, R]  ... end of step i
+//              [observables of step i]
+//              [accumAbsorbed, R, forward FFT]       ... start of step i+1
+//   tile pass  (a strided axis; `tile` consecutive lines of one state per CTA)
+//              forward FFT | forward FFT, exp(-i K dt), inverse FFT | inverse FFT
+// so a 2-D step is one row pass + one tile pass, a 3-D step one row pass and
+// three tile passes (Propagator.step, src/quantum_dynamics.zig:417-427).
+// Observables are per-CTA compensated partial sums combined in a fixed order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "cx.cuh"
+#include "line_kernel.cuh"
+#include "physics.cuh"
+
+namespace zqd {
+
+constexpr int NDV = 24; // reduction slots of the N-D passes
+
+// norm | pos[d] | epot | acf re, im | mom[d] | ekin | pop[S] | absorbed, this step [S] | absorbed, next step [S]
+struct NdSlots {
+    int d, S;
+    __host__ __device__ constexpr int norm() const { return 0; }
+    __host__ __device__ constexpr int pos() const { return 1; }
+    __host__ __device__ constexpr int epot() const { return 1 + d; }
+    __host__ __device__ constexpr int acf() const { return 2 + d; }
+    __host__ __device__ constexpr int mom() const { return 4 + d; }
+    __host__ __device__ constexpr int ekin() const { return 4 + 2 * d; }
+    __host__ __device__ constexpr int pop() const { return 5 + 2 * d; }
+    __host__ __device__ constexpr int abs() const { return 5 + 2 * d + S; }
+    __host__ __device__ constexpr int absn() const { return 5 + 2 * d + 2 * S; }
+    __host__ __device__ constexpr int count() const { return 5 + 2 * d + 3 * S; }
+};
+
+template <typename T> struct NdJob {
+    int d, n, logn, S;
+    size_t N;
+    double lo[3], span[3], mass[3];
+    double dr, dk, dkunit[3];
+    double dt_re, dt_im;
+    int adiabatic, track, has_cap, ic_state, ic_adia;
+    double cap_lo[3], cap_hi[3], cap_exp, x0[3], p0[3], gamma[3];
+    cx<T>* psi;   // [S][N]
+    cx<T>* phi;   // [S][N] scratch: the forward transform of the end-of-step psi
+    cx<T>* psi0;  // [S][N] autocorrelation reference
+    const cx<T>* orth; // [northo][S][N] relaxed states (imaginary time)
+    Tab<T>* R;    // [NSYM][N]
+    double* V;    // [S*S][N]
+    double* U;    // [S*S][N]
+    double* capw; // [N]
+    const Tab<T>* tw; // [n] exp(-2 pi i t / n)
+    double* part;     // per-CTA partial sums [blocks][NDV][2]
+    int rows_per_cta; // row pass: rows of the last axis per CTA
+    int tile;         // tile pass: lines per CTA
+    int* stopped;     // set by the finalize kernel when stop_norm ends the solve
+    PotDev pot;
+};
+
+// row-pass modes
+enum : uint32_t {
+    RM_INV = 1u << 0,    // inverse FFT along the last axis, then 1/N
+    RM_REND = 1u << 1,   // accumAbsorbed (if tracking) then R: end of a step
+    RM_OBS = 1u << 2,    // position-space observables (after RM_REND)
+    RM_PHI = 1u << 3,    // forward FFT of the end-of-step psi into phi (momentum observables)
+    RM_RSTART = 1u << 4, // accumAbsorbed (if tracking) then R: start of the next step
+    RM_FWD = 1u << 5,    // forward FFT along the last axis
+    RM_STORE = 1u << 6,  // write psi back
+};
+// tile-pass modes
+enum : uint32_t {
+    TM_FWD = 1u << 0,
+    TM_KPHASE = 1u << 1, // after the forward FFT along axis 0: psi *= exp(-i K dt)
+    TM_INV = 1u << 2,
+    TM_KOBS = 1u << 3,   // after the forward FFT along axis 0: momentum observables, no store
+    TM_PHI = 1u << 4,    // operate on phi instead of psi
+};
+
+template <typename T> __host__ __device__ inline int tile_ldp(int n) { return padded_len<T>(n) | 1; }
+// dynamic shared memory: nbuf line buffers of `lines` lines + the twiddle table
+template <typename T> __host__ __device__ inline size_t nd_smem_bytes(int nbuf, int lines, int n) {
+    return (size_t)nbuf * lines * tile_ldp<T>(n) * sizeof(cx<T>) + (size_t)n * sizeof(Tab<T>);
+}
+
+template <typename T> __device__ __forceinline__ void grid_coords(const NdJob<T>& J, size_t gidx, double* r) {
+    // Grid.init (wavepacket.zig:55-74): last axis fastest
+    size_t t = gidx;
+    for (int l = 0; l < J.d; ++l) {
+        const int j = J.d - l - 1;
+        r[j] = __dadd_rn(J.lo[j], __dmul_rn((double)(t % (size_t)J.n), J.span[j]) / (double)J.n);
+        t /= (size_t)J.n;
+    }
+}
+template <typename T> __device__ __forceinline__ void grid_wavenumbers(const NdJob<T>& J, size_t gidx, double* k) {
+    size_t t = gidx;
+    for (int l = 0; l < J.d; ++l) {
+        const int j = J.d - l - 1;
+        const int idx = (int)(t % (size_t)J.n);
+        k[j] = __dmul_rn(idx < J.n / 2 ? (double)idx : __dsub_rn((double)idx, (double)J.n), J.dkunit[j]);
+        t /= (size_t)J.n;
+    }
+}
+
+// Radix-R Stockham pass over `ngroups` groups of G lines of n = 2^logn points
+// (line (g, s) at index s * ngroups + g, stride ldp).  A thread handles butterfly
+// i of all G lines of a group, so the G states of a grid point meet in one thread.
+template <typename T, int G, int R, int SIGN, bool FIRST, bool LAST, typename H>
+__device__ __forceinline__ void tpass(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int ldp, int logn, int p,
+                                      int logp, const Tab<T>* __restrict__ twm, int ngroups, H& h) {
+    constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
+    const int logmr = logn - LR, mr = 1 << logmr;
+    const int tshift = logn - logp - LR;
+    const int items = ngroups << logmr;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int g = it >> logmr, i = it & (mr - 1);
+        cx<T> v[G][R];
+#pragma unroll
+        for (int s = 0; s < G; ++s)
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[s][r] = in[(s * ngroups + g) * ldp + padx<T>(i + r * mr)];
+        if constexpr (FIRST) h.template first<R>(g, i, mr, v);
+        const int kk = i & (p - 1);
+        if (p > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const Tab<T> w = twm[(r * kk) << tshift];
+#pragma unroll
+                for (int s = 0; s < G; ++s) v[s][r] = tmul<SIGN>(v[s][r], w);
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < G; ++s) dft<R, SIGN, T>(v[s]);
+        const int o0 = ((i - kk) << LR) + kk;
+        if constexpr (LAST) h.template last<R>(g, o0, p, v);
+#pragma unroll
+        for (int s = 0; s < G; ++s)
+#pragma unroll
+            for (int r = 0; r < R; ++r) out[(s * ngroups + g) * ldp + padx<T>(o0 + r * p)] = v[s][r];
+    }
+    __syncthreads();
+}
+
+// Full n-point transform of the staged lines, ping-ponging a -> b -> ...; the
+// hooks run in the first / last pass.  Returns the buffer holding the result.
+template <typename T, int G, int SIGN, bool HF, bool HL, typename H>
+__device__ __forceinline__ cx<T>* tfft(cx<T>* a, cx<T>* b, int ldp, int logn, const Tab<T>* twm, int ngroups, H& h) {
+    int p = 1, logp = 0, rem = logn;
+    bool first = true;
+    cx<T>* in = a;
+    cx<T>* out = b;
+    while (rem > 0) {
+        const int LR = rem >= 3 ? 3 : rem;
+        const bool last = rem == LR;
+        if (LR == 3) {
+            if (first && last) tpass<T, G, 8, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+            else if (first) tpass<T, G, 8, SIGN, HF, false>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+            else if (last) tpass<T, G, 8, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+            else tpass<T, G, 8, SIGN, false, false>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+        } else if (LR == 2) {
+            if (first) tpass<T, G, 4, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+            else tpass<T, G, 4, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+        } else {
+            if (first) tpass<T, G, 2, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+            else tpass<T, G, 2, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
+        }
+        cx<T>* t = in;
+        in = out;
+        out = t;
+        p <<= LR;
+        logp += LR;
+        rem -= LR;
+        first = false;
+    }
+    return in;
+}
+
+struct NdNoHook {
+    template <int R, typename V> __device__ __forceinline__ void first(int, int, int, V&) {}
+    template <int R, typename V> __device__ __forceinline__ void last(int, int, int, V&) {}
+};
+
+// per-CTA reduction of nv compensated sums into part[block][NDV][2] (fixed order)
+__device__ __forceinline__ void block_partials(Acc (&a)[NDV], int nv, double* __restrict__ part, size_t block) {
+    __shared__ double red[16][NDV][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int v = 0; v < NDV; ++v) {
+        if (v < nv) {
+            double s = a[v].s, c = a[v].c;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double s2 = __shfl_down_sync(0xffffffffu, s, off), c2 = __shfl_down_sync(0xffffffffu, c, off);
+                Acc t;
+                t.s = s;
+                t.c = c;
+                t.add(s2);
+                t.c += c2;
+                s = t.s;
+                c = t.c;
+            }
+            if (lane == 0) {
+                red[warp][v][0] = s;
+                red[warp][v][1] = c;
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        Acc t;
+        for (int w = 0; w < nw; ++w) {
+            t.add(red[w][threadIdx.x][0]);
+            t.c += red[w][threadIdx.x][1];
+        }
+        part[(block * NDV + threadIdx.x) * 2] = t.s;
+        part[(block * NDV + threadIdx.x) * 2 + 1] = t.c;
+    }
+    __syncthreads();
+}
+
+// sum of slot v over partial blocks [b0, b1) in block order
+__device__ __forceinline__ Acc sum_partials(const double* __restrict__ part, size_t b0, size_t b1, int v) {
+    Acc t;
+    for (size_t b = b0; b < b1; ++b) {
+        t.add(part[(b * NDV + v) * 2]);
+        t.c += part[(b * NDV + v) * 2 + 1];
+    }
+    return t;
+}
+
+// ------------------------------------------------------------ row pass
+template <typename T, int S> struct RowHook {
+    const NdJob<T>* J;
+    Acc* acc;
+    NdSlots sl;
+    uint32_t mode, obs; // obs: WM_* bits wanted by RM_OBS
+    size_t row0;        // first grid point of the CTA's rows
+    int n;
+    T last_scale;       // 1/N after an inverse transform, 1 otherwise
+
+    __device__ __forceinline__ void absorbed(const cx<T>* x, size_t gidx, int slot) {
+        const double w = J->capw[gidx];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            double are = 0, aim = 0;
+            if (J->adiabatic && S > 1) {
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const double u = J->U[(size_t)(k * S + i) * J->N + gidx];
+                    are += (double)x[k].x * u;
+                    aim += (double)x[k].y * u;
+                }
+            } else {
+                are = (double)x[i].x;
+                aim = (double)x[i].y;
+            }
+            acc[slot + i].add(w * (are * are + aim * aim));
+        }
+    }
+    __device__ __forceinline__ void apply_r(cx<T>* x, size_t gidx) const {
+        constexpr int NSYM = S * (S + 1) / 2;
+        Tab<T> r[NSYM];
+#pragma unroll
+        for (int c = 0; c < NSYM; ++c) r[c] = J->R[(size_t)c * J->N + gidx];
+        cx<T> y[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            cx<T> a = mk<T>(0, 0);
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int p = i < k ? i : k, q = i < k ? k : i;
+                a = add<T>(a, tmul<-1>(x[k], r[p * S - p * (p - 1) / 2 + (q - p)]));
+            }
+            y[i] = a;
+        }
+#pragma unroll
+        for (int i = 0; i < S; ++i) x[i] = y[i];
+    }
+    __device__ __forceinline__ void observe(const cx<T>* x, size_t gidx) {
+        double m2 = 0;
+        const bool adia = J->adiabatic && S > 1;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const double w = (double)x[s].x * (double)x[s].x + (double)x[s].y * (double)x[s].y;
+            m2 += w;
+            if ((obs & WM_POP) && !adia) acc[sl.pop() + s].add(w);
+        }
+        acc[sl.norm()].add(m2);
+        if (obs & WM_POS) {
+            double r[3];
+            grid_coords(*J, gidx, r);
+            for (int k = 0; k < J->d; ++k) acc[sl.pos() + k].add(m2 * r[k]);
+        }
+        if (obs & (WM_EPOT | WM_ETOT)) {
+            double e = 0;
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int k = 0; k < S; ++k)
+                    e += ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) *
+                         J->V[(size_t)(i * S + k) * J->N + gidx];
+            acc[sl.epot()].add(e);
+        }
+        if (obs & WM_ACF) {
+            double re = 0, im = 0;
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                const cx<T> z0 = J->psi0[(size_t)s * J->N + gidx];
+                re += (double)z0.x * (double)x[s].x + (double)z0.y * (double)x[s].y;
+                im += (double)z0.x * (double)x[s].y - (double)z0.y * (double)x[s].x;
+            }
+            acc[sl.acf()].add(re);
+            acc[sl.acf() + 1].add(im);
+        }
+        if ((obs & WM_POP) && adia) {
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                double are = 0, aim = 0;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const double u = J->U[(size_t)(k * S + i) * J->N + gidx];
+                    are += (double)x[k].x * u;
+                    aim += (double)x[k].y * u;
+                }
+                acc[sl.pop() + i].add(are * are + aim * aim);
+            }
+        }
+    }
+    // first pass of the forward transform: start of the next step
+    template <int R> __device__ __forceinline__ void first(int g, int i, int mr, cx<T> (&v)[S][R]) {
+        if (!(mode & RM_RSTART)) return;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const size_t gidx = row0 + (size_t)g * n + i + r * mr;
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = v[s][r];
+            if (J->track) absorbed(x, gidx, sl.absn());
+            apply_r(x, gidx);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][r] = x[s];
+        }
+    }
+    // last pass of the inverse transform (or a pass of its own): end of the step
+    template <int R> __device__ __forceinline__ void last(int g, int o0, int p, cx<T> (&v)[S][R]) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const size_t gidx = row0 + (size_t)g * n + o0 + r * p;
+            cx<T> x[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) x[s] = scale<T>(v[s][r], last_scale);
+            if (mode & RM_REND) {
+                if (J->track) absorbed(x, gidx, sl.abs());
+                apply_r(x, gidx);
+            }
+            if (mode & RM_OBS) observe(x, gidx);
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][r] = x[s];
+        }
+    }
+};
+
+// rows_per_cta rows (of every state) per CTA; `mode` selects the stages
+template <typename T, int S>
+__global__ void __launch_bounds__(512) nd_row_kernel(NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base) {
+    if (*J.stopped) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = J.n, logn = J.logn, L = J.rows_per_cta;
+    const int ldp = tile_ldp<T>(n), lines = S * L;
+    cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* buf1 = buf0 + lines * ldp;
+    cx<T>* buf2 = buf1 + lines * ldp; // only with RM_PHI
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(buf0 + ((mode & RM_PHI) ? 3 : 2) * lines * ldp);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    const size_t row0 = (size_t)blockIdx.x * L * n;
+    for (int e = threadIdx.x; e < lines * n; e += blockDim.x) { // line (state s, row l) = s * L + l
+        const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
+        buf0[(s * L + l) * ldp + padx<T>(x)] = J.psi[(size_t)s * J.N + row0 + (size_t)l * n + x];
+    }
+    __syncthreads();
+    const NdSlots sl{J.d, S};
+    Acc acc[NDV];
+    RowHook<T, S> h{&J, acc, sl, mode, obs, row0, n, (T)(1.0 / (double)J.N)};
+    cx<T>* cur = buf0;
+    cx<T>* oth = buf1;
+    if (mode & RM_INV) {
+        cur = tfft<T, S, 1, false, true>(cur, oth, ldp, logn, twm, L, h);
+        oth = cur == buf0 ? buf1 : buf0;
+    } else if (mode & (RM_REND | RM_OBS)) { // end-of-step stages without a transform
+        h.last_scale = (T)1;
+        for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
+            const int l = it / n, x = it - l * n;
+            cx<T> v[S][1];
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s][0] = cur[(s * L + l) * ldp + padx<T>(x)];
+            h.template last<1>(l, x, 1, v);
+#pragma unroll
+            for (int s = 0; s < S; ++s) cur[(s * L + l) * ldp + padx<T>(x)] = v[s][0];
+        }
+        __syncthreads();
+    }
+    if (mode & RM_PHI) { // forward FFT of a copy into phi; cur must survive for RM_RSTART
+        for (int e = threadIdx.x; e < lines * ldp; e += blockDim.x) oth[e] = cur[e];
+        __syncthreads();
+        NdNoHook none;
+        cx<T>* res = tfft<T, S, -1, false, false>(oth, buf2, ldp, logn, twm, L, none);
+        for (int e = threadIdx.x; e < lines * n; e += blockDim.x) {
+            const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
+            J.phi[(size_t)s * J.N + row0 + (size_t)l * n + x] = res[(s * L + l) * ldp + padx<T>(x)];
+        }
+        __syncthreads();
+    }
+    if (mode & RM_FWD) cur = tfft<T, S, -1, true, false>(cur, oth, ldp, logn, twm, L, h);
+    if (mode & RM_STORE)
+        for (int e = threadIdx.x; e < lines * n; e += blockDim.x) {
+            const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
+            J.psi[(size_t)s * J.N + row0 + (size_t)l * n + x] = cur[(s * L + l) * ldp + padx<T>(x)];
+        }
+    if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials(acc, sl.count(), J.part, part_base + blockIdx.x);
+}
+
+// ------------------------------------------------------------ tile pass
+template <typename T> struct TileHook {
+    const NdJob<T>* J;
+    Acc* acc;
+    NdSlots sl;
+    uint32_t mode;
+    size_t c0, stride; // grid index of line g at position t along the axis: c0 + t * stride + g
+    template <int R> __device__ __forceinline__ void first(int, int, int, cx<T> (&)[1][R]) {}
+    template <int R> __device__ __forceinline__ void last(int g, int o0, int p, cx<T> (&v)[1][R]) {
+        if (!(mode & (TM_KPHASE | TM_KOBS))) return;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const size_t gidx = c0 + (size_t)(o0 + r * p) * stride + g;
+            double k[3];
+            grid_wavenumbers(*J, gidx, k);
+            double K = 0; // Hamiltonian.init: sum_j 0.5 k_j^2 / m_j (wavepacket.zig:109-119)
+            for (int j = 0; j < J->d; ++j) K += __dmul_rn(__dmul_rn(0.5, k[j]), k[j]) / J->mass[j];
+            if (mode & TM_KPHASE) { // exp(Complex(0, -K) * dt) (quantum_dynamics.zig:397-399)
+                const double zre = __dsub_rn(__dmul_rn(0.0, J->dt_re), __dmul_rn(-K, J->dt_im));
+                const double zim = __dadd_rn(__dmul_rn(0.0, J->dt_im), __dmul_rn(-K, J->dt_re));
+                double ore, oim;
+                cexp_dev(zre, zim, ore, oim);
+                v[0][r] = tmul<-1>(v[0][r], mktab<T>(ore, oim));
+            } else { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268)
+                const double w = (double)v[0][r].x * (double)v[0][r].x + (double)v[0][r].y * (double)v[0][r].y;
+                for (int j = 0; j < J->d; ++j) acc[sl.mom() + j].add(w * k[j]);
+                acc[sl.ekin()].add(w * K);
+            }
+        }
+    }
+};
+
+// one state's tile of J.tile consecutive lines along `axis` (stride n^(d-1-axis))
+template <typename T>
+__global__ void __launch_bounds__(512) nd_tile_kernel(NdJob<T> J, int axis, uint32_t mode, size_t part_base) {
+    if (*J.stopped) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = J.n, logn = J.logn, Tn = J.tile;
+    const int ldp = tile_ldp<T>(n);
+    cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* buf1 = buf0 + Tn * ldp;
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(buf1 + Tn * ldp);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    size_t stride = 1;
+    for (int a = axis + 1; a < J.d; ++a) stride *= (size_t)n;
+    const size_t tiles_per_outer = stride / Tn;
+    const size_t outer = blockIdx.x / tiles_per_outer, inner0 = (blockIdx.x % tiles_per_outer) * Tn;
+    const size_t c0 = outer * stride * n + inner0;
+    cx<T>* data = ((mode & TM_PHI) ? J.phi : J.psi) + (size_t)blockIdx.y * J.N;
+    for (int e = threadIdx.x; e < n * Tn; e += blockDim.x) { // coalesced rows of Tn elements
+        const int t = e / Tn, c = e - t * Tn;
+        buf0[c * ldp + padx<T>(t)] = data[c0 + (size_t)t * stride + c];
+    }
+    __syncthreads();
+    Acc acc[NDV];
+    TileHook<T> h{&J, acc, NdSlots{J.d, J.S}, mode, c0, stride};
+    cx<T>* cur = buf0;
+    if (mode & TM_FWD) {
+        cx<T>* oth = cur == buf0 ? buf1 : buf0;
+        if (mode & (TM_KPHASE | TM_KOBS)) cur = tfft<T, 1, -1, false, true>(cur, oth, ldp, logn, twm, Tn, h);
+        else cur = tfft<T, 1, -1, false, false>(cur, oth, ldp, logn, twm, Tn, h);
+    }
+    if (mode & TM_KOBS) {
+        block_partials(acc, NdSlots{J.d, J.S}.count(), J.part, part_base + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
+        return;
+    }
+    if (mode & TM_INV) {
+        NdNoHook none;
+        cur = tfft<T, 1, 1, false, false>(cur, cur == buf0 ? buf1 : buf0, ldp, logn, twm, Tn, none);
+    }
+    for (int e = threadIdx.x; e < n * Tn; e += blockDim.x) {
+        const int t = e / Tn, c = e - t * Tn;
+        data[c0 + (size_t)t * stride + c] = cur[c * ldp + padx<T>(t)];
+    }
+}
+
+// ------------------------------------------------------------ setup, imaginary time, bookkeeping
+// V(r, t), eigh, R (with_R) and cap weights at every grid point (wavepacket.zig:96-168,
+// quantum_dynamics.zig:387-468); no sign continuity in more than one dimension
+template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double t, int with_R) {
+    if (*J.stopped) return;
+    const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (g >= J.N) return;
+    double r[3];
+    grid_coords(J, g, r);
+    double Vl[S * S], Vu[S * S], Wl[S], Ul[S * S];
+    pot_eval(J.pot, r, t, Vl);
+    for (int a = 0; a < S; ++a)
+        for (int b = 0; b < S; ++b) Vu[a * S + b] = Vl[(a < b ? a : b) * S + (a < b ? b : a)];
+    eigh_dev<S>(Vu, Wl, Ul);
+    for (int e = 0; e < S * S; ++e) J.V[(size_t)e * J.N + g] = Vl[e];
+    if (S > 1)
+        for (int e = 0; e < S * S; ++e) J.U[(size_t)e * J.N + g] = Ul[e];
+    if (!with_R) return;
+    double cap_sum = 0;
+    if (J.has_cap)
+        for (int j = 0; j < J.d; ++j) {
+            const double dist = fmax(0.0, fmax(J.cap_lo[j] - r[j], r[j] - J.cap_hi[j]));
+            if (dist > 0) cap_sum = __dadd_rn(cap_sum, exp(__dmul_rn(J.cap_exp, dist)) - 1);
+        }
+    const double decay = exp(__dmul_rn(__dmul_rn(-0.5, cap_sum), hypot(J.dt_re, J.dt_im)));
+    if (J.capw) J.capw[g] = 1 - decay * decay;
+    int k = 0;
+    for (int a = 0; a < S; ++a)
+        for (int b = a; b < S; ++b) {
+            double re, im;
+            propagator_entry<S>(Wl, Ul, J.dt_re, J.dt_im, decay, a, b, re, im);
+            J.R[(size_t)k * J.N + g] = mktab<T>(re, im);
+            ++k;
+        }
+}
+
+// setGaussian (wavepacket.zig:355-371) and the partial norms
+template <typename T> __global__ void nd_gauss_kernel(NdJob<T> J, size_t part_base) {
+    Acc acc[NDV];
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
+        double r[3];
+        grid_coords(J, g, r);
+        double ere = 0, eim = 0;
+        for (int j = 0; j < J.d; ++j) {
+            const double dx = __dsub_rn(r[j], J.x0[j]);
+            ere = __dadd_rn(ere, __dmul_rn(__dmul_rn(__dmul_rn(-0.5, J.gamma[j]), dx), dx));
+            eim = __dadd_rn(eim, __dmul_rn(J.p0[j], dx));
+        }
+        double zr, zi;
+        cexp_dev(ere, eim, zr, zi);
+        for (int s = 0; s < J.S; ++s) {
+            const cx<T> z = s == J.ic_state ? mk<T>((T)zr, (T)zi) : mk<T>(0, 0);
+            J.psi[(size_t)s * J.N + g] = z;
+            acc[0].add((double)z.x * (double)z.x + (double)z.y * (double)z.y);
+        }
+    }
+    block_partials(acc, 1, J.part, part_base + blockIdx.x);
+}
+
+// psi /= sqrt(norm) (Complex.div by (s, 0), wavepacket.zig:282-284); optionally toDia and the acf reference
+template <typename T, int S>
+__global__ void nd_normalize_kernel(NdJob<T> J, size_t p0, size_t p1, int to_dia, int save_psi0) {
+    if (*J.stopped) return;
+    __shared__ double sq_sh;
+    if (threadIdx.x == 0) sq_sh = sqrt(sum_partials(J.part, p0, p1, 0).value() * J.dr);
+    __syncthreads();
+    const double sq = sq_sh, den = sq * sq;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
+        cx<T> x[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const cx<T> z = J.psi[(size_t)s * J.N + g];
+            x[s] = mk<T>((T)((double)z.x * sq / den), (T)((double)z.y * sq / den));
+        }
+        if (to_dia && S > 1) { // toDia (wavepacket.zig:398-419)
+            cx<T> y[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                double re = 0, im = 0;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const double u = J.U[(size_t)(i * S + k) * J.N + g];
+                    re += (double)x[k].x * u;
+                    im += (double)x[k].y * u;
+                }
+                y[i] = mk<T>((T)re, (T)im);
+            }
+#pragma unroll
+            for (int i = 0; i < S; ++i) x[i] = y[i];
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            J.psi[(size_t)s * J.N + g] = x[s];
+            if (save_psi0) J.psi0[(size_t)s * J.N + g] = x[s];
+        }
+    }
+}
+
+// partial sums of |psi|^2 (slot 0) or of <phi_o|psi> (slots 0, 1)
+template <typename T> __global__ void nd_dot_kernel(NdJob<T> J, int o, size_t part_base) {
+    if (*J.stopped) return;
+    Acc acc[NDV];
+    const cx<T>* ph = o >= 0 ? J.orth + (size_t)o * J.S * J.N : nullptr;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)J.S * J.N;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const cx<T> z = J.psi[e];
+        if (ph) {
+            const cx<T> p = ph[e];
+            acc[0].add((double)p.x * (double)z.x + (double)p.y * (double)z.y);
+            acc[1].add((double)p.x * (double)z.y - (double)p.y * (double)z.x);
+        } else {
+            acc[0].add((double)z.x * (double)z.x + (double)z.y * (double)z.y);
+        }
+    }
+    block_partials(acc, ph ? 2 : 1, J.part, part_base + blockIdx.x);
+}
+
+// psi -= <phi_o|psi> dr phi_o (quantum_dynamics.zig:898-904)
+template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, size_t p0, size_t p1) {
+    if (*J.stopped) return;
+    __shared__ double ov[2];
+    if (threadIdx.x < 2) ov[threadIdx.x] = sum_partials(J.part, p0, p1, threadIdx.x).value() * J.dr;
+    __syncthreads();
+    const double ore = ov[0], oim = ov[1];
+    const cx<T>* ph = J.orth + (size_t)o * J.S * J.N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)J.S * J.N;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const cx<T> p = ph[e], z = J.psi[e];
+        J.psi[e] = mk<T>((T)((double)z.x - (ore * (double)p.x - oim * (double)p.y)),
+                         (T)((double)z.y - (ore * (double)p.y + oim * (double)p.x)));
+    }
+}
+
+// Sums the step's partials (fixed order), assembles the observables row, updates the
+// absorbed populations and stop flag.  part ranges: [x0, x1) position-space and
+// absorbed sums of the row passes, [k0, k1) momentum-space sums of the tile pass.
+// kind 0: the row of a step; 1: the final observables (no bookkeeping);
+// 2: only record the absorbed sums of the next step's first accumAbsorbed.
+struct NdBook {
+    double pop_abs[4];
+    double carry[4]; // absorbed sums of the next step's first accumAbsorbed
+};
+template <typename T>
+__global__ void nd_finalize_kernel(NdJob<T> J, size_t x0, size_t x1, size_t k0, size_t k1, uint32_t mask,
+                                   double* row, NdBook* book, int* rows_out, int row_index, int has_stop,
+                                   double stop_norm, int kind) {
+    if (kind != 1 && *J.stopped) return;
+    __shared__ double out[NDV];
+    const NdSlots sl{J.d, J.S};
+    if (threadIdx.x < sl.count()) {
+        const int v = threadIdx.x;
+        const bool kslot = v >= sl.mom() && v <= sl.ekin();
+        out[v] = kslot ? (k1 > k0 ? sum_partials(J.part, k0, k1, v).value() : 0.0) : sum_partials(J.part, x0, x1, v).value();
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    if (kind == 2) {
+        for (int s = 0; s < J.S; ++s) book->carry[s] = out[sl.absn() + s];
+        return;
+    }
+    const RowLayout L{J.d, J.S};
+    const bool c_pos = mask & WM_POS, c_mom = mask & WM_MOM, c_pop = mask & WM_POP;
+    const bool c_ekin = (mask & WM_EKIN) || (mask & WM_ETOT), c_epot = (mask & WM_EPOT) || (mask & WM_ETOT);
+    const bool c_norm = (mask & WM_NORM) || has_stop, c_acf = mask & WM_ACF;
+    if (kind == 0)
+        for (int s = 0; s < J.S; ++s) { // accumAbsorbed adds sum * dr twice per step (quantum_dynamics.zig:497)
+            book->pop_abs[s] += book->carry[s] * J.dr;
+            book->pop_abs[s] += out[sl.abs() + s] * J.dr;
+            book->carry[s] = out[sl.absn() + s];
+        }
+    const double norm = out[sl.norm()] * J.dr;
+    row[L.norm()] = c_norm ? norm : nan("");
+    for (int k = 0; k < J.d; ++k) {
+        row[L.pos() + k] = c_pos ? out[sl.pos() + k] * J.dr : nan("");
+        row[L.mom() + k] = c_mom ? out[sl.mom() + k] * J.dk : nan("");
+    }
+    for (int s = 0; s < J.S; ++s) row[L.pop() + s] = c_pop ? out[sl.pop() + s] * J.dr + book->pop_abs[s] : nan("");
+    row[L.epot()] = c_epot ? out[sl.epot()] * J.dr : nan("");
+    row[L.ekin()] = c_ekin ? out[sl.ekin()] * J.dk : nan("");
+    row[L.acf()] = c_acf ? out[sl.acf()] * J.dr : nan("");
+    row[L.acf() + 1] = c_acf ? out[sl.acf() + 1] * J.dr : nan("");
+    if (kind == 0) {
+        *rows_out = row_index + 1;
+        if (has_stop && norm < stop_norm) *J.stopped = 1;
+    }
+}
+
+} // namespace zqd
