@@ -45,10 +45,12 @@ struct zqd_job {
     zqd::DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
     zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
+    cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     float last_ms = 0;
     size_t device_bytes = 0;
     uint64_t h2d = 0, d2h = 0; // bytes copied by this job
     ~zqd_job() {
+        if (nd_graph) cudaGraphExecDestroy(nd_graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);

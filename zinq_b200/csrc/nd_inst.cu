@@ -64,9 +64,12 @@ NdJob<T> describe(zqd_job* J) {
     D.U = J->U.as<double>();
     D.capw = J->capw.as<double>();
     D.tw = J->tw.as<Tab<T>>();
+    D.kphase = J->expk.as<double2>();
     D.part = J->part.as<double>();
+    D.nparts = J->part.bytes / (NDV * 2 * sizeof(double));
     D.rows_per_cta = J->nd_rows;
     D.tile = J->nd_tile;
+    while ((1 << D.logtile) < J->nd_tile) ++D.logtile;
     D.stopped = J->flags.as<int>();
     D.pot = J->pot.dev;
     return D;
@@ -84,7 +87,8 @@ struct Launch {
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
         const int nbuf = (mode & RM_PHI) ? 3 : 2;
         const size_t smem = nd_smem_bytes<T>(nbuf, S * J->nd_rows, J->n);
-        nd_row_kernel<T, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
+        if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
+        else nd_row_kernel<T, 3, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -92,7 +96,9 @@ struct Launch {
         NdJob<T> d = D;
         if (nostop) d.stopped = J->flags.as<int>() + 1;
         const size_t smem = nd_smem_bytes<T>(2, J->nd_tile, J->n);
-        nd_tile_kernel<T><<<dim3((unsigned)ntile_blocks, S), J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
+        const dim3 grid((unsigned)ntile_blocks, S);
+        if (D.d == 2) nd_tile_kernel<T, 2><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
+        else nd_tile_kernel<T, 3><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -104,6 +110,13 @@ struct Launch {
         if ((rc = tile(0, TM_FWD | TM_KPHASE | TM_INV, 0))) return rc;
         for (int a = 1; a <= D.d - 2; ++a)
             if ((rc = tile(a, TM_INV, 0))) return rc;
+        return ZQD_OK;
+    }
+    double* scal() const { return J->book.as<NdBook>()->scal; }
+    // scalar sums of slots [0, nv) over partial blocks [b0, b1) into scal()
+    int reduce(size_t b0, size_t b1, int nv) {
+        nd_reduce_kernel<<<1, 32 * nv, 0, J->stream>>>(D.part, D.nparts, b0, b1, nv, D.stopped, scal());
+        ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
     // momentum observables of phi (the forward transform along the last axis is already done)
@@ -121,19 +134,24 @@ int ZQD_ND_CREATE(zqd_job* J) {
     const size_t N = J->N, c = sizeof(cx<T>), tb = sizeof(Tab<T>);
     const Opts& o = J->o;
     const int n = J->n;
-    // launch shapes: rows per CTA so a CTA has ~128 threads and fits in shared memory
-    const int budget = 200 * 1024;
-    const bool any_k = true; // the final observables always need the momentum-space round trip
-    J->nd_row_bufs = any_k ? 3 : 2;
-    int L = std::max(1, std::min<int>((int)(N / n), 1024 / n));
-    while (L > 1 && nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget) L >>= 1;
+    // Launch shapes.  Row pass: L rows (all S states) per CTA, about 2048 points a CTA, at
+    // least two CTAs per SM where the grid allows, within the shared-memory budget (three
+    // line buffers: the final observables always need the momentum-space copy).
+    // Tile pass: Tn lines per CTA, rows of Tn * c >= 32 bytes (one sector), shrunk from
+    // 128 bytes until the grid has two CTAs per SM.
+    const int budget = 200 * 1024, sms2 = 2 * 148;
+    J->nd_row_bufs = 3;
+    int L = std::max(1, std::min<int>((int)(N / n), 2048 / (S * n)));
+    while (L > 1 && (N / n / L < (size_t)sms2 || nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget)) L >>= 1;
     if (nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget)
-        return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS (npoint at most 1024 per axis)");
+        return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS");
     J->nd_rows = L;
-    J->nd_row_threads = std::max(32, std::min(512, (L * n / 8 + 31) / 32 * 32));
-    int Tn = std::min(n, (int)(128 / c)); // 128-byte rows of the tile
-    while (Tn > 1 && Tn * n / 8 > 512) Tn >>= 1;
-    while (Tn > 1 && nd_smem_bytes<T>(2, Tn, n) > (size_t)budget) Tn >>= 1;
+    J->nd_row_threads = std::max(32, std::min(512, (S * L * n / 8 + 31) / 32 * 32));
+    const int tmin = std::max(1, (int)(32 / c));
+    int Tn = std::min(n, (int)(128 / c));
+    while (Tn > tmin && ((size_t)S * (N / n / Tn) < (size_t)sms2 || Tn * n / 8 > 512 ||
+                         nd_smem_bytes<T>(2, Tn, n) > (size_t)budget)) Tn >>= 1;
+    if (nd_smem_bytes<T>(2, Tn, n) > (size_t)budget) return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE TILE PASS");
     J->nd_tile = Tn;
     J->nd_tile_threads = std::max(32, std::min(512, (Tn * n / 8 + 31) / 32 * 32));
     const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
@@ -148,6 +166,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
     if (S > 1 && (rc = J->U.alloc((size_t)S * S * N * sizeof(double)))) return rc;
     if (o.has_cap && (rc = J->capw.alloc(N * sizeof(double)))) return rc;
     if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
+    if ((rc = J->expk.alloc((size_t)J->d * n * sizeof(double2)))) return rc;
     if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
     if ((rc = J->book.alloc(sizeof(NdBook)))) return rc;
     if ((rc = J->flags.alloc(2 * sizeof(int)))) return rc;
@@ -167,13 +186,19 @@ int ZQD_ND_CREATE(zqd_job* J) {
     NdJob<T> D = describe(J);
     nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(D, 0.0, 1);
     ZQD_CUDA(cudaGetLastError());
-    for (auto f : {nd_row_kernel<T, S>}) ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
-    ZQD_CUDA(cudaFuncSetAttribute(nd_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+    nd_kphase_kernel<T><<<(unsigned)((J->d * n + 127) / 128), 128, 0, J->stream>>>(D, J->expk.as<double2>());
+    ZQD_CUDA(cudaGetLastError());
+    for (auto f : {nd_row_kernel<T, 2, S>, nd_row_kernel<T, 3, S>})
+        ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+    for (auto f : {nd_tile_kernel<T, 2>, nd_tile_kernel<T, 3>})
+        ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     return ZQD_OK;
 }
 
-int ZQD_ND_RUN(zqd_job* J) {
+namespace {
+// every launch of a run, in stream order (captured into a graph by ZQD_ND_RUN)
+int enqueue(zqd_job* J) {
     const Opts& o = J->o;
     Launch Lc{J, describe(J)};
     const size_t N = J->N;
@@ -191,7 +216,6 @@ int ZQD_ND_RUN(zqd_job* J) {
     const size_t SN = (size_t)S * N * sizeof(cx<T>);
     const unsigned ng = (unsigned)Lc.ngrid;
     int rc;
-    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
     for (int s = 0; s < J->nsolve; ++s) {
         Lc.D.orth = J->orth.as<cx<T>>();
         double* hist = J->hist.as<double>() + (size_t)s * (iters + 1) * HC;
@@ -201,28 +225,32 @@ int ZQD_ND_RUN(zqd_job* J) {
         // setGaussian, normalise, toDia, acf reference (quantum_dynamics.zig:867-882)
         nd_gauss_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G);
         ZQD_CUDA(cudaGetLastError());
-        nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G, Lc.G + ng, o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
+        if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc;
+        nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
         ZQD_CUDA(cudaGetLastError());
         auto finalize = [&](size_t x0, size_t x1, bool k, uint32_t mask, int i) -> int {
-            nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, x0, x1, Lc.K, k ? Lc.K + S * Lc.ntile_blocks : Lc.K, mask,
+            nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, x0, x1, Lc.K, k ? Lc.K + S * Lc.ntile_blocks : Lc.K, mask,
                                                           hist + (size_t)i * HC, J->book.as<NdBook>(), rows_out, i,
                                                           o.has_cap && o.cap_has_stop, o.cap_stop_norm, 0);
             ZQD_CUDA(cudaGetLastError());
             return ZQD_OK;
         };
         auto carry = [&](size_t r0, size_t r1) -> int { // absorbed sums of the next step's start
-            nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, r0, r1, Lc.K, Lc.K, 0, J->fin.as<double>() + (size_t)s * HC,
+            nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, r0, r1, Lc.K, Lc.K, 0, J->fin.as<double>() + (size_t)s * HC,
                                                           J->book.as<NdBook>(), rows_out, 0, 0, 0.0, 2);
             ZQD_CUDA(cudaGetLastError());
             return ZQD_OK;
         };
         auto itp_ops = [&]() -> int { // quantum_dynamics.zig:898-906
+            int rc2;
             for (int j = 0; j < s; ++j) {
                 nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G);
-                nd_orth_apply_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G, Lc.G + ng);
+                if ((rc2 = Lc.reduce(Lc.G, Lc.G + ng, 2))) return rc2;
+                nd_orth_apply_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.scal());
             }
             nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, -1, Lc.G);
-            nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G, Lc.G + ng, 0, 0);
+            if ((rc2 = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc2;
+            nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), 0, 0);
             ZQD_CUDA(cudaGetLastError());
             return ZQD_OK;
         };
@@ -242,14 +270,14 @@ int ZQD_ND_RUN(zqd_job* J) {
             } else {
                 if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
                 if (o.imag_nstate && (rc = itp_ops())) return rc; // every i, the initial state included
-                if (i == 0) ZQD_CUDA(cudaMemsetAsync(Lc.D.part, 0, Lc.nrow_blocks * NDV * 2 * sizeof(double), J->stream));
                 if (o.pot_td) {
                     nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, (double)i * o.time_step, 0);
                     ZQD_CUDA(cudaGetLastError());
                 }
                 if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1))) return rc;
                 if (needk && (rc = Lc.kobs())) return rc;
-                if ((rc = finalize(Lc.R0, Lc.R1 + Lc.nrow_blocks, needk, mask, i))) return rc;
+                // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
+                if ((rc = finalize(i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, i))) return rc;
                 if (i < iters) {
                     if (o.pot_td) {
                         nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, ((double)i + 0.5) * o.time_step, 1);
@@ -264,13 +292,37 @@ int ZQD_ND_RUN(zqd_job* J) {
         const uint32_t all = WM_ALL_OBS | (acf ? (uint32_t)WM_ACF : 0u);
         if ((rc = Lc.row(RM_OBS | RM_PHI, all, Lc.R1, true))) return rc;
         if ((rc = Lc.kobs(true))) return rc;
-        nd_finalize_kernel<T><<<1, 32, 0, J->stream>>>(Lc.D, Lc.R1, Lc.R1 + Lc.nrow_blocks, Lc.K, Lc.K + S * Lc.ntile_blocks,
+        nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, Lc.R1, Lc.R1 + Lc.nrow_blocks, Lc.K, Lc.K + S * Lc.ntile_blocks,
                                                       all, J->fin.as<double>() + (size_t)s * HC, J->book.as<NdBook>(),
                                                       rows_out, 0, 0, 0.0, 1);
         ZQD_CUDA(cudaGetLastError());
         if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)
             ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice, J->stream));
     }
+    return ZQD_OK;
+}
+} // namespace
+
+// A run is a fixed sequence of launches: it is captured into a CUDA graph on the
+// first call and the graph is replayed by every later call on the job.
+int ZQD_ND_RUN(zqd_job* J) {
+    if (!J->nd_graph) {
+        ZQD_CUDA(cudaStreamBeginCapture(J->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(J);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(J->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        ZQD_CUDA(e);
+        const cudaError_t ei = cudaGraphInstantiate(&J->nd_graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) J->nd_graph = nullptr;
+        ZQD_CUDA(ei);
+    }
+    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+    ZQD_CUDA(cudaGraphLaunch(J->nd_graph, J->stream));
     ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));

@@ -58,9 +58,11 @@ template <typename T> struct NdJob {
     double* U;    // [S*S][N]
     double* capw; // [N]
     const Tab<T>* tw; // [n] exp(-2 pi i t / n)
-    double* part;     // per-CTA partial sums [blocks][NDV][2]
+    const double2* kphase; // [D][n] exp(Complex(0, -k^2 / (2 m_j)) * dt) of axis j
+    double* part;     // per-CTA partial sums, slot-major: [NDV][nparts][2]
+    size_t nparts;
     int rows_per_cta; // row pass: rows of the last axis per CTA
-    int tile;         // tile pass: lines per CTA
+    int tile, logtile; // tile pass: lines per CTA (a power of two) and its log2
     int* stopped;     // set by the finalize kernel when stop_norm ends the solve
     PotDev pot;
 };
@@ -85,9 +87,12 @@ enum : uint32_t {
 };
 
 template <typename T> __host__ __device__ inline int tile_ldp(int n) { return padded_len<T>(n) | 1; }
-// dynamic shared memory: nbuf line buffers of `lines` lines + the twiddle table
+// dynamic shared memory: nbuf line buffers of `lines` lines, then the twiddle table on a 16-byte boundary
+template <typename T> __host__ __device__ inline size_t nd_tw_offset(int nbuf, int lines, int n) {
+    return ((size_t)nbuf * lines * tile_ldp<T>(n) * sizeof(cx<T>) + 15) & ~(size_t)15;
+}
 template <typename T> __host__ __device__ inline size_t nd_smem_bytes(int nbuf, int lines, int n) {
-    return (size_t)nbuf * lines * tile_ldp<T>(n) * sizeof(cx<T>) + (size_t)n * sizeof(Tab<T>);
+    return nd_tw_offset<T>(nbuf, lines, n) + (size_t)n * sizeof(Tab<T>);
 }
 
 template <typename T> __device__ __forceinline__ void grid_coords(const NdJob<T>& J, size_t gidx, double* r) {
@@ -187,88 +192,145 @@ struct NdNoHook {
     template <int R, typename V> __device__ __forceinline__ void last(int, int, int, V&) {}
 };
 
-// per-CTA reduction of nv compensated sums into part[block][NDV][2] (fixed order)
-__device__ __forceinline__ void block_partials(Acc (&a)[NDV], int nv, double* __restrict__ part, size_t block) {
-    __shared__ double red[16][NDV][2];
+// slot indices of the reductions for a (D, S) pair, compile-time (same order as NdSlots)
+template <int D, int S> struct Slots {
+    static constexpr int norm = 0, pos = 1, epot = 1 + D, acf = 2 + D, mom = 4 + D, ekin = 4 + 2 * D, pop = 5 + 2 * D,
+                         abs = 5 + 2 * D + S, absn = 5 + 2 * D + 2 * S, count = 5 + 2 * D + 3 * S;
+};
+
+// per-CTA reduction of NV compensated sums into slots [first, first + NV) of the
+// slot-major partial array part[NDV][P][2], at column `block` (fixed order)
+template <int NV>
+__device__ __forceinline__ void block_partials(const double (&a)[NV], int first, double* __restrict__ part, size_t P,
+                                               size_t block) {
+    __shared__ double red[16][NV][2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
-    for (int v = 0; v < NDV; ++v) {
-        if (v < nv) {
-            double s = a[v].s, c = a[v].c;
+    for (int v = 0; v < NV; ++v) {
+        double s = a[v], c = 0.0; // a thread's plain sum over its few points, then compensated combination
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double s2 = __shfl_down_sync(0xffffffffu, s, off), c2 = __shfl_down_sync(0xffffffffu, c, off);
-                Acc t;
-                t.s = s;
-                t.c = c;
-                t.add(s2);
-                t.c += c2;
-                s = t.s;
-                c = t.c;
-            }
-            if (lane == 0) {
-                red[warp][v][0] = s;
-                red[warp][v][1] = c;
-            }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double s2 = __shfl_down_sync(0xffffffffu, s, off), c2 = __shfl_down_sync(0xffffffffu, c, off);
+            Acc t;
+            t.s = s;
+            t.c = c;
+            t.add(s2);
+            t.c += c2;
+            s = t.s;
+            c = t.c;
+        }
+        if (lane == 0) {
+            red[warp][v][0] = s;
+            red[warp][v][1] = c;
         }
     }
     __syncthreads();
-    if (threadIdx.x < nv) {
+    if (threadIdx.x < NV) {
         Acc t;
         for (int w = 0; w < nw; ++w) {
             t.add(red[w][threadIdx.x][0]);
             t.c += red[w][threadIdx.x][1];
         }
-        part[(block * NDV + threadIdx.x) * 2] = t.s;
-        part[(block * NDV + threadIdx.x) * 2 + 1] = t.c;
+        const size_t o = ((size_t)(first + threadIdx.x) * P + block) * 2;
+        part[o] = t.s;
+        part[o + 1] = t.c;
     }
     __syncthreads();
 }
 
-// sum of slot v over partial blocks [b0, b1) in block order
-__device__ __forceinline__ Acc sum_partials(const double* __restrict__ part, size_t b0, size_t b1, int v) {
+// Sum of slot v over partial blocks [b0, b1), computed by one whole warp: lane l
+// takes blocks b0 + l, b0 + l + 32, ... in order, then a fixed butterfly; the
+// result (identical in every lane) does not depend on timing.
+__device__ __forceinline__ double warp_sum_partials(const double* __restrict__ part, size_t P, size_t b0, size_t b1,
+                                                    int v) {
+    const int lane = threadIdx.x & 31;
+    const double2* __restrict__ src = reinterpret_cast<const double2*>(part) + (size_t)v * P;
     Acc t;
-    for (size_t b = b0; b < b1; ++b) {
-        t.add(part[(b * NDV + v) * 2]);
-        t.c += part[(b * NDV + v) * 2 + 1];
+    size_t b = b0 + lane;
+    for (; b + 96 < b1; b += 128) { // four independent loads in flight
+        const double2 x0 = src[b], x1 = src[b + 32], x2 = src[b + 64], x3 = src[b + 96];
+        t.add(x0.x);
+        t.c += x0.y;
+        t.add(x1.x);
+        t.c += x1.y;
+        t.add(x2.x);
+        t.c += x2.y;
+        t.add(x3.x);
+        t.c += x3.y;
     }
-    return t;
+    for (; b < b1; b += 32) {
+        const double2 x = src[b];
+        t.add(x.x);
+        t.c += x.y;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double s2 = __shfl_xor_sync(0xffffffffu, t.s, off), c2 = __shfl_xor_sync(0xffffffffu, t.c, off);
+        // combine in lane order so both partners compute the same value
+        Acc u;
+        if (lane & off) {
+            u.s = s2;
+            u.c = c2;
+            u.add(t.s);
+            u.c += t.c;
+        } else {
+            u.s = t.s;
+            u.c = t.c;
+            u.add(s2);
+            u.c += c2;
+        }
+        t = u;
+    }
+    return t.value();
+}
+
+// scalars for the imaginary-time kernels: out[v] = sum of slot v over [b0, b1), v < nv (one warp per slot)
+static __global__ void nd_reduce_kernel(const double* __restrict__ part, size_t P, size_t b0, size_t b1, int nv,
+                                        const int* stopped, double* __restrict__ out) {
+    if (*stopped) return;
+    const int w = threadIdx.x >> 5;
+    if (w >= nv) return;
+    const double v = warp_sum_partials(part, P, b0, b1, w);
+    if ((threadIdx.x & 31) == 0) out[w] = v;
+}
+
+// index of grid point g along axis j (last axis fastest; n = 2^logn)
+template <int D> __device__ __forceinline__ int axis_index(size_t g, int j, int logn) {
+    return (int)(g >> (logn * (D - 1 - j))) & ((1 << logn) - 1);
 }
 
 // ------------------------------------------------------------ row pass
-template <typename T, int S> struct RowHook {
-    const NdJob<T>* J;
-    Acc* acc;
-    NdSlots sl;
-    uint32_t mode, obs; // obs: WM_* bits wanted by RM_OBS
-    size_t row0;        // first grid point of the CTA's rows
-    int n;
-    T last_scale;       // 1/N after an inverse transform, 1 otherwise
-
-    __device__ __forceinline__ void absorbed(const cx<T>* x, size_t gidx, int slot) {
-        const double w = J->capw[gidx];
+// accumAbsorbed at one grid point into slots [SLOT, SLOT + S) (quantum_dynamics.zig:470-500)
+template <typename T, int S, int SLOT, int NV>
+__device__ __forceinline__ void nd_absorbed(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, double (&acc)[NV]) {
+    const double w = J.capw[g];
 #pragma unroll
-        for (int i = 0; i < S; ++i) {
-            double are = 0, aim = 0;
-            if (J->adiabatic && S > 1) {
+    for (int i = 0; i < S; ++i) {
+        double are = 0, aim = 0;
+        if (J.adiabatic && S > 1) {
 #pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    const double u = J->U[(size_t)(k * S + i) * J->N + gidx];
-                    are += (double)x[k].x * u;
-                    aim += (double)x[k].y * u;
-                }
-            } else {
-                are = (double)x[i].x;
-                aim = (double)x[i].y;
+            for (int k = 0; k < S; ++k) {
+                const double u = J.U[(size_t)(k * S + i) * J.N + g];
+                are += (double)x[k].x * u;
+                aim += (double)x[k].y * u;
             }
-            acc[slot + i].add(w * (are * are + aim * aim));
+        } else {
+            are = (double)x[i].x;
+            aim = (double)x[i].y;
         }
+        acc[SLOT + i] += w * (are * are + aim * aim);
     }
-    __device__ __forceinline__ void apply_r(cx<T>* x, size_t gidx) const {
-        constexpr int NSYM = S * (S + 1) / 2;
-        Tab<T> r[NSYM];
+}
+
+// the CTA's R entries of one point (complex symmetric, upper triangle stored)
+template <typename T, int S> struct RPoint {
+    Tab<T> r[S * (S + 1) / 2];
+    __device__ __forceinline__ void load(const NdJob<T>& J, size_t g) {
 #pragma unroll
-        for (int c = 0; c < NSYM; ++c) r[c] = J->R[(size_t)c * J->N + gidx];
+        for (int c = 0; c < S * (S + 1) / 2; ++c) r[c] = J.R[(size_t)c * J.N + g];
+    }
+    // psi <- R psi (Propagator.applyR, quantum_dynamics.zig:501-520)
+    __device__ __forceinline__ void apply(cx<T> (&x)[S]) const {
         cx<T> y[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) {
@@ -283,205 +345,223 @@ template <typename T, int S> struct RowHook {
 #pragma unroll
         for (int i = 0; i < S; ++i) x[i] = y[i];
     }
-    __device__ __forceinline__ void observe(const cx<T>* x, size_t gidx) {
-        double m2 = 0;
-        const bool adia = J->adiabatic && S > 1;
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            const double w = (double)x[s].x * (double)x[s].x + (double)x[s].y * (double)x[s].y;
-            m2 += w;
-            if ((obs & WM_POP) && !adia) acc[sl.pop() + s].add(w);
-        }
-        acc[sl.norm()].add(m2);
-        if (obs & WM_POS) {
-            double r[3];
-            grid_coords(*J, gidx, r);
-            for (int k = 0; k < J->d; ++k) acc[sl.pos() + k].add(m2 * r[k]);
-        }
-        if (obs & (WM_EPOT | WM_ETOT)) {
-            double e = 0;
-#pragma unroll
-            for (int i = 0; i < S; ++i)
-#pragma unroll
-                for (int k = 0; k < S; ++k)
-                    e += ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) *
-                         J->V[(size_t)(i * S + k) * J->N + gidx];
-            acc[sl.epot()].add(e);
-        }
-        if (obs & WM_ACF) {
-            double re = 0, im = 0;
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const cx<T> z0 = J->psi0[(size_t)s * J->N + gidx];
-                re += (double)z0.x * (double)x[s].x + (double)z0.y * (double)x[s].y;
-                im += (double)z0.x * (double)x[s].y - (double)z0.y * (double)x[s].x;
-            }
-            acc[sl.acf()].add(re);
-            acc[sl.acf() + 1].add(im);
-        }
-        if ((obs & WM_POP) && adia) {
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                double are = 0, aim = 0;
-#pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    const double u = J->U[(size_t)(k * S + i) * J->N + gidx];
-                    are += (double)x[k].x * u;
-                    aim += (double)x[k].y * u;
-                }
-                acc[sl.pop() + i].add(are * are + aim * aim);
-            }
-        }
-    }
-    // first pass of the forward transform: start of the next step
-    template <int R> __device__ __forceinline__ void first(int g, int i, int mr, cx<T> (&v)[S][R]) {
-        if (!(mode & RM_RSTART)) return;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const size_t gidx = row0 + (size_t)g * n + i + r * mr;
-            cx<T> x[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) x[s] = v[s][r];
-            if (J->track) absorbed(x, gidx, sl.absn());
-            apply_r(x, gidx);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s][r] = x[s];
-        }
-    }
-    // last pass of the inverse transform (or a pass of its own): end of the step
-    template <int R> __device__ __forceinline__ void last(int g, int o0, int p, cx<T> (&v)[S][R]) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const size_t gidx = row0 + (size_t)g * n + o0 + r * p;
-            cx<T> x[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) x[s] = scale<T>(v[s][r], last_scale);
-            if (mode & RM_REND) {
-                if (J->track) absorbed(x, gidx, sl.abs());
-                apply_r(x, gidx);
-            }
-            if (mode & RM_OBS) observe(x, gidx);
-#pragma unroll
-            for (int s = 0; s < S; ++s) v[s][r] = x[s];
-        }
-    }
 };
 
-// rows_per_cta rows (of every state) per CTA; `mode` selects the stages
-template <typename T, int S>
-__global__ void __launch_bounds__(512) nd_row_kernel(NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base) {
+// position-space observables at one point (Observables.init, quantum_dynamics.zig:300-360;
+// Wavefunction.norm/pos/pop/epot, wavepacket.zig:206-300)
+template <typename T, int D, int S, int NV>
+__device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, uint32_t obs, double (&acc)[NV]) {
+    using SL = Slots<D, S>;
+    double m2 = 0;
+    const bool adia = J.adiabatic && S > 1;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const double w = (double)x[s].x * (double)x[s].x + (double)x[s].y * (double)x[s].y;
+        m2 += w;
+        if ((obs & WM_POP) && !adia) acc[SL::pop + s] += w;
+    }
+    acc[SL::norm] += m2;
+    if (obs & WM_POS) {
+#pragma unroll
+        for (int j = 0; j < D; ++j) { // Grid.init coordinate (wavepacket.zig:55-74)
+            const double r = __dadd_rn(J.lo[j], __dmul_rn((double)axis_index<D>(g, j, J.logn), J.span[j]) / (double)J.n);
+            acc[SL::pos + j] += m2 * r;
+        }
+    }
+    if (obs & (WM_EPOT | WM_ETOT)) { // V is symmetric: diagonal plus twice the upper triangle
+        double e = 0;
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            e += ((double)x[i].x * (double)x[i].x + (double)x[i].y * (double)x[i].y) * J.V[(size_t)(i * S + i) * J.N + g];
+#pragma unroll
+            for (int k = i + 1; k < S; ++k)
+                e += 2.0 * ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) *
+                     J.V[(size_t)(i * S + k) * J.N + g];
+        }
+        acc[SL::epot] += e;
+    }
+    if (obs & WM_ACF) {
+        double re = 0, im = 0;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            const cx<T> z0 = J.psi0[(size_t)s * J.N + g];
+            re += (double)z0.x * (double)x[s].x + (double)z0.y * (double)x[s].y;
+            im += (double)z0.x * (double)x[s].y - (double)z0.y * (double)x[s].x;
+        }
+        acc[SL::acf] += re;
+        acc[SL::acf + 1] += im;
+    }
+    if ((obs & WM_POP) && adia) {
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            double are = 0, aim = 0;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const double u = J.U[(size_t)(k * S + i) * J.N + g];
+                are += (double)x[k].x * u;
+                aim += (double)x[k].y * u;
+            }
+            acc[SL::pop + i] += are * are + aim * aim;
+        }
+    }
+}
+
+// One sweep over the CTA's points (all S states of a point in one thread):
+// end of step i     1/N (after the inverse transform), accumAbsorbed + R, observables;
+//                   the values are copied to `phi_src` when given (momentum observables)
+// start of step i+1 accumAbsorbed + R
+// R is loaded once per point for both applications.  Returns after a barrier.
+template <typename T, int D, int S, int NV>
+__device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T>* phi_src, int ldp, int L, size_t row0,
+                                             uint32_t mode, uint32_t obs, double (&acc)[NV]) {
+    using SL = Slots<D, S>;
+    const int logn = J.logn, pts = L << logn;
+    const T inv_n = (T)(1.0 / (double)J.N);
+    const bool useR = mode & (RM_REND | RM_RSTART);
+    for (int it = threadIdx.x; it < pts; it += blockDim.x) {
+        const int l = it >> logn, x = it & ((1 << logn) - 1);
+        const size_t g = row0 + it;
+        RPoint<T, S> R;
+        if (useR) R.load(J, g);
+        cx<T> v[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) v[s] = buf[(s * L + l) * ldp + padx<T>(x)];
+        if (mode & RM_INV)
+#pragma unroll
+            for (int s = 0; s < S; ++s) v[s] = scale<T>(v[s], inv_n);
+        if (mode & RM_REND) {
+            if (J.track) nd_absorbed<T, S, SL::abs>(J, v, g, acc);
+            R.apply(v);
+        }
+        if (mode & RM_OBS) nd_observe<T, D, S>(J, v, g, obs, acc);
+        if (phi_src)
+#pragma unroll
+            for (int s = 0; s < S; ++s) phi_src[(s * L + l) * ldp + padx<T>(x)] = v[s];
+        if (mode & RM_RSTART) {
+            if (J.track) nd_absorbed<T, S, SL::absn>(J, v, g, acc);
+            R.apply(v);
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) buf[(s * L + l) * ldp + padx<T>(x)] = v[s];
+    }
+    __syncthreads();
+}
+
+// L rows of the last axis (all S states) per CTA: [inverse FFT] -> sweep -> [phi] -> [forward FFT] -> store
+template <typename T, int D, int S>
+__global__ void __launch_bounds__(512)
+    nd_row_kernel(const __grid_constant__ NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base) {
     if (*J.stopped) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    using SL = Slots<D, S>;
     const int n = J.n, logn = J.logn, L = J.rows_per_cta;
-    const int ldp = tile_ldp<T>(n), lines = S * L;
+    const int ldp = tile_ldp<T>(n), lines = S * L, pts = L << logn;
     cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* buf1 = buf0 + lines * ldp;
     cx<T>* buf2 = buf1 + lines * ldp; // only with RM_PHI
-    Tab<T>* twm = reinterpret_cast<Tab<T>*>(buf0 + ((mode & RM_PHI) ? 3 : 2) * lines * ldp);
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>((mode & RM_PHI) ? 3 : 2, lines, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
-    const size_t row0 = (size_t)blockIdx.x * L * n;
-    for (int e = threadIdx.x; e < lines * n; e += blockDim.x) { // line (state s, row l) = s * L + l
-        const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
-        buf0[(s * L + l) * ldp + padx<T>(x)] = J.psi[(size_t)s * J.N + row0 + (size_t)l * n + x];
+    const size_t row0 = (size_t)blockIdx.x * pts;
+    for (int e = threadIdx.x; e < S * pts; e += blockDim.x) { // line (state s, row l) = s * L + l
+        const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
+        buf0[(s * L + l) * ldp + padx<T>(x)] = J.psi[(size_t)s * J.N + row0 + rem];
     }
     __syncthreads();
-    const NdSlots sl{J.d, S};
-    Acc acc[NDV];
-    RowHook<T, S> h{&J, acc, sl, mode, obs, row0, n, (T)(1.0 / (double)J.N)};
+    NdNoHook none;
     cx<T>* cur = buf0;
     cx<T>* oth = buf1;
     if (mode & RM_INV) {
-        cur = tfft<T, S, 1, false, true>(cur, oth, ldp, logn, twm, L, h);
+        cur = tfft<T, 1, 1, false, false>(cur, oth, ldp, logn, twm, lines, none);
         oth = cur == buf0 ? buf1 : buf0;
-    } else if (mode & (RM_REND | RM_OBS)) { // end-of-step stages without a transform
-        h.last_scale = (T)1;
-        for (int it = threadIdx.x; it < L * n; it += blockDim.x) {
-            const int l = it / n, x = it - l * n;
-            cx<T> v[S][1];
+    }
+    if (mode & (RM_INV | RM_REND | RM_OBS | RM_RSTART | RM_PHI)) {
+        double acc[SL::count];
 #pragma unroll
-            for (int s = 0; s < S; ++s) v[s][0] = cur[(s * L + l) * ldp + padx<T>(x)];
-            h.template last<1>(l, x, 1, v);
-#pragma unroll
-            for (int s = 0; s < S; ++s) cur[(s * L + l) * ldp + padx<T>(x)] = v[s][0];
+        for (int v = 0; v < SL::count; ++v) acc[v] = 0.0;
+        nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr, ldp, L, row0, mode, obs, acc);
+        if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
+    }
+    if (mode & RM_PHI) { // forward FFT of the end-of-step copy into phi
+        cx<T>* res = tfft<T, 1, -1, false, false>(oth, buf2, ldp, logn, twm, lines, none);
+        for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
+            const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
+            J.phi[(size_t)s * J.N + row0 + rem] = res[(s * L + l) * ldp + padx<T>(x)];
         }
         __syncthreads();
     }
-    if (mode & RM_PHI) { // forward FFT of a copy into phi; cur must survive for RM_RSTART
-        for (int e = threadIdx.x; e < lines * ldp; e += blockDim.x) oth[e] = cur[e];
-        __syncthreads();
-        NdNoHook none;
-        cx<T>* res = tfft<T, S, -1, false, false>(oth, buf2, ldp, logn, twm, L, none);
-        for (int e = threadIdx.x; e < lines * n; e += blockDim.x) {
-            const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
-            J.phi[(size_t)s * J.N + row0 + (size_t)l * n + x] = res[(s * L + l) * ldp + padx<T>(x)];
-        }
-        __syncthreads();
-    }
-    if (mode & RM_FWD) cur = tfft<T, S, -1, true, false>(cur, oth, ldp, logn, twm, L, h);
+    if (mode & RM_FWD) cur = tfft<T, 1, -1, false, false>(cur, oth, ldp, logn, twm, lines, none);
     if (mode & RM_STORE)
-        for (int e = threadIdx.x; e < lines * n; e += blockDim.x) {
-            const int s = e / (L * n), rem = e - s * L * n, l = rem / n, x = rem - l * n;
-            J.psi[(size_t)s * J.N + row0 + (size_t)l * n + x] = cur[(s * L + l) * ldp + padx<T>(x)];
+        for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
+            const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
+            J.psi[(size_t)s * J.N + row0 + rem] = cur[(s * L + l) * ldp + padx<T>(x)];
         }
-    if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials(acc, sl.count(), J.part, part_base + blockIdx.x);
 }
 
 // ------------------------------------------------------------ tile pass
-template <typename T> struct TileHook {
-    const NdJob<T>* J;
-    Acc* acc;
-    NdSlots sl;
+template <typename T, int D> struct TileHook {
+    const NdJob<T>& J;
+    double (&acc)[D + 1]; // mom[D], ekin
     uint32_t mode;
-    size_t c0, stride; // grid index of line g at position t along the axis: c0 + t * stride + g
+    size_t c0;
+    int lstride; // log2 of the axis stride
     template <int R> __device__ __forceinline__ void first(int, int, int, cx<T> (&)[1][R]) {}
     template <int R> __device__ __forceinline__ void last(int g, int o0, int p, cx<T> (&v)[1][R]) {
-        if (!(mode & (TM_KPHASE | TM_KOBS))) return;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const size_t gidx = c0 + (size_t)(o0 + r * p) * stride + g;
-            double k[3];
-            grid_wavenumbers(*J, gidx, k);
-            double K = 0; // Hamiltonian.init: sum_j 0.5 k_j^2 / m_j (wavepacket.zig:109-119)
-            for (int j = 0; j < J->d; ++j) K += __dmul_rn(__dmul_rn(0.5, k[j]), k[j]) / J->mass[j];
-            if (mode & TM_KPHASE) { // exp(Complex(0, -K) * dt) (quantum_dynamics.zig:397-399)
-                const double zre = __dsub_rn(__dmul_rn(0.0, J->dt_re), __dmul_rn(-K, J->dt_im));
-                const double zim = __dadd_rn(__dmul_rn(0.0, J->dt_im), __dmul_rn(-K, J->dt_re));
-                double ore, oim;
-                cexp_dev(zre, zim, ore, oim);
-                v[0][r] = tmul<-1>(v[0][r], mktab<T>(ore, oim));
-            } else { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268)
+            const size_t gidx = c0 + ((size_t)(o0 + r * p) << lstride) + g;
+            if (mode & TM_KPHASE) {
+                // exp(Complex(0, -K) * dt) with K = sum_j k_j^2 / (2 m_j) (quantum_dynamics.zig:397-399) as
+                // the product of the per-axis factors; differs from the exponential of the sum by rounding only
+                double2 f = J.kphase[axis_index<D>(gidx, 0, J.logn)];
+#pragma unroll
+                for (int j = 1; j < D; ++j) {
+                    const double2 e = J.kphase[j * J.n + axis_index<D>(gidx, j, J.logn)];
+                    f = make_double2(__dsub_rn(__dmul_rn(f.x, e.x), __dmul_rn(f.y, e.y)),
+                                     __dadd_rn(__dmul_rn(f.x, e.y), __dmul_rn(f.y, e.x)));
+                }
+                v[0][r] = tmul<-1>(v[0][r], mktab<T>(f.x, f.y));
+            } else { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268); K as in Hamiltonian.init
                 const double w = (double)v[0][r].x * (double)v[0][r].x + (double)v[0][r].y * (double)v[0][r].y;
-                for (int j = 0; j < J->d; ++j) acc[sl.mom() + j].add(w * k[j]);
-                acc[sl.ekin()].add(w * K);
+                double K = 0;
+#pragma unroll
+                for (int j = 0; j < D; ++j) { // Grid.init wavenumber (wavepacket.zig:66-68)
+                    const int idx = axis_index<D>(gidx, j, J.logn);
+                    const double k = __dmul_rn(idx < J.n / 2 ? (double)idx : __dsub_rn((double)idx, (double)J.n), J.dkunit[j]);
+                    K += __dmul_rn(__dmul_rn(0.5, k), k) / J.mass[j];
+                    acc[j] += w * k;
+                }
+                acc[D] += w * K;
             }
         }
     }
 };
 
-// one state's tile of J.tile consecutive lines along `axis` (stride n^(d-1-axis))
-template <typename T>
-__global__ void __launch_bounds__(512) nd_tile_kernel(NdJob<T> J, int axis, uint32_t mode, size_t part_base) {
+// one state's tile of J.tile consecutive lines along `axis` (stride n^(D-1-axis))
+template <typename T, int D>
+__global__ void __launch_bounds__(512)
+    nd_tile_kernel(const __grid_constant__ NdJob<T> J, int axis, uint32_t mode, size_t part_base) {
     if (*J.stopped) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int n = J.n, logn = J.logn, Tn = J.tile;
+    const int n = J.n, logn = J.logn, Tn = J.tile, logt = J.logtile;
     const int ldp = tile_ldp<T>(n);
     cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* buf1 = buf0 + Tn * ldp;
-    Tab<T>* twm = reinterpret_cast<Tab<T>*>(buf1 + Tn * ldp);
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>(2, Tn, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
-    size_t stride = 1;
-    for (int a = axis + 1; a < J.d; ++a) stride *= (size_t)n;
-    const size_t tiles_per_outer = stride / Tn;
-    const size_t outer = blockIdx.x / tiles_per_outer, inner0 = (blockIdx.x % tiles_per_outer) * Tn;
-    const size_t c0 = outer * stride * n + inner0;
+    const int lstride = logn * (D - 1 - axis);
+    const int ltpo = lstride - logt; // log2 of the tiles per outer index
+    const size_t outer = (size_t)blockIdx.x >> ltpo, inner0 = ((size_t)blockIdx.x & ((1u << ltpo) - 1)) << logt;
+    const size_t c0 = ((outer << logn) << lstride) + inner0;
     cx<T>* data = ((mode & TM_PHI) ? J.phi : J.psi) + (size_t)blockIdx.y * J.N;
-    for (int e = threadIdx.x; e < n * Tn; e += blockDim.x) { // coalesced rows of Tn elements
-        const int t = e / Tn, c = e - t * Tn;
-        buf0[c * ldp + padx<T>(t)] = data[c0 + (size_t)t * stride + c];
+    for (int e = threadIdx.x; e < n << logt; e += blockDim.x) { // coalesced rows of Tn elements
+        const int t = e >> logt, c = e & (Tn - 1);
+        buf0[c * ldp + padx<T>(t)] = data[c0 + ((size_t)t << lstride) + c];
     }
     __syncthreads();
-    Acc acc[NDV];
-    TileHook<T> h{&J, acc, NdSlots{J.d, J.S}, mode, c0, stride};
+    double acc[D + 1];
+#pragma unroll
+    for (int j = 0; j <= D; ++j) acc[j] = 0.0;
+    TileHook<T, D> h{J, acc, mode, c0, lstride};
     cx<T>* cur = buf0;
     if (mode & TM_FWD) {
         cx<T>* oth = cur == buf0 ? buf1 : buf0;
@@ -489,17 +569,31 @@ __global__ void __launch_bounds__(512) nd_tile_kernel(NdJob<T> J, int axis, uint
         else cur = tfft<T, 1, -1, false, false>(cur, oth, ldp, logn, twm, Tn, h);
     }
     if (mode & TM_KOBS) {
-        block_partials(acc, NdSlots{J.d, J.S}.count(), J.part, part_base + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
+        block_partials<D + 1>(acc, Slots<D, 1>::mom, J.part, J.nparts, part_base + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
         return;
     }
     if (mode & TM_INV) {
         NdNoHook none;
         cur = tfft<T, 1, 1, false, false>(cur, cur == buf0 ? buf1 : buf0, ldp, logn, twm, Tn, none);
     }
-    for (int e = threadIdx.x; e < n * Tn; e += blockDim.x) {
-        const int t = e / Tn, c = e - t * Tn;
-        data[c0 + (size_t)t * stride + c] = cur[c * ldp + padx<T>(t)];
+    for (int e = threadIdx.x; e < n << logt; e += blockDim.x) {
+        const int t = e >> logt, c = e & (Tn - 1);
+        data[c0 + ((size_t)t << lstride) + c] = cur[c * ldp + padx<T>(t)];
     }
+}
+
+// per-axis kinetic phase exp(Complex(0, -k_i^2 / (2 m_j)) * dt) (Propagator.init, quantum_dynamics.zig:397-399)
+template <typename T> __global__ void nd_kphase_kernel(const __grid_constant__ NdJob<T> J, double2* out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= J.d * J.n) return;
+    const int j = e / J.n, idx = e - j * J.n;
+    const double k = __dmul_rn(idx < J.n / 2 ? (double)idx : __dsub_rn((double)idx, (double)J.n), J.dkunit[j]);
+    const double K = __dmul_rn(__dmul_rn(0.5, k), k) / J.mass[j];
+    const double zre = __dsub_rn(__dmul_rn(0.0, J.dt_re), __dmul_rn(-K, J.dt_im));
+    const double zim = __dadd_rn(__dmul_rn(0.0, J.dt_im), __dmul_rn(-K, J.dt_re));
+    double ore, oim;
+    cexp_dev(zre, zim, ore, oim);
+    out[e] = make_double2(ore, oim);
 }
 
 // ------------------------------------------------------------ setup, imaginary time, bookkeeping
@@ -539,8 +633,8 @@ template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double 
 }
 
 // setGaussian (wavepacket.zig:355-371) and the partial norms
-template <typename T> __global__ void nd_gauss_kernel(NdJob<T> J, size_t part_base) {
-    Acc acc[NDV];
+template <typename T> __global__ void nd_gauss_kernel(const __grid_constant__ NdJob<T> J, size_t part_base) {
+    double acc[1] = {0.0};
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
         double r[3];
         grid_coords(J, g, r);
@@ -555,20 +649,17 @@ template <typename T> __global__ void nd_gauss_kernel(NdJob<T> J, size_t part_ba
         for (int s = 0; s < J.S; ++s) {
             const cx<T> z = s == J.ic_state ? mk<T>((T)zr, (T)zi) : mk<T>(0, 0);
             J.psi[(size_t)s * J.N + g] = z;
-            acc[0].add((double)z.x * (double)z.x + (double)z.y * (double)z.y);
+            acc[0] += (double)z.x * (double)z.x + (double)z.y * (double)z.y;
         }
     }
-    block_partials(acc, 1, J.part, part_base + blockIdx.x);
+    block_partials<1>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
 }
 
 // psi /= sqrt(norm) (Complex.div by (s, 0), wavepacket.zig:282-284); optionally toDia and the acf reference
 template <typename T, int S>
-__global__ void nd_normalize_kernel(NdJob<T> J, size_t p0, size_t p1, int to_dia, int save_psi0) {
+__global__ void nd_normalize_kernel(NdJob<T> J, const double* __restrict__ sum, int to_dia, int save_psi0) {
     if (*J.stopped) return;
-    __shared__ double sq_sh;
-    if (threadIdx.x == 0) sq_sh = sqrt(sum_partials(J.part, p0, p1, 0).value() * J.dr);
-    __syncthreads();
-    const double sq = sq_sh, den = sq * sq;
+    const double sq = sqrt(sum[0] * J.dr), den = sq * sq;
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
         cx<T> x[S];
 #pragma unroll
@@ -601,31 +692,28 @@ __global__ void nd_normalize_kernel(NdJob<T> J, size_t p0, size_t p1, int to_dia
 }
 
 // partial sums of |psi|^2 (slot 0) or of <phi_o|psi> (slots 0, 1)
-template <typename T> __global__ void nd_dot_kernel(NdJob<T> J, int o, size_t part_base) {
+template <typename T> __global__ void nd_dot_kernel(const __grid_constant__ NdJob<T> J, int o, size_t part_base) {
     if (*J.stopped) return;
-    Acc acc[NDV];
+    double acc[2] = {0.0, 0.0};
     const cx<T>* ph = o >= 0 ? J.orth + (size_t)o * J.S * J.N : nullptr;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)J.S * J.N;
          e += (size_t)gridDim.x * blockDim.x) {
         const cx<T> z = J.psi[e];
         if (ph) {
             const cx<T> p = ph[e];
-            acc[0].add((double)p.x * (double)z.x + (double)p.y * (double)z.y);
-            acc[1].add((double)p.x * (double)z.y - (double)p.y * (double)z.x);
+            acc[0] += (double)p.x * (double)z.x + (double)p.y * (double)z.y;
+            acc[1] += (double)p.x * (double)z.y - (double)p.y * (double)z.x;
         } else {
-            acc[0].add((double)z.x * (double)z.x + (double)z.y * (double)z.y);
+            acc[0] += (double)z.x * (double)z.x + (double)z.y * (double)z.y;
         }
     }
-    block_partials(acc, ph ? 2 : 1, J.part, part_base + blockIdx.x);
+    block_partials<2>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
 }
 
 // psi -= <phi_o|psi> dr phi_o (quantum_dynamics.zig:898-904)
-template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, size_t p0, size_t p1) {
+template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, const double* __restrict__ sum) {
     if (*J.stopped) return;
-    __shared__ double ov[2];
-    if (threadIdx.x < 2) ov[threadIdx.x] = sum_partials(J.part, p0, p1, threadIdx.x).value() * J.dr;
-    __syncthreads();
-    const double ore = ov[0], oim = ov[1];
+    const double ore = sum[0] * J.dr, oim = sum[1] * J.dr;
     const cx<T>* ph = J.orth + (size_t)o * J.S * J.N;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)J.S * J.N;
          e += (size_t)gridDim.x * blockDim.x) {
@@ -643,6 +731,7 @@ template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, si
 struct NdBook {
     double pop_abs[4];
     double carry[4]; // absorbed sums of the next step's first accumAbsorbed
+    double scal[2];  // reduced sums for the imaginary-time kernels
 };
 template <typename T>
 __global__ void nd_finalize_kernel(NdJob<T> J, size_t x0, size_t x1, size_t k0, size_t k1, uint32_t mask,
@@ -651,10 +740,12 @@ __global__ void nd_finalize_kernel(NdJob<T> J, size_t x0, size_t x1, size_t k0, 
     if (kind != 1 && *J.stopped) return;
     __shared__ double out[NDV];
     const NdSlots sl{J.d, J.S};
-    if (threadIdx.x < sl.count()) {
-        const int v = threadIdx.x;
+    const int v = threadIdx.x >> 5; // one warp per slot, launched with 32 * NDV threads
+    if (v < sl.count()) {
         const bool kslot = v >= sl.mom() && v <= sl.ekin();
-        out[v] = kslot ? (k1 > k0 ? sum_partials(J.part, k0, k1, v).value() : 0.0) : sum_partials(J.part, x0, x1, v).value();
+        const double x = kslot ? (k1 > k0 ? warp_sum_partials(J.part, J.nparts, k0, k1, v) : 0.0)
+                               : warp_sum_partials(J.part, J.nparts, x0, x1, v);
+        if ((threadIdx.x & 31) == 0) out[v] = x;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
