@@ -65,6 +65,7 @@ NdJob<T> describe(zqd_job* J) {
     D.capw = J->capw.as<double>();
     D.tw = J->tw.as<Tab<T>>();
     D.kphase = J->expk.as<double2>();
+    D.axis = reinterpret_cast<const double4*>(J->expk.as<double2>() + (size_t)J->d * J->n);
     D.part = J->part.as<double>();
     D.nparts = J->part.bytes / (NDV * 2 * sizeof(double));
     D.rows_per_cta = J->nd_rows;
@@ -82,23 +83,23 @@ struct Launch {
     // partial-sum regions (in blocks)
     size_t R0, R1, R2, K, G;
 
-    int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false) {
+    int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false, NdFin f = NdFin{}) {
         NdJob<T> d = D;
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
         const int nbuf = (mode & RM_PHI) ? 3 : 2;
         const size_t smem = nd_smem_bytes<T>(nbuf, S * J->nd_rows, J->n);
-        if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
-        else nd_row_kernel<T, 3, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region);
+        if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
+        else nd_row_kernel<T, 3, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
-    int tile(int axis, uint32_t mode, size_t region, bool nostop = false) {
+    int tile(int axis, uint32_t mode, size_t region, bool nostop = false, NdFin f = NdFin{}) {
         NdJob<T> d = D;
         if (nostop) d.stopped = J->flags.as<int>() + 1;
         const size_t smem = nd_smem_bytes<T>(2, J->nd_tile, J->n);
         const dim3 grid((unsigned)ntile_blocks, S);
-        if (D.d == 2) nd_tile_kernel<T, 2><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
-        else nd_tile_kernel<T, 3><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region);
+        if (D.d == 2) nd_tile_kernel<T, 2><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region, f);
+        else nd_tile_kernel<T, 3><<<grid, J->nd_tile_threads, smem, J->stream>>>(d, axis, mode, region, f);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -120,11 +121,11 @@ struct Launch {
         return ZQD_OK;
     }
     // momentum observables of phi (the forward transform along the last axis is already done)
-    int kobs(bool nostop = false) {
+    int kobs(bool nostop, NdFin f) {
         int rc;
         for (int a = D.d - 2; a >= 1; --a)
             if ((rc = tile(a, TM_FWD | TM_PHI, 0, nostop))) return rc;
-        return tile(0, TM_FWD | TM_KOBS | TM_PHI, K, nostop);
+        return tile(0, TM_FWD | TM_KOBS | TM_PHI, K, nostop, f);
     }
 };
 
@@ -140,20 +141,25 @@ int ZQD_ND_CREATE(zqd_job* J) {
     // Tile pass: Tn lines per CTA, rows of Tn * c >= 32 bytes (one sector), shrunk from
     // 128 bytes until the grid has two CTAs per SM.
     const int budget = 200 * 1024, sms2 = 2 * 148;
+    const int max_items = 512; // 8-point groups of a CTA, one thread each
     J->nd_row_bufs = 3;
+    if (S * n > 8 * max_items) return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS (states x npoint at most 4096)");
+    static_assert(ND_IPT == 1, "launch shapes assume one 8-point group per thread");
     int L = std::max(1, std::min<int>((int)(N / n), 2048 / (S * n)));
     while (L > 1 && (N / n / L < (size_t)sms2 || nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget)) L >>= 1;
     if (nd_smem_bytes<T>(J->nd_row_bufs, S * L, n) > (size_t)budget)
         return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS");
     J->nd_rows = L;
-    J->nd_row_threads = std::max(32, std::min(512, (S * L * n / 8 + 31) / 32 * 32));
+    J->nd_row_threads = std::max(32, (S * L * n / 8 + 31) / 32 * 32);
     const int tmin = std::max(1, (int)(32 / c));
     int Tn = std::min(n, (int)(128 / c));
-    while (Tn > tmin && ((size_t)S * (N / n / Tn) < (size_t)sms2 || Tn * n / 8 > 512 ||
-                         nd_smem_bytes<T>(2, Tn, n) > (size_t)budget)) Tn >>= 1;
-    if (nd_smem_bytes<T>(2, Tn, n) > (size_t)budget) return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE TILE PASS");
+    while (Tn > 1 && (Tn * n / 8 > 256 || nd_smem_bytes<T>(2, Tn, n) > (size_t)budget ||
+                      (Tn > tmin && (size_t)S * (N / n / Tn) < (size_t)sms2)))
+        Tn >>= 1;
+    if (nd_smem_bytes<T>(2, Tn, n) > (size_t)budget || Tn * n / 8 > max_items)
+        return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE TILE PASS");
     J->nd_tile = Tn;
-    J->nd_tile_threads = std::max(32, std::min(512, (Tn * n / 8 + 31) / 32 * 32));
+    J->nd_tile_threads = std::max(32, (Tn * n / 8 + 31) / 32 * 32);
     const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
     const size_t nparts = 3 * nrow_blocks + S * ntile_blocks + 1024;
     int rc;
@@ -166,7 +172,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
     if (S > 1 && (rc = J->U.alloc((size_t)S * S * N * sizeof(double)))) return rc;
     if (o.has_cap && (rc = J->capw.alloc(N * sizeof(double)))) return rc;
     if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
-    if ((rc = J->expk.alloc((size_t)J->d * n * sizeof(double2)))) return rc;
+    if ((rc = J->expk.alloc((size_t)J->d * n * (sizeof(double2) + sizeof(double4))))) return rc; // phases, axis table
     if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
     if ((rc = J->book.alloc(sizeof(NdBook)))) return rc;
     if ((rc = J->flags.alloc(2 * sizeof(int)))) return rc;
@@ -186,7 +192,8 @@ int ZQD_ND_CREATE(zqd_job* J) {
     NdJob<T> D = describe(J);
     nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(D, 0.0, 1);
     ZQD_CUDA(cudaGetLastError());
-    nd_kphase_kernel<T><<<(unsigned)((J->d * n + 127) / 128), 128, 0, J->stream>>>(D, J->expk.as<double2>());
+    nd_kphase_kernel<T><<<(unsigned)((J->d * n + 127) / 128), 128, 0, J->stream>>>(
+        D, J->expk.as<double2>(), const_cast<double4*>(D.axis));
     ZQD_CUDA(cudaGetLastError());
     for (auto f : {nd_row_kernel<T, 2, S>, nd_row_kernel<T, 3, S>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
@@ -228,18 +235,23 @@ int enqueue(zqd_job* J) {
         if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc;
         nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
         ZQD_CUDA(cudaGetLastError());
-        auto finalize = [&](size_t x0, size_t x1, bool k, uint32_t mask, int i) -> int {
-            nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, x0, x1, Lc.K, k ? Lc.K + S * Lc.ntile_blocks : Lc.K, mask,
-                                                          hist + (size_t)i * HC, J->book.as<NdBook>(), rows_out, i,
-                                                          o.has_cap && o.cap_has_stop, o.cap_stop_norm, 0);
-            ZQD_CUDA(cudaGetLastError());
-            return ZQD_OK;
-        };
-        auto carry = [&](size_t r0, size_t r1) -> int { // absorbed sums of the next step's start
-            nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, r0, r1, Lc.K, Lc.K, 0, J->fin.as<double>() + (size_t)s * HC,
-                                                          J->book.as<NdBook>(), rows_out, 0, 0, 0.0, 2);
-            ZQD_CUDA(cudaGetLastError());
-            return ZQD_OK;
+        // finalize descriptors, run by the last CTA of the launch that ends a step
+        auto fin = [&](int kind, size_t x0, size_t x1, bool k, uint32_t mask, double* row, int i) {
+            NdFin f{};
+            f.row = row;
+            f.rows_out = rows_out;
+            f.book = J->book.as<NdBook>();
+            f.x0 = x0;
+            f.x1 = x1;
+            f.k0 = Lc.K;
+            f.k1 = k ? Lc.K + S * Lc.ntile_blocks : Lc.K;
+            f.stop_norm = o.cap_stop_norm;
+            f.mask = mask;
+            f.row_index = i;
+            f.kind = kind;
+            f.has_stop = kind == 0 && o.has_cap && o.cap_has_stop;
+            f.enabled = 1;
+            return f;
         };
         auto itp_ops = [&]() -> int { // quantum_dynamics.zig:898-906
             int rc2;
@@ -264,9 +276,9 @@ int enqueue(zqd_job* J) {
                 uint32_t mode = RM_OBS | RM_STORE | (needk ? RM_PHI : 0u);
                 if (i > 0) mode |= RM_INV | RM_REND;
                 if (i < iters) mode |= RM_RSTART | RM_FWD;
-                if ((rc = Lc.row(mode, obs, Lc.R0))) return rc;
-                if (needk && (rc = Lc.kobs())) return rc;
-                if ((rc = finalize(Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, i))) return rc;
+                const NdFin f = fin(0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
+                if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f))) return rc;
+                if (needk && (rc = Lc.kobs(false, f))) return rc;
             } else {
                 if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
                 if (o.imag_nstate && (rc = itp_ops())) return rc; // every i, the initial state included
@@ -274,28 +286,26 @@ int enqueue(zqd_job* J) {
                     nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, (double)i * o.time_step, 0);
                     ZQD_CUDA(cudaGetLastError());
                 }
-                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1))) return rc;
-                if (needk && (rc = Lc.kobs())) return rc;
                 // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
-                if ((rc = finalize(i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, i))) return rc;
+                const NdFin f = fin(0, i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
+                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f))) return rc;
+                if (needk && (rc = Lc.kobs(false, f))) return rc;
                 if (i < iters) {
                     if (o.pot_td) {
                         nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, ((double)i + 0.5) * o.time_step, 1);
                         ZQD_CUDA(cudaGetLastError());
                     }
-                    if ((rc = Lc.row(RM_RSTART | RM_FWD | RM_STORE, 0, Lc.R2))) return rc;
-                    if ((rc = carry(Lc.R2, Lc.R2 + Lc.nrow_blocks))) return rc;
+                    // the absorbed sums of step i+1's first accumAbsorbed
+                    const NdFin fc = fin(2, Lc.R2, Lc.R2 + Lc.nrow_blocks, false, 0, nullptr, 0);
+                    if ((rc = Lc.row(RM_RSTART | RM_FWD | RM_STORE, 0, Lc.R2, false, fc))) return rc;
                 }
             }
         }
         // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
         const uint32_t all = WM_ALL_OBS | (acf ? (uint32_t)WM_ACF : 0u);
         if ((rc = Lc.row(RM_OBS | RM_PHI, all, Lc.R1, true))) return rc;
-        if ((rc = Lc.kobs(true))) return rc;
-        nd_finalize_kernel<T><<<1, 32 * NDV, 0, J->stream>>>(Lc.D, Lc.R1, Lc.R1 + Lc.nrow_blocks, Lc.K, Lc.K + S * Lc.ntile_blocks,
-                                                      all, J->fin.as<double>() + (size_t)s * HC, J->book.as<NdBook>(),
-                                                      rows_out, 0, 0, 0.0, 1);
-        ZQD_CUDA(cudaGetLastError());
+        if ((rc = Lc.kobs(true, fin(1, Lc.R1, Lc.R1 + Lc.nrow_blocks, true, all, J->fin.as<double>() + (size_t)s * HC, 0))))
+            return rc;
         if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)
             ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice, J->stream));
     }

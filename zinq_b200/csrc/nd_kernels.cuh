@@ -59,6 +59,7 @@ template <typename T> struct NdJob {
     double* capw; // [N]
     const Tab<T>* tw; // [n] exp(-2 pi i t / n)
     const double2* kphase; // [D][n] exp(Complex(0, -k^2 / (2 m_j)) * dt) of axis j
+    const double4* axis;   // [D][n] per-axis grid values: coordinate r, wavenumber k, 0.5 k^2 / m_j
     double* part;     // per-CTA partial sums, slot-major: [NDV][nparts][2]
     size_t nparts;
     int rows_per_cta; // row pass: rows of the last axis per CTA
@@ -294,9 +295,195 @@ static __global__ void nd_reduce_kernel(const double* __restrict__ part, size_t 
     if ((threadIdx.x & 31) == 0) out[w] = v;
 }
 
+// Per-solve bookkeeping on the device.
+struct NdBook {
+    double pop_abs[4];
+    double carry[4];  // absorbed sums of the next step's first accumAbsorbed
+    double scal[2];   // reduced sums for the imaginary-time kernels
+    unsigned counter; // CTAs of the current launch that have written their partials
+};
+
+// What the last CTA of a row or tile launch does with the partial sums (enabled != 0):
+// kind 0: the observables row of step row_index (plus absorbed bookkeeping and stop_norm);
+// kind 1: the final observables (no bookkeeping); kind 2: only record the absorbed sums
+// of the next step's first accumAbsorbed.  [x0, x1): position-space and absorbed partial
+// blocks, [k0, k1): momentum-space blocks.
+struct NdFin {
+    double* row;
+    int* rows_out;
+    NdBook* book;
+    size_t x0, x1, k0, k1;
+    double stop_norm;
+    uint32_t mask;
+    int row_index, kind, has_stop, enabled;
+};
+
+// true in the CTA that finishes last (its partials and everyone else's are visible to it)
+__device__ __forceinline__ bool nd_last_cta(unsigned* counter, unsigned total) {
+    __shared__ bool last;
+    if (threadIdx.x < 32) __threadfence(); // the partial sums were written by the first warp
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(counter, 1u) == total - 1;
+        if (last) *counter = 0; // every CTA of this launch has counted; ready for the next one
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Sums the launch's partials in a fixed order and assembles the observables row
+// (Observables.init, quantum_dynamics.zig:300-360; accumAbsorbed bookkeeping :470-500;
+// stop_norm :933-944).  Run by every thread of one CTA.
+template <typename T> __device__ void nd_finalize_cta(const NdJob<T>& J, const NdFin& F) {
+    __shared__ double out[NDV];
+    const NdSlots sl{J.d, J.S};
+    const int nw = blockDim.x >> 5;
+    for (int v = threadIdx.x >> 5; v < sl.count(); v += nw) {
+        const bool kslot = v >= sl.mom() && v <= sl.ekin();
+        const double x = kslot ? (F.k1 > F.k0 ? warp_sum_partials(J.part, J.nparts, F.k0, F.k1, v) : 0.0)
+                               : warp_sum_partials(J.part, J.nparts, F.x0, F.x1, v);
+        if ((threadIdx.x & 31) == 0) out[v] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    NdBook* book = F.book;
+    if (F.kind == 2) {
+        for (int s = 0; s < J.S; ++s) book->carry[s] = out[sl.absn() + s];
+        return;
+    }
+    const uint32_t mask = F.mask;
+    double* row = F.row;
+    const RowLayout L{J.d, J.S};
+    const bool c_pos = mask & WM_POS, c_mom = mask & WM_MOM, c_pop = mask & WM_POP;
+    const bool c_ekin = (mask & WM_EKIN) || (mask & WM_ETOT), c_epot = (mask & WM_EPOT) || (mask & WM_ETOT);
+    const bool c_norm = (mask & WM_NORM) || F.has_stop, c_acf = mask & WM_ACF;
+    if (F.kind == 0)
+        for (int s = 0; s < J.S; ++s) { // accumAbsorbed adds sum * dr twice per step (quantum_dynamics.zig:497)
+            book->pop_abs[s] += book->carry[s] * J.dr;
+            book->pop_abs[s] += out[sl.abs() + s] * J.dr;
+            book->carry[s] = out[sl.absn() + s];
+        }
+    const double norm = out[sl.norm()] * J.dr;
+    row[L.norm()] = c_norm ? norm : nan("");
+    for (int k = 0; k < J.d; ++k) {
+        row[L.pos() + k] = c_pos ? out[sl.pos() + k] * J.dr : nan("");
+        row[L.mom() + k] = c_mom ? out[sl.mom() + k] * J.dk : nan("");
+    }
+    for (int s = 0; s < J.S; ++s) row[L.pop() + s] = c_pop ? out[sl.pop() + s] * J.dr + book->pop_abs[s] : nan("");
+    row[L.epot()] = c_epot ? out[sl.epot()] * J.dr : nan("");
+    row[L.ekin()] = c_ekin ? out[sl.ekin()] * J.dk : nan("");
+    row[L.acf()] = c_acf ? out[sl.acf()] * J.dr : nan("");
+    row[L.acf() + 1] = c_acf ? out[sl.acf() + 1] * J.dr : nan("");
+    if (F.kind == 0) {
+        *F.rows_out = F.row_index + 1;
+        if (F.has_stop && norm < F.stop_norm) *J.stopped = 1;
+    }
+}
+
 // index of grid point g along axis j (last axis fastest; n = 2^logn)
 template <int D> __device__ __forceinline__ int axis_index(size_t g, int j, int logn) {
     return (int)(g >> (logn * (D - 1 - j))) & ((1 << logn) - 1);
+}
+
+// ------------------------------------------------------------ register-resident transforms
+// Every Stockham pass reads elements i + r n/R of a line and writes elements o0 + r p.  In
+// the first pass (p = 1) and in a last radix-8 pass (p = n/8) both sets are i + r n/8: a
+// thread's first-pass inputs and last-pass outputs are the same eight elements of its line.
+// So the first pass runs on registers loaded straight from global memory, the last pass
+// leaves its outputs in registers (stored straight to global memory, or handed to the next
+// transform, whose first pass reads the same elements), and only the passes between them
+// go through shared memory.  Schedule: radix 8 first, radix 8/4/2 passes between, radix 8
+// last when n >= 64; for n = 16, 32 the last pass runs in shared memory and the thread
+// gathers its eight elements afterwards.  The inverse visits the middle passes in reverse.
+constexpr int ND_IPT = 1; // items (8-point groups) a thread holds; a CTA has one thread per item
+
+// radix schedule: first pass radix 8; `nmid` passes between (radix 8, the last of them
+// radix 2^rem in forward order, the first in inverse order); a last radix-8 pass if last8
+struct NdSched {
+    int nmid, rem;
+    bool last8;
+    __device__ __forceinline__ int lr(int j, bool inverse) const { // log2 radix of middle pass j
+        const int jj = inverse ? nmid - 1 - j : j;
+        return jj < nmid - 1 ? 3 : rem;
+    }
+};
+__device__ __forceinline__ NdSched nd_sched(int logn) {
+    NdSched s;
+    s.last8 = logn >= 6;
+    const int mid = logn - 3 - (s.last8 ? 3 : 0);
+    s.nmid = (mid + 2) / 3;
+    s.rem = mid - 3 * (s.nmid - 1);
+    return s;
+}
+
+// item it of the CTA -> (line g, 8-point group i); GFAST: consecutive items walk the lines
+template <bool GFAST> __device__ __forceinline__ void nd_item(int it, int logl, int logm, int& g, int& i) {
+    if (GFAST) {
+        g = it & ((1 << logl) - 1);
+        i = it >> logl;
+    } else {
+        i = it & ((1 << logm) - 1);
+        g = it >> logm;
+    }
+}
+
+// One n-point transform (SIGN -1 forward, +1 inverse, unnormalised) of `lines` lines.
+// In: v[k][r] = element i + r n/8 of line g for the thread's items k (it = tid + k blockDim).
+// Out: the same elements of the transformed lines.  a, b: shared line buffers (stride ldp).
+template <typename T, int SIGN, bool GFAST>
+__device__ __forceinline__ void nd_fft_regs(cx<T> (&v)[ND_IPT][8], cx<T>* a, cx<T>* b, int ldp, int logn, int logl,
+                                            const Tab<T>* __restrict__ twm, int lines) {
+    const NdSched sc = nd_sched(logn);
+    const int logm = logn - 3, items = lines << logm;
+    if (logn == 3) { // n = 8: the first pass is the last
+#pragma unroll
+        for (int k = 0; k < ND_IPT; ++k)
+            if (threadIdx.x + k * blockDim.x < items) dft<8, SIGN, T>(v[k]);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < ND_IPT; ++k) { // first pass, p = 1: outputs at 8 i + r
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it < items) {
+            int g, i;
+            nd_item<GFAST>(it, logl, logm, g, i);
+            dft<8, SIGN, T>(v[k]);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) a[g * ldp + padx<T>((i << 3) + r)] = v[k][r];
+        }
+    }
+    __syncthreads();
+    cx<T>* in = a;
+    cx<T>* out = b;
+    int logp = 3;
+    NdNoHook none;
+    for (int j = 0; j < sc.nmid; ++j) {
+        const int lr = sc.lr(j, SIGN > 0 && sc.last8);
+        if (lr == 3) tpass<T, 1, 8, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
+        else if (lr == 2) tpass<T, 1, 4, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
+        else tpass<T, 1, 2, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
+        cx<T>* t = in;
+        in = out;
+        out = t;
+        logp += lr;
+    }
+#pragma unroll
+    for (int k = 0; k < ND_IPT; ++k) { // last radix-8 pass (p = n/8, twiddle index r i), or the gather
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it < items) {
+            int g, i;
+            nd_item<GFAST>(it, logl, logm, g, i);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[k][r] = in[g * ldp + padx<T>(i + (r << logm))];
+            if (sc.last8) {
+#pragma unroll
+                for (int r = 1; r < 8; ++r) v[k][r] = tmul<SIGN>(v[k][r], twm[r * i]);
+                dft<8, SIGN, T>(v[k]);
+            }
+        }
+    }
+    __syncthreads(); // a and b are free again
 }
 
 // ------------------------------------------------------------ row pass
@@ -363,10 +550,8 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
     acc[SL::norm] += m2;
     if (obs & WM_POS) {
 #pragma unroll
-        for (int j = 0; j < D; ++j) { // Grid.init coordinate (wavepacket.zig:55-74)
-            const double r = __dadd_rn(J.lo[j], __dmul_rn((double)axis_index<D>(g, j, J.logn), J.span[j]) / (double)J.n);
-            acc[SL::pos + j] += m2 * r;
-        }
+        for (int j = 0; j < D; ++j) // Grid.init coordinate (wavepacket.zig:55-74), tabulated per axis
+            acc[SL::pos + j] += m2 * __ldg(&J.axis[j * J.n + axis_index<D>(g, j, J.logn)].x);
     }
     if (obs & (WM_EPOT | WM_ETOT)) { // V is symmetric: diagonal plus twice the upper triangle
         double e = 0;
@@ -447,103 +632,108 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
     __syncthreads();
 }
 
-// L rows of the last axis (all S states) per CTA: [inverse FFT] -> sweep -> [phi] -> [forward FFT] -> store
+// L rows of the last axis (all S states) per CTA:
+// global -> [inverse FFT] -> shared -> sweep -> [phi] -> [forward FFT] -> global
 template <typename T, int D, int S>
 __global__ void __launch_bounds__(512)
-    nd_row_kernel(const __grid_constant__ NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base) {
+    nd_row_kernel(const __grid_constant__ NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base,
+                  const __grid_constant__ NdFin F) {
     if (*J.stopped) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using SL = Slots<D, S>;
-    const int n = J.n, logn = J.logn, L = J.rows_per_cta;
-    const int ldp = tile_ldp<T>(n), lines = S * L, pts = L << logn;
+    const int n = J.n, logn = J.logn, L = J.rows_per_cta, logm = logn - 3;
+    const int ldp = tile_ldp<T>(n), lines = S * L, pts = L << logn, items = lines << logm;
     cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* buf1 = buf0 + lines * ldp;
     cx<T>* buf2 = buf1 + lines * ldp; // only with RM_PHI
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>((mode & RM_PHI) ? 3 : 2, lines, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
     const size_t row0 = (size_t)blockIdx.x * pts;
-    for (int e = threadIdx.x; e < S * pts; e += blockDim.x) { // line (state s, row l) = s * L + l
-        const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
-        buf0[(s * L + l) * ldp + padx<T>(x)] = J.psi[(size_t)s * J.N + row0 + rem];
+    // line g = s * L + l starts at psi[s * N + row0 + l * n]
+    auto gaddr = [&](int g) -> size_t { const int s = g / L; return (size_t)s * J.N + row0 + ((size_t)(g - s * L) << logn); };
+    cx<T> v[ND_IPT][8];
+#pragma unroll
+    for (int k = 0; k < ND_IPT; ++k) {
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it < items) {
+            int g, i;
+            nd_item<false>(it, 0, logm, g, i);
+            const cx<T>* src = J.psi + gaddr(g);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[k][r] = src[i + (r << logm)];
+        }
     }
-    __syncthreads();
-    NdNoHook none;
+    __syncthreads(); // twiddles staged
     cx<T>* cur = buf0;
     cx<T>* oth = buf1;
-    if (mode & RM_INV) {
-        cur = tfft<T, 1, 1, false, false>(cur, oth, ldp, logn, twm, lines, none);
-        oth = cur == buf0 ? buf1 : buf0;
-    }
-    if (mode & (RM_INV | RM_REND | RM_OBS | RM_RSTART | RM_PHI)) {
+    if (mode & RM_INV) nd_fft_regs<T, 1, false>(v, buf0, buf1, ldp, logn, 0, twm, lines);
+    const bool sweep = mode & (RM_INV | RM_REND | RM_OBS | RM_RSTART | RM_PHI);
+    if (sweep) { // to natural order in shared memory for the per-point stages
+#pragma unroll
+        for (int k = 0; k < ND_IPT; ++k) {
+            const int it = threadIdx.x + k * blockDim.x;
+            if (it < items) {
+                int g, i;
+                nd_item<false>(it, 0, logm, g, i);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) cur[g * ldp + padx<T>(i + (r << logm))] = v[k][r];
+            }
+        }
+        __syncthreads();
         double acc[SL::count];
 #pragma unroll
-        for (int v = 0; v < SL::count; ++v) acc[v] = 0.0;
+        for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
         nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr, ldp, L, row0, mode, obs, acc);
         if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
-    }
-    if (mode & RM_PHI) { // forward FFT of the end-of-step copy into phi
-        cx<T>* res = tfft<T, 1, -1, false, false>(oth, buf2, ldp, logn, twm, lines, none);
-        for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
-            const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
-            J.phi[(size_t)s * J.N + row0 + rem] = res[(s * L + l) * ldp + padx<T>(x)];
+        if (mode & RM_PHI) { // forward FFT of the end-of-step copy into phi
+            NdNoHook none;
+            cx<T>* res = tfft<T, 1, -1, false, false>(oth, buf2, ldp, logn, twm, lines, none);
+            for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
+                const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
+                J.phi[(size_t)s * J.N + row0 + rem] = res[(s * L + l) * ldp + padx<T>(x)];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int k = 0; k < ND_IPT; ++k) {
+            const int it = threadIdx.x + k * blockDim.x;
+            if (it < items) {
+                int g, i;
+                nd_item<false>(it, 0, logm, g, i);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[k][r] = cur[g * ldp + padx<T>(i + (r << logm))];
+            }
         }
         __syncthreads();
     }
-    if (mode & RM_FWD) cur = tfft<T, 1, -1, false, false>(cur, oth, ldp, logn, twm, lines, none);
+    if (mode & RM_FWD) nd_fft_regs<T, -1, false>(v, cur, oth, ldp, logn, 0, twm, lines);
     if (mode & RM_STORE)
-        for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
-            const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
-            J.psi[(size_t)s * J.N + row0 + rem] = cur[(s * L + l) * ldp + padx<T>(x)];
+#pragma unroll
+        for (int k = 0; k < ND_IPT; ++k) {
+            const int it = threadIdx.x + k * blockDim.x;
+            if (it < items) {
+                int g, i;
+                nd_item<false>(it, 0, logm, g, i);
+                cx<T>* dst = J.psi + gaddr(g);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) dst[i + (r << logm)] = v[k][r];
+            }
         }
+    if (F.enabled && nd_last_cta(&F.book->counter, gridDim.x)) nd_finalize_cta(J, F);
 }
 
 // ------------------------------------------------------------ tile pass
-template <typename T, int D> struct TileHook {
-    const NdJob<T>& J;
-    double (&acc)[D + 1]; // mom[D], ekin
-    uint32_t mode;
-    size_t c0;
-    int lstride; // log2 of the axis stride
-    template <int R> __device__ __forceinline__ void first(int, int, int, cx<T> (&)[1][R]) {}
-    template <int R> __device__ __forceinline__ void last(int g, int o0, int p, cx<T> (&v)[1][R]) {
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const size_t gidx = c0 + ((size_t)(o0 + r * p) << lstride) + g;
-            if (mode & TM_KPHASE) {
-                // exp(Complex(0, -K) * dt) with K = sum_j k_j^2 / (2 m_j) (quantum_dynamics.zig:397-399) as
-                // the product of the per-axis factors; differs from the exponential of the sum by rounding only
-                double2 f = J.kphase[axis_index<D>(gidx, 0, J.logn)];
-#pragma unroll
-                for (int j = 1; j < D; ++j) {
-                    const double2 e = J.kphase[j * J.n + axis_index<D>(gidx, j, J.logn)];
-                    f = make_double2(__dsub_rn(__dmul_rn(f.x, e.x), __dmul_rn(f.y, e.y)),
-                                     __dadd_rn(__dmul_rn(f.x, e.y), __dmul_rn(f.y, e.x)));
-                }
-                v[0][r] = tmul<-1>(v[0][r], mktab<T>(f.x, f.y));
-            } else { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268); K as in Hamiltonian.init
-                const double w = (double)v[0][r].x * (double)v[0][r].x + (double)v[0][r].y * (double)v[0][r].y;
-                double K = 0;
-#pragma unroll
-                for (int j = 0; j < D; ++j) { // Grid.init wavenumber (wavepacket.zig:66-68)
-                    const int idx = axis_index<D>(gidx, j, J.logn);
-                    const double k = __dmul_rn(idx < J.n / 2 ? (double)idx : __dsub_rn((double)idx, (double)J.n), J.dkunit[j]);
-                    K += __dmul_rn(__dmul_rn(0.5, k), k) / J.mass[j];
-                    acc[j] += w * k;
-                }
-                acc[D] += w * K;
-            }
-        }
-    }
-};
-
-// one state's tile of J.tile consecutive lines along `axis` (stride n^(D-1-axis))
+// one state's tile of J.tile consecutive lines along `axis` (stride n^(D-1-axis)):
+// global -> forward FFT -> [kinetic phase -> inverse FFT | momentum observables] -> global,
+// the elements in registers between the transforms (same elements, same threads)
 template <typename T, int D>
 __global__ void __launch_bounds__(512)
-    nd_tile_kernel(const __grid_constant__ NdJob<T> J, int axis, uint32_t mode, size_t part_base) {
+    nd_tile_kernel(const __grid_constant__ NdJob<T> J, int axis, uint32_t mode, size_t part_base,
+                   const __grid_constant__ NdFin F) {
     if (*J.stopped) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int n = J.n, logn = J.logn, Tn = J.tile, logt = J.logtile;
-    const int ldp = tile_ldp<T>(n);
+    const int n = J.n, logn = J.logn, Tn = J.tile, logt = J.logtile, logm = logn - 3;
+    const int ldp = tile_ldp<T>(n), items = Tn << logm;
     cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* buf1 = buf0 + Tn * ldp;
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>(2, Tn, n));
@@ -553,42 +743,105 @@ __global__ void __launch_bounds__(512)
     const size_t outer = (size_t)blockIdx.x >> ltpo, inner0 = ((size_t)blockIdx.x & ((1u << ltpo) - 1)) << logt;
     const size_t c0 = ((outer << logn) << lstride) + inner0;
     cx<T>* data = ((mode & TM_PHI) ? J.phi : J.psi) + (size_t)blockIdx.y * J.N;
-    for (int e = threadIdx.x; e < n << logt; e += blockDim.x) { // coalesced rows of Tn elements
-        const int t = e >> logt, c = e & (Tn - 1);
-        buf0[c * ldp + padx<T>(t)] = data[c0 + ((size_t)t << lstride) + c];
-    }
-    __syncthreads();
-    double acc[D + 1];
+    // element t of line g sits at data[c0 + (t << lstride) + g]; consecutive threads take consecutive lines
+    cx<T> v[ND_IPT][8];
 #pragma unroll
-    for (int j = 0; j <= D; ++j) acc[j] = 0.0;
-    TileHook<T, D> h{J, acc, mode, c0, lstride};
-    cx<T>* cur = buf0;
-    if (mode & TM_FWD) {
-        cx<T>* oth = cur == buf0 ? buf1 : buf0;
-        if (mode & (TM_KPHASE | TM_KOBS)) cur = tfft<T, 1, -1, false, true>(cur, oth, ldp, logn, twm, Tn, h);
-        else cur = tfft<T, 1, -1, false, false>(cur, oth, ldp, logn, twm, Tn, h);
+    for (int k = 0; k < ND_IPT; ++k) {
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it < items) {
+            int g, i;
+            nd_item<true>(it, logt, logm, g, i);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[k][r] = data[c0 + ((size_t)(i + (r << logm)) << lstride) + g];
+        }
     }
-    if (mode & TM_KOBS) {
-        block_partials<D + 1>(acc, Slots<D, 1>::mom, J.part, J.nparts, part_base + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
-        return;
+    __syncthreads(); // twiddles staged
+    if (mode & TM_FWD) nd_fft_regs<T, -1, true>(v, buf0, buf1, ldp, logn, logt, twm, Tn);
+    if (mode & (TM_KPHASE | TM_KOBS)) {
+        double acc[D + 1];
+#pragma unroll
+        for (int j = 0; j <= D; ++j) acc[j] = 0.0;
+#pragma unroll
+        for (int k = 0; k < ND_IPT; ++k) {
+            const int it = threadIdx.x + k * blockDim.x;
+            if (it < items) {
+                int g, i;
+                nd_item<true>(it, logt, logm, g, i);
+                const size_t gbase = c0 + g; // grid index of the line's element 0
+                if (mode & TM_KPHASE) {
+                    // exp(Complex(0, -K) * dt), K = sum_j k_j^2 / (2 m_j) (quantum_dynamics.zig:397-399), as the
+                    // product of per-axis factors (differs from the exponential of the sum by rounding only):
+                    // the factor of the line's other axes once, then one product per element
+                    double2 fl = make_double2(1.0, 0.0);
+#pragma unroll
+                    for (int j = 0; j < D; ++j)
+                        if (j != axis) {
+                            const double2 e = J.kphase[j * n + axis_index<D>(gbase, j, logn)];
+                            fl = make_double2(__dsub_rn(__dmul_rn(fl.x, e.x), __dmul_rn(fl.y, e.y)),
+                                              __dadd_rn(__dmul_rn(fl.x, e.y), __dmul_rn(fl.y, e.x)));
+                        }
+                    double2 f0[8];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) f0[r] = J.kphase[axis * n + i + (r << logm)];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        const double2 f = make_double2(__dsub_rn(__dmul_rn(f0[r].x, fl.x), __dmul_rn(f0[r].y, fl.y)),
+                                                       __dadd_rn(__dmul_rn(f0[r].x, fl.y), __dmul_rn(f0[r].y, fl.x)));
+                        v[k][r] = tmul<-1>(v[k][r], mktab<T>(f.x, f.y));
+                    }
+                } else { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268), per-axis tables
+                    double Kl = 0, kl[D];
+#pragma unroll
+                    for (int j = 0; j < D; ++j) {
+                        kl[j] = 0;
+                        if (j != axis) {
+                            const double4 a = J.axis[j * n + axis_index<D>(gbase, j, logn)];
+                            Kl += a.z;
+                            kl[j] = a.y;
+                        }
+                    }
+                    double4 a0[8];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) a0[r] = J.axis[axis * n + i + (r << logm)];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) {
+                        const double w = (double)v[k][r].x * (double)v[k][r].x + (double)v[k][r].y * (double)v[k][r].y;
+#pragma unroll
+                        for (int j = 0; j < D; ++j) acc[j] += w * (j == axis ? a0[r].y : kl[j]);
+                        acc[D] += w * (Kl + a0[r].z);
+                    }
+                }
+            }
+        }
+        if (mode & TM_KOBS) {
+            block_partials<D + 1>(acc, Slots<D, 1>::mom, J.part, J.nparts,
+                                  part_base + (size_t)blockIdx.y * gridDim.x + blockIdx.x);
+            if (F.enabled && nd_last_cta(&F.book->counter, gridDim.x * gridDim.y)) nd_finalize_cta(J, F);
+            return;
+        }
     }
-    if (mode & TM_INV) {
-        NdNoHook none;
-        cur = tfft<T, 1, 1, false, false>(cur, cur == buf0 ? buf1 : buf0, ldp, logn, twm, Tn, none);
-    }
-    for (int e = threadIdx.x; e < n << logt; e += blockDim.x) {
-        const int t = e >> logt, c = e & (Tn - 1);
-        data[c0 + ((size_t)t << lstride) + c] = cur[c * ldp + padx<T>(t)];
+    if (mode & TM_INV) nd_fft_regs<T, 1, true>(v, buf0, buf1, ldp, logn, logt, twm, Tn);
+#pragma unroll
+    for (int k = 0; k < ND_IPT; ++k) {
+        const int it = threadIdx.x + k * blockDim.x;
+        if (it < items) {
+            int g, i;
+            nd_item<true>(it, logt, logm, g, i);
+#pragma unroll
+            for (int r = 0; r < 8; ++r) data[c0 + ((size_t)(i + (r << logm)) << lstride) + g] = v[k][r];
+        }
     }
 }
 
 // per-axis kinetic phase exp(Complex(0, -k_i^2 / (2 m_j)) * dt) (Propagator.init, quantum_dynamics.zig:397-399)
-template <typename T> __global__ void nd_kphase_kernel(const __grid_constant__ NdJob<T> J, double2* out) {
+// and the per-axis grid table: r (Grid.init, wavepacket.zig:55-74), k (:66-68), 0.5 k^2 / m_j (:109-119)
+template <typename T> __global__ void nd_kphase_kernel(const __grid_constant__ NdJob<T> J, double2* out, double4* axis) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= J.d * J.n) return;
     const int j = e / J.n, idx = e - j * J.n;
     const double k = __dmul_rn(idx < J.n / 2 ? (double)idx : __dsub_rn((double)idx, (double)J.n), J.dkunit[j]);
     const double K = __dmul_rn(__dmul_rn(0.5, k), k) / J.mass[j];
+    axis[e] = make_double4(__dadd_rn(J.lo[j], __dmul_rn((double)idx, J.span[j]) / (double)J.n), k, K, 0.0);
     const double zre = __dsub_rn(__dmul_rn(0.0, J.dt_re), __dmul_rn(-K, J.dt_im));
     const double zim = __dadd_rn(__dmul_rn(0.0, J.dt_im), __dmul_rn(-K, J.dt_re));
     double ore, oim;
@@ -720,63 +973,6 @@ template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, co
         const cx<T> p = ph[e], z = J.psi[e];
         J.psi[e] = mk<T>((T)((double)z.x - (ore * (double)p.x - oim * (double)p.y)),
                          (T)((double)z.y - (ore * (double)p.y + oim * (double)p.x)));
-    }
-}
-
-// Sums the step's partials (fixed order), assembles the observables row, updates the
-// absorbed populations and stop flag.  part ranges: [x0, x1) position-space and
-// absorbed sums of the row passes, [k0, k1) momentum-space sums of the tile pass.
-// kind 0: the row of a step; 1: the final observables (no bookkeeping);
-// 2: only record the absorbed sums of the next step's first accumAbsorbed.
-struct NdBook {
-    double pop_abs[4];
-    double carry[4]; // absorbed sums of the next step's first accumAbsorbed
-    double scal[2];  // reduced sums for the imaginary-time kernels
-};
-template <typename T>
-__global__ void nd_finalize_kernel(NdJob<T> J, size_t x0, size_t x1, size_t k0, size_t k1, uint32_t mask,
-                                   double* row, NdBook* book, int* rows_out, int row_index, int has_stop,
-                                   double stop_norm, int kind) {
-    if (kind != 1 && *J.stopped) return;
-    __shared__ double out[NDV];
-    const NdSlots sl{J.d, J.S};
-    const int v = threadIdx.x >> 5; // one warp per slot, launched with 32 * NDV threads
-    if (v < sl.count()) {
-        const bool kslot = v >= sl.mom() && v <= sl.ekin();
-        const double x = kslot ? (k1 > k0 ? warp_sum_partials(J.part, J.nparts, k0, k1, v) : 0.0)
-                               : warp_sum_partials(J.part, J.nparts, x0, x1, v);
-        if ((threadIdx.x & 31) == 0) out[v] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    if (kind == 2) {
-        for (int s = 0; s < J.S; ++s) book->carry[s] = out[sl.absn() + s];
-        return;
-    }
-    const RowLayout L{J.d, J.S};
-    const bool c_pos = mask & WM_POS, c_mom = mask & WM_MOM, c_pop = mask & WM_POP;
-    const bool c_ekin = (mask & WM_EKIN) || (mask & WM_ETOT), c_epot = (mask & WM_EPOT) || (mask & WM_ETOT);
-    const bool c_norm = (mask & WM_NORM) || has_stop, c_acf = mask & WM_ACF;
-    if (kind == 0)
-        for (int s = 0; s < J.S; ++s) { // accumAbsorbed adds sum * dr twice per step (quantum_dynamics.zig:497)
-            book->pop_abs[s] += book->carry[s] * J.dr;
-            book->pop_abs[s] += out[sl.abs() + s] * J.dr;
-            book->carry[s] = out[sl.absn() + s];
-        }
-    const double norm = out[sl.norm()] * J.dr;
-    row[L.norm()] = c_norm ? norm : nan("");
-    for (int k = 0; k < J.d; ++k) {
-        row[L.pos() + k] = c_pos ? out[sl.pos() + k] * J.dr : nan("");
-        row[L.mom() + k] = c_mom ? out[sl.mom() + k] * J.dk : nan("");
-    }
-    for (int s = 0; s < J.S; ++s) row[L.pop() + s] = c_pop ? out[sl.pop() + s] * J.dr + book->pop_abs[s] : nan("");
-    row[L.epot()] = c_epot ? out[sl.epot()] * J.dr : nan("");
-    row[L.ekin()] = c_ekin ? out[sl.ekin()] * J.dk : nan("");
-    row[L.acf()] = c_acf ? out[sl.acf()] * J.dr : nan("");
-    row[L.acf() + 1] = c_acf ? out[sl.acf() + 1] * J.dr : nan("");
-    if (kind == 0) {
-        *rows_out = row_index + 1;
-        if (has_stop && norm < stop_norm) *J.stopped = 1;
     }
 }
 
