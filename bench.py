@@ -62,6 +62,64 @@ def units(opts):
     return sum(o["grid"]["npoint"] ** len(o["grid"]["bounds"]) * NSTATE * o["iterations"] for o in opts)
 
 
+# ---------------------------------------------------------------- N-D workloads (reported beside the headline)
+def coupled_harmonic_2d(npoint=512, iters=2000):
+    """2-D three-state coupled harmonic surfaces, 512^2 on [-12, 12]^2, dt 0.05; constants from a fixed seed."""
+    import numpy as np
+
+    rng = np.random.default_rng(20261203)
+    a, b, c = rng.uniform(-1, 1, 3), rng.uniform(-1, 1, 3), rng.uniform(0, 0.2, 3)
+    coup = "0.05*exp(-(r1^2+r2^2)/2)"
+    mat = [[(f"0.5*(r1^2+r2^2)+{a[i]:.17g}*r1+{b[i]:.17g}*r2+{c[i]:.17g}" if i == j else coup) for j in range(3)]
+           for i in range(3)]
+    return {"grid": {"bounds": [[-12, 12], [-12, 12]], "npoint": npoint},
+            "initial_conditions": {"position": [-2, 0], "momentum": [1, 0], "gamma": [1, 1], "state": 0,
+                                   "adiabatic": False},
+            "potential": {"custom": {"ndim": 2, "matrix": mat}}, "mass": [1, 1], "iterations": iters,
+            "time_step": 0.05, "adiabatic": False, "write": {"population": "P", "total_energy": "E", "norm": "N"}}
+
+
+def anharmonic_3d(iters, imaginary):
+    """3-D anharmonic well, 128^3 on [-8, 8]^3, dt 0.02: imaginary-time relaxation or real time with the ACF."""
+    opt = {"grid": {"bounds": [[-8, 8]] * 3, "npoint": 128},
+           "initial_conditions": {"position": [1, 1, 1], "momentum": [0, 0, 0], "gamma": [1, 1, 1], "state": 0,
+                                  "adiabatic": False},
+           "potential": {"custom": {"ndim": 3, "matrix": [["0.5*(r1^2+r2^2+r3^2)+0.1*(r1^2*r2-r2^3/3)+0.05*r3^4"]]}},
+           "mass": [1, 1, 1], "iterations": iters, "time_step": 0.02, "adiabatic": False,
+           "write": {} if imaginary else {"acf": "A"}}
+    if imaginary:
+        opt["imaginary"] = {"nstate": 1}
+    return opt
+
+
+def wide_grid_2d(iters=100):
+    """2-D two-state grid of 2048^2 (134 MB of FP64 wavefunction, larger than L2): the HBM-bound case."""
+    mat = [["0.5*(r1^2+r2^2)", "0.01*exp(-r1^2)"], ["0.01*exp(-r1^2)", "0.5*(r1^2+r2^2)+0.1"]]
+    return {"grid": {"bounds": [[-20, 20], [-20, 20]], "npoint": 2048},
+            "initial_conditions": {"position": [-2, 0], "momentum": [1, 0], "gamma": [1, 1], "state": 0,
+                                   "adiabatic": False},
+            "potential": {"custom": {"ndim": 2, "matrix": mat}}, "mass": [1, 1], "iterations": iters,
+            "time_step": 0.05, "adiabatic": False, "write": {"population": "P"}}
+
+
+def nd_bytes_per_step(opt, c):
+    """Algorithmic bytes of one step: N [2 (2d-1) S c + 2 S^2 c + a S c] (+ (2d-1) S N c with ekin/mom)."""
+    d = len(opt["grid"]["bounds"])
+    N = opt["grid"]["npoint"] ** d
+    S = len(opt["potential"]["custom"]["matrix"])
+    w = opt.get("write") or {}
+    a = 1 if "acf" in w else 0
+    b = N * (2 * (2 * d - 1) * S * c + 2 * S * S * c + a * S * c)
+    if any(k in w for k in ("kinetic_energy", "momentum", "total_energy")):
+        b += (2 * d - 1) * S * N * c
+    return b
+
+
+def nd_units(opt):
+    d = len(opt["grid"]["bounds"])
+    return opt["grid"]["npoint"] ** d * len(opt["potential"]["custom"]["matrix"]) * opt["iterations"]
+
+
 def config(extra=None):
     c = {"workload": "1-D two-state tanh crossing, 8192 pts x 2 states, 5 momenta, 4000 steps, dt 1",
          "jobs": len(MOMENTA), "npoint": NPOINT, "nstate": NSTATE, "iterations": ITERS,
@@ -168,6 +226,46 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+def nd_legs(qd, torch, flush, reps=2):
+    """2-D and 3-D workloads on one GPU: device time per run (graph replay), HBM roofline per step."""
+    import numpy as np
+
+    peak, peak_kind = measured_peak()
+    cases = [("2d_512sq_3states_2000steps", coupled_harmonic_2d()),
+             ("3d_128cube_itp_500steps", anharmonic_3d(500, True)),
+             ("3d_128cube_realtime_acf_2000steps", anharmonic_3d(2000, False)),
+             ("2d_2048sq_2states_100steps_larger_than_l2", wide_grid_2d())]
+    out = {}
+    for name, opt in cases:
+        leg = {"units_per_run": nd_units(opt)}
+        pops = {}
+        for prec in ("fp32", "fp64"):
+            job = qd.Job(opt, prec)
+            job.run()  # captures the run's graph; warm-up
+            ts = []
+            for _ in range(reps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                ts.append(job.run())
+            ms = statistics.mean(ts)
+            c = 16 if prec == "fp64" else 8
+            bstep = nd_bytes_per_step(opt, c)
+            achieved = bstep * opt["iterations"] / (ms / 1e3) / 1e9
+            leg[prec] = {"value": nd_units(opt) / (ms / 1e3), "unit": UNIT, "ms_per_run": ms,
+                         "us_per_step": 1e3 * ms / opt["iterations"],
+                         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                      "frac": achieved / peak, "bytes_per_step": bstep, "peak_kind": peak_kind}}
+            h = job.result(want_wavefunction=False).observables[0].history
+            if "population" in h:
+                pops[prec] = h["population"]
+            job.close()
+        leg["fp32_over_fp64"] = leg["fp32"]["value"] / leg["fp64"]["value"]
+        if len(pops) == 2:
+            leg["pop_err_fp32_vs_fp64"] = float(np.max(np.abs(pops["fp32"] - pops["fp64"])))
+        out[name] = leg
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -175,6 +273,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="zinq_b200", choices=["zinq_b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-nd", action="store_true", help="skip the 2-D / 3-D legs")
     ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
                     help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
     args = ap.parse_args()
@@ -304,6 +403,8 @@ def main():
                              "kernel keeps psi in shared memory across steps, so frac > 1 is on-chip residency"},
         "clocks": clocks,
     }
+    if not args.no_nd:
+        line["nd"] = nd_legs(qd, torch, flush)
     if not args.no_cpu:
         sample = workload(ITERS)[2:4]
         dt, _ = oracle_sample(sample, 1)

@@ -86,8 +86,7 @@ struct Launch {
     int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false, NdFin f = NdFin{}) {
         NdJob<T> d = D;
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
-        const int nbuf = (mode & RM_PHI) ? 3 : 2;
-        const size_t smem = nd_smem_bytes<T>(nbuf, S * J->nd_rows, J->n);
+        const size_t smem = nd_smem_bytes<T>(2, S * J->nd_rows, J->n);
         if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
         else nd_row_kernel<T, 3, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
         ZQD_CUDA(cudaGetLastError());
@@ -142,7 +141,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
     // 128 bytes until the grid has two CTAs per SM.
     const int budget = 200 * 1024, sms2 = 2 * 148;
     const int max_items = 512; // 8-point groups of a CTA, one thread each
-    J->nd_row_bufs = 3;
+    J->nd_row_bufs = 2;
     if (S * n > 8 * max_items) return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE ROW PASS (states x npoint at most 4096)");
     static_assert(ND_IPT == 1, "launch shapes assume one 8-point group per thread");
     int L = std::max(1, std::min<int>((int)(N / n), 2048 / (S * n)));

@@ -645,8 +645,7 @@ __global__ void __launch_bounds__(512)
     const int ldp = tile_ldp<T>(n), lines = S * L, pts = L << logn, items = lines << logm;
     cx<T>* buf0 = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* buf1 = buf0 + lines * ldp;
-    cx<T>* buf2 = buf1 + lines * ldp; // only with RM_PHI
-    Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>((mode & RM_PHI) ? 3 : 2, lines, n));
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>(2, lines, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
     const size_t row0 = (size_t)blockIdx.x * pts;
     // line g = s * L + l starts at psi[s * N + row0 + l * n]
@@ -685,17 +684,8 @@ __global__ void __launch_bounds__(512)
         for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
         nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr, ldp, L, row0, mode, obs, acc);
         if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
-        if (mode & RM_PHI) { // forward FFT of the end-of-step copy into phi
-            NdNoHook none;
-            cx<T>* res = tfft<T, 1, -1, false, false>(oth, buf2, ldp, logn, twm, lines, none);
-            for (int e = threadIdx.x; e < S * pts; e += blockDim.x) {
-                const int s = e / pts, rem = e - s * pts, l = rem >> logn, x = rem & (n - 1);
-                J.phi[(size_t)s * J.N + row0 + rem] = res[(s * L + l) * ldp + padx<T>(x)];
-            }
-            __syncthreads();
-        }
 #pragma unroll
-        for (int k = 0; k < ND_IPT; ++k) {
+        for (int k = 0; k < ND_IPT; ++k) { // the next step's first-pass inputs; frees cur
             const int it = threadIdx.x + k * blockDim.x;
             if (it < items) {
                 int g, i;
@@ -705,6 +695,32 @@ __global__ void __launch_bounds__(512)
             }
         }
         __syncthreads();
+        if (mode & RM_PHI) { // forward FFT of the end-of-step copy (in oth) into phi, through oth and cur
+            cx<T> w[ND_IPT][8];
+#pragma unroll
+            for (int k = 0; k < ND_IPT; ++k) {
+                const int it = threadIdx.x + k * blockDim.x;
+                if (it < items) {
+                    int g, i;
+                    nd_item<false>(it, 0, logm, g, i);
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) w[k][r] = oth[g * ldp + padx<T>(i + (r << logm))];
+                }
+            }
+            __syncthreads();
+            nd_fft_regs<T, -1, false>(w, oth, cur, ldp, logn, 0, twm, lines);
+#pragma unroll
+            for (int k = 0; k < ND_IPT; ++k) {
+                const int it = threadIdx.x + k * blockDim.x;
+                if (it < items) {
+                    int g, i;
+                    nd_item<false>(it, 0, logm, g, i);
+                    cx<T>* dst = J.phi + gaddr(g);
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) dst[i + (r << logm)] = w[k][r];
+                }
+            }
+        }
     }
     if (mode & RM_FWD) nd_fft_regs<T, -1, false>(v, cur, oth, ldp, logn, 0, twm, lines);
     if (mode & RM_STORE)
