@@ -147,6 +147,12 @@ typedef struct {
     /* this build */
     zqd_precision precision;
     int log; /* compute every observable on log steps, like run(..., log=true) */
+    /* Initial wavefunction (this build; the reference has no such input, its solve always starts
+       from setGaussian, src/quantum_dynamics.zig:867).  NULL: the Gaussian of initial_conditions.
+       Otherwise nstate x npoint^ndim complex values (re, im interleaved, state-major, last axis
+       fastest) that replace the Gaussian; the solve then normalises them and applies toDia when
+       ic_adiabatic, as after setGaussian.  Chains an imaginary-time relaxation into real time. */
+    const double* ic_wavefunction;
 } zqd_options;
 
 /* Fills the reference's field defaults (log_interval 1, cap exponent 0.001,

@@ -1074,6 +1074,11 @@ struct Sim {
     }
     void setGaussian() { // :355-371
         std::fill(psi.begin(), psi.end(), cplx{0, 0});
+        if (o.ic_wavefunction) { // chaining extension: the given state instead of the Gaussian
+            for (size_t e = 0; e < (size_t)S * N; ++e) psi[e] = {o.ic_wavefunction[2 * e], o.ic_wavefunction[2 * e + 1]};
+            normalize();
+            return;
+        }
         for (size_t i = 0; i < N; ++i) {
             cplx ex{0, 0};
             for (int j = 0; j < d; ++j) {

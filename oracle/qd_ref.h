@@ -93,6 +93,10 @@ typedef struct {
     uint32_t write_mask;
     int nthreads; /* OpenMP threads for per-point loops and FFT lines (results do not depend on it) */
     qr_potential pot;
+    /* Chaining extension (no reference counterpart: its solve always starts from setGaussian):
+       NULL, or nstate x npoint^ndim complex values (re, im interleaved, state-major) that
+       replace the Gaussian; they are normalised like setGaussian's result. */
+    const double* ic_wavefunction;
 } qr_options;
 
 typedef struct qr_result qr_result;

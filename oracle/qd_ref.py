@@ -66,7 +66,7 @@ class _Opt(C.Structure):
         ("cap_exponent", C.c_double), ("cap_has_stop_norm", C.c_int), ("cap_stop_norm", C.c_double),
         ("imag_nstate", C.c_uint32), ("has_spectrum", C.c_int), ("spectrum_padding", C.c_uint32),
         ("spectrum_threshold", C.c_double), ("write_mask", C.c_uint32), ("nthreads", C.c_int),
-        ("pot", _Pot),
+        ("pot", _Pot), ("ic_wavefunction", C.POINTER(C.c_double)),
     ]
 
 
@@ -142,8 +142,11 @@ def _read_matrix(path):
     return data[: nrow * ncol].reshape(nrow, ncol)
 
 
-def run(opt: dict, nthreads: int = 1, want_wavefunction: bool = True):
-    """Run one ``quantum_dynamics`` job on the oracle; returns a list of Observables."""
+def run(opt: dict, nthreads: int = 1, want_wavefunction: bool = True, initial_wavefunction=None):
+    """Run one ``quantum_dynamics`` job on the oracle; returns a list of Observables.
+
+    initial_wavefunction: optional complex array (nstate x npoint^ndim) replacing the Gaussian,
+    for chaining an imaginary-time relaxation into real time (no reference counterpart)."""
     keep = []
 
     def arr(x):
@@ -197,6 +200,10 @@ def run(opt: dict, nthreads: int = 1, want_wavefunction: bool = True):
             wm |= W_BITS[k]
     o.write_mask = wm
     o.nthreads = int(nthreads)
+    if initial_wavefunction is not None:
+        w = np.ascontiguousarray(np.asarray(initial_wavefunction, dtype=np.complex128)).view(np.float64).ravel()
+        keep.append(w)
+        o.ic_wavefunction = _dptr(w)
 
     (pname, pval), = opt["potential"].items()
     pval = dict(POT_DEFAULTS.get(pname, {}), **(pval or {}))

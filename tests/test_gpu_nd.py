@@ -156,3 +156,43 @@ def test_batch_mixing_line_and_nd_jobs():
     for o, b in zip([one_d, two_d, one_d], batch):
         s = qd.run(o, want_wavefunction=False)
         np.testing.assert_array_equal(b.observables[0].history["population"], s.observables[0].history["population"])
+
+
+# ---------------------------------------------------------------- relaxation chained into real time
+def _chain(opt_itp, opt_rt, run_gpu):
+    """Imaginary-time relaxation, then real time from the relaxed state (GPU chain or oracle chain)."""
+    if run_gpu:
+        relaxed = qd.run(opt_itp).observables[0].wavefunction
+        return relaxed, qd.run(opt_rt, initial_wavefunction=relaxed)
+    relaxed = qd_ref.run(opt_itp)[0].wavefunction
+    return relaxed, qd_ref.run(opt_rt, initial_wavefunction=relaxed)
+
+
+@pytest.mark.parametrize("npoint", [16, 32])
+def test_3d_relaxation_chained_into_real_time(npoint):
+    # the anharmonic-well workload at a reduced grid: ITP, then real time with the autocorrelation
+    itp = anharmonic_3d(npoint=npoint, iters=150, write={"total_energy": "E"}, imaginary=1)
+    rt = anharmonic_3d(npoint=npoint, iters=120, write={"acf": "A", "total_energy": "E", "norm": "N"})
+    g_relaxed, g = _chain(itp, rt, True)
+    r_relaxed, r = _chain(itp, rt, False)
+    assert np.linalg.norm(g_relaxed - r_relaxed) / np.linalg.norm(r_relaxed) <= 1e-10
+    ga, ra = g.observables[0].history["acf"], r[0].history["acf"]
+    assert float(np.max(np.abs(ga - ra))) <= 1e-10
+    for name, key in (("total_energy", "etot"), ("norm", "norm")):
+        assert float(np.max(np.abs(g.observables[0].history[name] - r[0].history[key]))) <= 1e-10
+
+
+def test_1d_relaxation_chained_into_real_time_fp32():
+    # FP32 real-time leg from the FP64-relaxed state: autocorrelation within 1e-5 of the oracle chain
+    itp = {"grid": {"bounds": [[-10, 10]], "npoint": 256},
+           "initial_conditions": {"position": [1], "momentum": [0], "gamma": [1], "state": 0, "adiabatic": False},
+           "potential": {"custom": {"ndim": 1, "matrix": [["0.5*r1^2+0.05*r1^4"]]}}, "mass": [1], "iterations": 300,
+           "time_step": 0.02, "adiabatic": False, "imaginary": {"nstate": 1}, "write": {}}
+    rt = dict(itp)
+    rt.pop("imaginary")
+    rt["write"] = {"acf": "A"}
+    rt["iterations"] = 500
+    relaxed = qd_ref.run(itp)[0].wavefunction
+    g = qd.run(rt, precision="fp32", initial_wavefunction=relaxed).observables[0].history["acf"]
+    r = qd_ref.run(rt, initial_wavefunction=relaxed)[0].history["acf"]
+    assert float(np.max(np.abs(g - r))) <= 1e-5

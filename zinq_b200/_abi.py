@@ -59,7 +59,7 @@ class ZqdOptions(C.Structure):
         ("fft_plan", C.c_int),
         ("imaginary_nstate", C.c_uint32),
         ("has_spectrum", C.c_int), ("spectrum_padding", C.c_uint32), ("spectrum_threshold", C.c_double),
-        ("precision", C.c_int), ("log", C.c_int),
+        ("precision", C.c_int), ("log", C.c_int), ("ic_wavefunction", DP),
     ]
 
 

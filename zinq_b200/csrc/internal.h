@@ -36,6 +36,7 @@ struct Opts {
     bool adiabatic = false, has_cap = false, cap_track = false, cap_has_stop = false, has_spectrum = false, log = false;
     double cap_exponent = 0.001, cap_stop_norm = 0, spectrum_threshold = 1e-6;
     zqd_precision precision = ZQD_FP64;
+    std::vector<double> ic_wfn; // 2 * S * N doubles when an initial wavefunction is given
     // potential
     int pkind = 0;
     std::vector<double> harmonic_k;

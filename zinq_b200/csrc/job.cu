@@ -260,6 +260,18 @@ template <typename T> static int create_line(zqd_job* J) {
     if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
     if ((rc = J->jobs.alloc((size_t)J->nsolve * sizeof(LineJob<T>)))) return rc;
     if ((rc = J->scratch.alloc(n + 16))) return rc;
+    if (!J->o.ic_wfn.empty()) { // initial wavefunction in the cluster-permuted layout
+        if ((rc = J->psi_init.alloc(S * n * c))) return rc;
+        std::vector<cx<T>> h(S * n);
+        for (size_t st = 0; st < S; ++st)
+            for (size_t p = 0; p < n; ++p) {
+                const size_t cc = p / J->m, j = p - cc * J->m, x = cc + J->C * j;
+                h[st * n + p] = mk<T>((T)J->o.ic_wfn[2 * (st * n + x)], (T)J->o.ic_wfn[2 * (st * n + x) + 1]);
+            }
+        ZQD_CUDA(cudaMemcpyAsync(J->psi_init.p, h.data(), S * n * c, cudaMemcpyHostToDevice, J->stream));
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        J->h2d += S * n * c;
+    }
     J->device_bytes = J->R.bytes + J->expk.bytes + J->V.bytes + J->U.bytes + J->capw.bytes + J->tw.bytes +
                       J->psi_save.bytes + J->psi0.bytes + J->orth.bytes + J->hist.bytes;
     // twiddles
@@ -313,6 +325,7 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
         L.cap_exp = o.cap_exponent;
     }
     L.R = J->R.as<Tab<T>>();
+    L.psi_init = J->psi_init.as<cx<T>>();
     L.expk = J->expk.as<Tab<T>>();
     L.V = J->V.as<double>();
     L.U = J->U.as<double>();

@@ -73,6 +73,7 @@ template <typename T> struct LineJob {
     cx<T>* psi_save; // [S][n] permuted, written at the end of the solve
     cx<T>* psi0;     // [S][n] permuted, autocorrelation reference
     const cx<T>* orth;
+    const cx<T>* psi_init; // [S][n] permuted initial wavefunction replacing the Gaussian, or null
     int northo;
     double* hist;
     double* fin;

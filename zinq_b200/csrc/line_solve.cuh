@@ -239,7 +239,9 @@ __device__ __noinline__ void line_initial_state(const LineCtx<T>& X, double lo, 
     for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
         const int s = e / m, j = e - s * m;
         cx<T> z = mk<T>(0, 0);
-        if (s == J.ic_state) {
+        if (J.psi_init) {
+            z = J.psi_init[(size_t)s * n + X.base + j];
+        } else if (s == J.ic_state) {
             const double dx = __dsub_rn(grid_r<C>(lo, span, n, X.cta, j), J.x0);
             const double ere = __dmul_rn(__dmul_rn(__dmul_rn(-0.5, J.gamma), dx), dx);
             const double eim = __dmul_rn(J.p0, dx);

@@ -58,6 +58,7 @@ NdJob<T> describe(zqd_job* J) {
     D.psi = J->psi_save.as<cx<T>>();
     D.phi = J->phi.as<cx<T>>();
     D.psi0 = J->psi0.as<cx<T>>();
+    D.psi_init = J->psi_init.as<cx<T>>();
     D.orth = J->orth.as<cx<T>>();
     D.R = J->R.as<Tab<T>>();
     D.V = J->V.as<double>();
@@ -173,6 +174,14 @@ int ZQD_ND_CREATE(zqd_job* J) {
     if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
     if ((rc = J->expk.alloc((size_t)J->d * n * (sizeof(double2) + sizeof(double4))))) return rc; // phases, axis table
     if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
+    if (!o.ic_wfn.empty()) { // initial wavefunction, natural order
+        if ((rc = J->psi_init.alloc((size_t)S * N * c))) return rc;
+        std::vector<cx<T>> h((size_t)S * N);
+        for (size_t e = 0; e < (size_t)S * N; ++e) h[e] = mk<T>((T)o.ic_wfn[2 * e], (T)o.ic_wfn[2 * e + 1]);
+        ZQD_CUDA(cudaMemcpyAsync(J->psi_init.p, h.data(), (size_t)S * N * c, cudaMemcpyHostToDevice, J->stream));
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        J->h2d += (size_t)S * N * c;
+    }
     if ((rc = J->book.alloc(sizeof(NdBook)))) return rc;
     if ((rc = J->flags.alloc(2 * sizeof(int)))) return rc;
     const size_t rows = (size_t)o.iterations + 1;

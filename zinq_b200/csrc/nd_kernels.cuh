@@ -52,6 +52,7 @@ template <typename T> struct NdJob {
     cx<T>* psi;   // [S][N]
     cx<T>* phi;   // [S][N] scratch: the forward transform of the end-of-step psi
     cx<T>* psi0;  // [S][N] autocorrelation reference
+    const cx<T>* psi_init; // [S][N] initial wavefunction replacing the Gaussian, or null
     const cx<T>* orth; // [northo][S][N] relaxed states (imaginary time)
     Tab<T>* R;    // [NSYM][N]
     double* V;    // [S*S][N]
@@ -916,7 +917,7 @@ template <typename T> __global__ void nd_gauss_kernel(const __grid_constant__ Nd
         double zr, zi;
         cexp_dev(ere, eim, zr, zi);
         for (int s = 0; s < J.S; ++s) {
-            const cx<T> z = s == J.ic_state ? mk<T>((T)zr, (T)zi) : mk<T>(0, 0);
+            const cx<T> z = J.psi_init ? J.psi_init[(size_t)s * J.N + g] : s == J.ic_state ? mk<T>((T)zr, (T)zi) : mk<T>(0, 0);
             J.psi[(size_t)s * J.N + g] = z;
             acc[0] += (double)z.x * (double)z.x + (double)z.y * (double)z.y;
         }

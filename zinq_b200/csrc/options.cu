@@ -116,6 +116,12 @@ int copy_options(const zqd_options* in, Opts& o) {
     default:
         return fail(ZQD_ERR_INVALID_INPUT, "UNKNOWN POTENTIAL KIND");
     }
+    if (in->ic_wavefunction && o.ndim >= 1 && o.ndim <= ZQD_MAX_NDIM && o.pot_ns >= 1 && o.pot_ns <= ZQD_MAX_NSTATE &&
+        o.npoint >= 1 && o.npoint <= (1u << 24)) {
+        size_t N = 1;
+        for (uint32_t i = 0; i < o.ndim; ++i) N *= o.npoint;
+        o.ic_wfn.assign(in->ic_wavefunction, in->ic_wavefunction + 2 * (size_t)o.pot_ns * N);
+    }
     return ZQD_OK;
 }
 

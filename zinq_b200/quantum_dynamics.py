@@ -72,8 +72,11 @@ class _Keep:
         return a.ctypes.data_as(_abi.DP)
 
 
-def to_struct(opt: dict, precision: str = "fp64", log: bool = False):
-    """Translate a reference-schema options dict into zqd_options; returns (struct, keepalive)."""
+def to_struct(opt: dict, precision: str = "fp64", log: bool = False, initial_wavefunction=None):
+    """Translate a reference-schema options dict into zqd_options; returns (struct, keepalive).
+
+    initial_wavefunction: optional complex array (nstate x npoint^ndim, state-major, last axis
+    fastest) replacing the Gaussian of initial_conditions (zqd_options.ic_wavefunction)."""
     L = _abi.load()
     keep = _Keep()
     o = _abi.ZqdOptions()
@@ -132,6 +135,9 @@ def to_struct(opt: dict, precision: str = "fp64", log: bool = False):
         o.spectrum_threshold = float(spec.get("threshold", 1e-6))
     o.precision = _abi.PRECISION[precision]
     o.log = int(bool(log))
+    if initial_wavefunction is not None:
+        w = np.ascontiguousarray(np.asarray(initial_wavefunction, dtype=np.complex128)).view(np.float64).ravel()
+        o.ic_wavefunction = keep.arr(w)
 
     (pname, pval), = opt["potential"].items()
     pval = dict(POT_DEFAULTS.get(pname, {}), **(pval or {}))
@@ -205,10 +211,14 @@ def _shape(opt):
     return int(g["npoint"]) ** len(g["bounds"])
 
 
-def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction: bool = True) -> Result:
-    """quantum_dynamics.run on the GPU (src/quantum_dynamics.zig:567-603)."""
+def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction: bool = True,
+        initial_wavefunction=None) -> Result:
+    """quantum_dynamics.run on the GPU (src/quantum_dynamics.zig:567-603).
+
+    initial_wavefunction replaces the initial Gaussian (e.g. the relaxed state of an
+    imaginary-time run, to continue in real time); None keeps the reference's behaviour."""
     L = _abi.load()
-    o, keep = to_struct(opt, precision, log)
+    o, keep = to_struct(opt, precision, log, initial_wavefunction)
     res = C.c_void_p()
     check(L.zqd_run(C.byref(o), C.byref(res)))
     try:
@@ -245,10 +255,10 @@ def run_batch(opts: list, precision: str = "fp64", want_wavefunction: bool = Fal
 class Job:
     """Staged form: device tables built at construction, `run()` propagates with no host copies."""
 
-    def __init__(self, opt: dict, precision: str = "fp64"):
+    def __init__(self, opt: dict, precision: str = "fp64", initial_wavefunction=None):
         self._L = _abi.load()
         self.opt = opt
-        self._o, self._keep = to_struct(opt, precision)
+        self._o, self._keep = to_struct(opt, precision, False, initial_wavefunction)
         self._h = C.c_void_p()
         check(self._L.zqd_job_create(C.byref(self._o), C.byref(self._h)))
 
