@@ -196,3 +196,12 @@ def test_1d_relaxation_chained_into_real_time_fp32():
     g = qd.run(rt, precision="fp32", initial_wavefunction=relaxed).observables[0].history["acf"]
     r = qd_ref.run(rt, initial_wavefunction=relaxed)[0].history["acf"]
     assert float(np.max(np.abs(g - r))) <= 1e-5
+
+
+def test_3d_spectrum_of_real_time_leg():
+    opt = anharmonic_3d(npoint=16, iters=300, write={})
+    opt["spectrum"] = {"padding": 100, "threshold": 1e-5}
+    g = qd.run(opt, want_wavefunction=False).observables[0].spectrum
+    r = qd_ref.run(opt, want_wavefunction=False)[0].spectrum
+    np.testing.assert_allclose(g[0], r[0], rtol=0, atol=1e-10)
+    assert float(np.max(np.abs(g[1] - r[1]))) <= 1e-9 * max(1.0, float(np.max(np.abs(r[1]))))

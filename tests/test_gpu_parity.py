@@ -194,3 +194,20 @@ def test_runs_are_bitwise_deterministic():
     b = qd.run(config1())
     np.testing.assert_array_equal(a.observables[0].wavefunction, b.observables[0].wavefunction)
     np.testing.assert_array_equal(a.observables[0].history["total_energy"], b.observables[0].history["total_energy"])
+
+
+# ---------------------------------------------------------------- spectrum (calcSpectrum on the device)
+@pytest.mark.parametrize("padding,threshold,iters", [(0, 1e-6, 400), (700, 1e-4, 513), (1, 0.5, 1)])
+def test_spectrum_matches_oracle(padding, threshold, iters):
+    opt = {"grid": {"bounds": [[-10, 10]], "npoint": 256},
+           "initial_conditions": {"position": [1.5], "momentum": [0.3], "gamma": [1.2], "state": 0, "adiabatic": False},
+           "potential": {"custom": {"ndim": 1, "matrix": [["0.5*r1^2+0.05*r1^4"]]}}, "mass": [1],
+           "iterations": iters, "time_step": 0.05, "adiabatic": False,
+           "spectrum": {"padding": padding, "threshold": threshold}, "write": {}}
+    g = qd.run(opt, want_wavefunction=False).observables[0].spectrum
+    r = qd_ref.run(opt, want_wavefunction=False)[0].spectrum
+    assert g is not None and r is not None
+    assert g[0].shape == r[0].shape and g[1].shape == r[1].shape
+    np.testing.assert_allclose(g[0], r[0], rtol=0, atol=1e-10)
+    scale = max(1.0, float(np.max(np.abs(r[1]))))
+    assert float(np.max(np.abs(g[1] - r[1]))) <= 1e-9 * scale

@@ -78,6 +78,10 @@ struct SolveOut {
     std::vector<double> acfpad, sigma;
 };
 
+// calcSpectrum of one solve from its device history (spectrum.cu)
+int spectrum_device(cudaStream_t st, const double* d_hist, int hc, int col, size_t rows, const Opts& o, SolveOut& so,
+                    uint64_t& d2h);
+
 } // namespace zqd
 
 struct zqd_result {

@@ -394,6 +394,12 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
         so.rows = (size_t)nrows[s];
         so.hist.assign(hist.begin() + (size_t)s * rows * J->hc, hist.begin() + ((size_t)s * rows + so.rows) * J->hc);
         so.fin.assign(fin.begin() + (size_t)s * J->hc, fin.begin() + (size_t)(s + 1) * J->hc);
+        if (J->o.has_spectrum) { // exportWrite's calcSpectrum (quantum_dynamics.zig:257-276), on the device
+            const int rc = spectrum_device(J->stream, J->hist.as<double>() + (size_t)s * rows * J->hc, J->hc,
+                                           RowLayout{J->d, J->S}.acf(), so.rows, J->o, so, J->d2h);
+            if (rc) return rc;
+            R->d2h = J->d2h;
+        }
         const cx<T>* src = (s + 1 < J->nsolve) ? orth.data() + (size_t)s * SN : save.data();
         so.psi.resize(2 * SN);
         if (J->d == 1) {

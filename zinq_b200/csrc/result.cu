@@ -84,7 +84,7 @@ extern "C" int zqd_result_spectrum(const zqd_result* r, uint32_t s, const double
     if (!r) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
     if (s >= r->solves.size()) return fail(ZQD_ERR_NOT_FOUND, "SOLVE INDEX OUT OF RANGE");
     const SolveOut& so = r->solves[s];
-    if (so.sigma.empty()) return fail(ZQD_ERR_NOT_FOUND, "NO SPECTRUM WAS COMPUTED");
+    if (so.acfpad.empty()) return fail(ZQD_ERR_NOT_FOUND, "NO SPECTRUM WAS COMPUTED");
     if (acf_padded) *acf_padded = so.acfpad.data();
     if (nacf) *nacf = so.acfpad.size() / 2;
     if (sigma) *sigma = so.sigma.data();

@@ -42,6 +42,7 @@ class Observables:
     acf: complex | None
     history: dict = field(default_factory=dict)
     wavefunction: np.ndarray | None = None
+    spectrum: tuple | None = None  # (windowed, padded acf; sigma) of calcSpectrum when `spectrum` is set
 
 
 @dataclass
@@ -193,8 +194,14 @@ def _collect(res_ptr):
                 a = np.ctypeslib.as_array(ptr, shape=(rows.value * cols.value,)).copy().reshape(rows.value, cols.value)
                 hist[name] = a[:, 0] + 1j * a[:, 1] if name == "acf" else a
         acf = None if np.isnan(ob.acf_re) else complex(ob.acf_re, ob.acf_im)
+        spec = None
+        ap, na, sg, ns = _abi.DP(), C.c_size_t(), _abi.DP(), C.c_size_t()
+        if L.zqd_result_spectrum(res_ptr, s, C.byref(ap), C.byref(na), C.byref(sg), C.byref(ns)) == 0:
+            a = np.ctypeslib.as_array(ap, shape=(2 * na.value,)).copy() if na.value else np.zeros(0)
+            sig = np.ctypeslib.as_array(sg, shape=(ns.value,)).copy() if ns.value else np.zeros(0)
+            spec = (a[0::2] + 1j * a[1::2], sig)
         out.append(Observables(pos=np.array(ob.pos[:d]), mom=np.array(ob.mom[:d]), pop=np.array(ob.pop[:S]),
-                               epot=ob.epot, ekin=ob.ekin, norm=ob.norm, acf=acf, history=hist))
+                               epot=ob.epot, ekin=ob.ekin, norm=ob.norm, acf=acf, history=hist, spectrum=spec))
     return out
 
 
