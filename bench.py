@@ -276,7 +276,22 @@ def main():
     ap.add_argument("--no-nd", action="store_true", help="skip the 2-D / 3-D legs")
     ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
                     help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
+    ap.add_argument("--nd-case", nargs=3, metavar=("WORKLOAD", "PRECISION", "STEPS"), default=None,
+                    help="run one 2-D/3-D workload (c3 | c4 | c4itp | wide) for STEPS steps twice and exit; "
+                         "for ncu captures")
     args = ap.parse_args()
+
+    if args.nd_case:
+        from zinq_b200 import quantum_dynamics as qd
+
+        case, prec, steps = args.nd_case[0], args.nd_case[1], int(args.nd_case[2])
+        opt = {"c3": lambda: coupled_harmonic_2d(iters=steps), "c4": lambda: anharmonic_3d(steps, False),
+               "c4itp": lambda: anharmonic_3d(steps, True), "wide": lambda: wide_grid_2d(steps)}[case]()
+        job = qd.Job(opt, prec)
+        for _ in range(2):
+            ms = job.run()
+        print(json.dumps({"nd_case": case, "precision": prec, "ms": ms, "us_per_step": 1e3 * ms / steps}))
+        return
 
     if args.profile_case:
         from zinq_b200 import quantum_dynamics as qd
