@@ -291,6 +291,37 @@ void zqd_expr_destroy(zqd_expr* e);
  */
 int zqd_eigh_batch(uint32_t n, size_t count, const double* host_V, double* host_W, double* host_U);
 
+/* ------------------------------------------------------------------ server
+ * A request loop around quantum_dynamics.run for streams of independent jobs
+ * (the reference runs one job per process and has no counterpart).  Submission
+ * validates and copies the options (errors come back at once, with the
+ * reference's messages).  Worker threads admit requests in arrival order while
+ * their estimated device memory fits the budget; 1-D single-solve requests of
+ * the same precision, state count and grid size that wait together share one
+ * launch of the resident line kernel.  zqd_server_wait blocks until a request
+ * is done and returns its result (owned by the caller) and its latency from
+ * submission to completion.  Results equal those of zqd_run on the same options.
+ */
+typedef struct zqd_server zqd_server;
+typedef struct {
+    uint32_t struct_size;         /* sizeof(zqd_server_config); set by zqd_server_config_init */
+    uint32_t workers;             /* host threads, each running one launch at a time (default 4) */
+    uint32_t max_batch;           /* requests per grouped launch (default 16) */
+    uint64_t device_budget_bytes; /* 0: 90% of the device memory free at creation */
+} zqd_server_config;
+typedef struct {
+    uint64_t submitted, completed, failed, queued;
+    uint64_t grouped_launches, grouped_jobs;
+    uint64_t device_budget_bytes, device_bytes_in_use, peak_device_bytes;
+} zqd_server_stats;
+void zqd_server_config_init(zqd_server_config* cfg);
+int zqd_server_create(const zqd_server_config* cfg, zqd_server** out);
+int zqd_server_submit(zqd_server* server, const zqd_options* opt, uint64_t* ticket);
+int zqd_server_wait(zqd_server* server, uint64_t ticket, zqd_result** out, double* latency_ms);
+int zqd_server_stats_get(zqd_server* server, zqd_server_stats* out);
+/* waits for every submitted request, then frees the server */
+void zqd_server_destroy(zqd_server* server);
+
 /* ------------------------------------------------------------------ device */
 int zqd_device_count(void);
 int zqd_set_device(int device);

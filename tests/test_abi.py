@@ -125,3 +125,15 @@ def test_expression_compiles(good):
     h = C.c_void_p()
     assert lib.zqd_expr_compile(good.encode(), len(good), 1, C.byref(h)) == 0, lib.zqd_last_error()
     lib.zqd_expr_destroy(h)
+
+
+def test_server_config_defaults_and_no_device_status():
+    lib = _abi.load()
+    cfg = _abi.ZqdServerConfig()
+    lib.zqd_server_config_init(C.byref(cfg))
+    assert cfg.struct_size == C.sizeof(_abi.ZqdServerConfig) and cfg.workers == 4 and cfg.max_batch == 16
+    import torch
+
+    if not torch.cuda.is_available():
+        h = C.c_void_p()
+        assert lib.zqd_server_create(C.byref(cfg), C.byref(h)) == -12  # ZQD_ERR_NO_DEVICE

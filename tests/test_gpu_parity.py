@@ -211,3 +211,18 @@ def test_spectrum_matches_oracle(padding, threshold, iters):
     np.testing.assert_allclose(g[0], r[0], rtol=0, atol=1e-10)
     scale = max(1.0, float(np.max(np.abs(r[1]))))
     assert float(np.max(np.abs(g[1] - r[1]))) <= 1e-9 * scale
+
+
+@pytest.mark.parametrize("nstate,precision", [(3, "fp64"), (4, "fp64"), (4, "fp32")])
+def test_longest_lines_read_the_propagator_table_from_global_memory(nstate, precision):
+    # 16384 points x 3-4 states: the R slice no longer fits in shared memory beside the wavefunction
+    mat = [[("0.01*tanh(1.6*r1)" if i % 2 == 0 else "-0.01*tanh(1.6*r1)") if i == j else "0.005*exp(-r1^2)"
+            for j in range(nstate)] for i in range(nstate)]
+    opt = {"grid": {"bounds": [[-30, 30]], "npoint": 16384},
+           "initial_conditions": {"position": [-8], "momentum": [15], "gamma": [0.5], "state": 0, "adiabatic": False},
+           "potential": {"custom": {"ndim": 1, "matrix": mat}}, "mass": [2000], "iterations": 200, "time_step": 1,
+           "adiabatic": False, "write": {"population": "P", "total_energy": "E"}}
+    if precision == "fp64":
+        compare(opt)
+    else:
+        compare(opt, precision="fp32", pop_tol=FP32_POP_TOL, obs_tol=1e-4)

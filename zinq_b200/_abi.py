@@ -72,6 +72,17 @@ class ZqdObservables(C.Structure):
     ]
 
 
+class ZqdServerConfig(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
+                ("device_budget_bytes", C.c_uint64)]
+
+
+class ZqdServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "queued", "grouped_launches",
+                                          "grouped_jobs", "device_budget_bytes", "device_bytes_in_use",
+                                          "peak_device_bytes")]
+
+
 # (name, restype, argtypes) for every entry point of zinq_qd.h
 VP = C.c_void_p
 SIGNATURES = [
@@ -112,6 +123,12 @@ SIGNATURES = [
     ("zqd_expr_eval_points", C.c_int, [VP, DP, C.c_size_t, C.c_double, DP]),
     ("zqd_expr_destroy", None, [VP]),
     ("zqd_eigh_batch", C.c_int, [C.c_uint32, C.c_size_t, DP, DP, DP]),
+    ("zqd_server_config_init", None, [C.POINTER(ZqdServerConfig)]),
+    ("zqd_server_create", C.c_int, [C.POINTER(ZqdServerConfig), C.POINTER(VP)]),
+    ("zqd_server_submit", C.c_int, [VP, C.POINTER(ZqdOptions), C.POINTER(C.c_uint64)]),
+    ("zqd_server_wait", C.c_int, [VP, C.c_uint64, C.POINTER(VP), C.POINTER(C.c_double)]),
+    ("zqd_server_stats_get", C.c_int, [VP, C.POINTER(ZqdServerStats)]),
+    ("zqd_server_destroy", None, [VP]),
     ("zqd_device_count", C.c_int, []),
     ("zqd_set_device", C.c_int, [C.c_int]),
 ]

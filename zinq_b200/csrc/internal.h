@@ -16,6 +16,13 @@ namespace zqd {
 
 void set_error(const std::string& msg);
 int fail(int status, const std::string& msg);
+const char* last_error();
+
+// Device buffers of jobs come from the device's stream-ordered memory pool: cudaFree waits for
+// every stream of the device, which would stall concurrent jobs (the server runs several at a
+// time); a pool free waits for nothing.  Freed blocks stay cached in the pool for later jobs.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void dev_free(void* p);
 
 #define ZQD_CUDA(call)                                                                                             \
     do {                                                                                                           \

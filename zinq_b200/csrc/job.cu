@@ -149,13 +149,15 @@ static int choose_line_shape(zqd_job* J) {
     if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
     const int target = J->fp32 ? 4096 : 2048;
     int fallback = -1;
-    for (int pass = 0; pass < 2; ++pass) {
+    // pass 0: at most `target` points per CTA; 1: any size; 2: R read from global memory
+    for (int pass = 0; pass < 3; ++pass) {
+        const bool rg = pass == 2;
         for (int C = 1; C <= 16; C <<= 1) {
             if (forced && C != forced) continue;
             if (J->n % C) continue;
             const int m = J->n / C;
             if (m < 8 || m / C < 1) continue;
-            const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m) : line_smem_bytes<double>(J->S, C, m);
+            const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m, rg) : line_smem_bytes<double>(J->S, C, m, rg);
             if (smem > budget) continue;
             const int threads = std::max(32, (m / 8 + 31) / 32 * 32);
             if (threads > (J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value)) continue;
@@ -169,9 +171,9 @@ static int choose_line_shape(zqd_job* J) {
             J->E = 8 * J->S;
             J->threads = threads;
             J->smem = smem;
+            J->r_global = rg;
             return ZQD_OK;
         }
-        if (forced) break;
     }
     return fail(ZQD_ERR_UNSUPPORTED, "1-D GRID DOES NOT FIT THE RESIDENT CLUSTER KERNEL (at most 16 CTAs of 4096 points)");
 }
@@ -326,6 +328,7 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
     }
     L.R = J->R.as<Tab<T>>();
     L.psi_init = J->psi_init.as<cx<T>>();
+    L.r_global = J->r_global ? 1 : 0;
     L.expk = J->expk.as<Tab<T>>();
     L.V = J->V.as<double>();
     L.U = J->U.as<double>();
@@ -443,11 +446,20 @@ static int nd_run(zqd_job* J) {
 extern "C" int zqd_job_create(const zqd_options* opt, zqd_job** out) {
     if (!out) return fail(ZQD_ERR_INVALID_INPUT, "NULL OUTPUT HANDLE");
     *out = nullptr;
+    Opts o;
+    int rc = copy_options(opt, o);
+    if (rc) return rc;
+    if ((rc = validate(o))) return rc;
+    return zqd::job_create_opts(std::move(o), out);
+}
+
+// A job from already copied and validated options (zqd_job_create, the server).
+int zqd::job_create_opts(Opts&& o, zqd_job** out) {
+    *out = nullptr;
     std::unique_ptr<zqd_job> J(new (std::nothrow) zqd_job());
     if (!J) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
-    int rc = copy_options(opt, J->o);
-    if (rc) return rc;
-    if ((rc = validate(J->o))) return rc;
+    J->o = std::move(o);
+    int rc;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ZQD_ERR_NO_DEVICE, "no CUDA device");
     J->S = J->o.pot_ns;
@@ -529,6 +541,7 @@ struct zqd_batch {
     float last_ms = 0;
     uint32_t launches = 0;
     ~zqd_batch() {
+        if (stream) cudaStreamSynchronize(stream);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -582,7 +595,8 @@ extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, 
         g->shape = LaunchShape{a->S, a->C, a->E, 0, 0, B->stream};
         for (uint32_t k = i + 1; k < njobs; ++k) {
             zqd_job* b = B->jobs[k].get();
-            if (!done[k] && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C) {
+            if (!done[k] && b->d == 1 && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C &&
+                b->r_global == a->r_global) {
                 g->members.push_back(b);
                 done[k] = true;
             }
@@ -619,6 +633,54 @@ extern "C" int zqd_batch_run(zqd_batch* B) {
     for (auto& g : B->groups)
         for (zqd_job* J : g->members) J->last_ms = ms;
     return ZQD_OK;
+}
+
+// One grouped launch of 1-D single-solve jobs of the same precision, state count and cluster
+// shape (the batch's grouping, for callers that hold the jobs themselves); waits for it.
+int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, float* ms) {
+    if (jobs.empty()) return ZQD_OK;
+    const zqd_job* a = jobs[0];
+    for (const zqd_job* J : jobs)
+        if (J->d != 1 || J->nsolve != 1 || J->fp32 != a->fp32 || J->S != a->S || J->C != a->C || J->r_global != a->r_global)
+            return fail(ZQD_ERR_INVALID_INPUT, "JOBS OF ONE GROUP MUST SHARE PRECISION, STATES AND CLUSTER SHAPE");
+    LaunchShape sh{a->S, a->C, a->E, 0, 0, st};
+    for (const zqd_job* J : jobs) {
+        sh.threads = std::max(sh.threads, J->threads);
+        sh.smem = std::max(sh.smem, J->smem);
+    }
+    DevBuf descs;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ZQD_CUDA(cudaEventCreate(&e0));
+    ZQD_CUDA(cudaEventCreate(&e1));
+    auto go = [&]() -> int {
+        int rc;
+        if (a->fp32) {
+            std::vector<LineJob<float>> d;
+            for (zqd_job* J : jobs) d.push_back(line_job_desc<float>(J, 0));
+            if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+            ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
+            ZQD_CUDA(cudaEventRecord(e0, st));
+            if ((rc = launch_line_s<float>(&sh, descs.p, (int)jobs.size()))) return rc;
+        } else {
+            std::vector<LineJob<double>> d;
+            for (zqd_job* J : jobs) d.push_back(line_job_desc<double>(J, 0));
+            if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+            ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
+            ZQD_CUDA(cudaEventRecord(e0, st));
+            if ((rc = launch_line_s<double>(&sh, descs.p, (int)jobs.size()))) return rc;
+        }
+        ZQD_CUDA(cudaEventRecord(e1, st));
+        ZQD_CUDA(cudaStreamSynchronize(st));
+        float t = 0;
+        ZQD_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        for (zqd_job* J : jobs) J->last_ms = t;
+        if (ms) *ms = t;
+        return ZQD_OK;
+    };
+    const int rc = go();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
 }
 
 extern "C" int zqd_batch_result(zqd_batch* B, uint32_t i, zqd_result** out) {

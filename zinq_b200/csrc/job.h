@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -13,13 +14,11 @@ namespace zqd {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
+    ~DevBuf() { dev_free(p); }
     int alloc(size_t b) {
         bytes = b;
         if (b == 0) return ZQD_OK;
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = dev_alloc(&p, b);
         if (e != cudaSuccess) {
             p = nullptr;
             return fail(ZQD_ERR_DEVICE_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
@@ -31,6 +30,12 @@ struct DevBuf {
 
 } // namespace zqd
 
+struct zqd_job;
+namespace zqd {
+int job_create_opts(Opts&& o, zqd_job** out);
+int run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, float* ms);
+} // namespace zqd
+
 struct zqd_job {
     zqd::Opts o;
     int S = 1, d = 1, n = 0;
@@ -38,6 +43,7 @@ struct zqd_job {
     int C = 1, m = 0, q = 0, E = 8, threads = 32;
     size_t smem = 0;
     bool fp32 = false;
+    bool r_global = false; // 1-D: R read from global memory (the largest lines)
     int nsolve = 1, hc = 0;
     zqd::PotStore pot;
     cudaStream_t stream = nullptr;
@@ -47,10 +53,12 @@ struct zqd_job {
     zqd::DevBuf psi_init;               // initial wavefunction replacing the Gaussian (1-D: permuted layout)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
+    bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)
     float last_ms = 0;
     size_t device_bytes = 0;
     uint64_t h2d = 0, d2h = 0; // bytes copied by this job
     ~zqd_job() {
+        if (stream) cudaStreamSynchronize(stream); // the buffers are released without a device-wide wait
         if (nd_graph) cudaGraphExecDestroy(nd_graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);

@@ -74,6 +74,7 @@ template <typename T> struct LineJob {
     cx<T>* psi0;     // [S][n] permuted, autocorrelation reference
     const cx<T>* orth;
     const cx<T>* psi_init; // [S][n] permuted initial wavefunction replacing the Gaussian, or null
+    int r_global;          // R read from global memory instead of shared memory
     int northo;
     double* hist;
     double* fin;

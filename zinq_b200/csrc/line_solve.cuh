@@ -18,8 +18,10 @@
 namespace zqd {
 
 // dynamic shared memory of one CTA
-template <typename T> __host__ __device__ inline size_t line_smem_bytes(int S, int C, int m) {
-    const size_t ld = (size_t)padded_len<T>(m), nsym = (size_t)S * (S + 1) / 2;
+// r_global: the R table is read from global memory (L2) instead of being staged, for the
+// largest lines whose R slice does not fit next to the wavefunction buffers
+template <typename T> __host__ __device__ inline size_t line_smem_bytes(int S, int C, int m, bool r_global = false) {
+    const size_t ld = (size_t)padded_len<T>(m), nsym = r_global ? 0 : (size_t)S * (S + 1) / 2;
     return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 2 : 1) + nsym + 1) * (size_t)m * sizeof(Tab<T>);
 }
 
@@ -219,13 +221,13 @@ template <typename T, int S, int C> __device__ __noinline__ void line_orthogonal
 // time-dependent Hamiltonian.update (wavepacket.zig:137-143) and, with_R,
 // Propagator.update into the shared-memory R table
 template <typename T, int S, int C>
-__device__ __noinline__ void line_ham_update(const LineCtx<T>& X, double t, bool with_R, Tab<T>* Rs, double lo,
-                                             double span) {
+__device__ __noinline__ void line_ham_update(const LineCtx<T>& X, double t, bool with_R, Tab<T>* Rs, int rstride,
+                                             double lo, double span) {
     const LineJob<T>& J = *X.J;
     for (int j = threadIdx.x; j < X.m; j += blockDim.x) {
         const double r = grid_r<C>(lo, span, X.n, X.cta, j);
         td_point_update<T, S>(J.pot, r, t, with_R, J.dt_re, J.dt_im, with_R ? capdecay(J, r) : 1.0, J.V, J.U,
-                              (size_t)X.n, X.base + j, Rs, (size_t)X.m, (size_t)j);
+                              (size_t)X.n, X.base + j, Rs, (size_t)rstride, (size_t)j);
     }
     __syncthreads();
 }
@@ -305,6 +307,7 @@ template <typename T, int S, int C> struct LineSolver {
     const Tab<T>* twm;
     const Tab<T>* twc;
     const Tab<T>* Rs;
+    int rstride; // component stride of Rs: m when staged in shared memory, n when read from global
     const Tab<T>* eks;
     const double* capw; // this CTA's slice of the global tables
     const double* Ug;
@@ -331,7 +334,7 @@ template <typename T, int S, int C> struct LineSolver {
 #pragma unroll
             for (int s = 0; s < S; ++s) x[s] = v[s][r];
             if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
-            apply_r_point<T, S>(x, Rs, m, j);
+            apply_r_point<T, S>(x, Rs, rstride, j);
 #pragma unroll
             for (int s = 0; s < S; ++s) v[s][r] = x[s];
         }
@@ -384,7 +387,7 @@ template <typename T, int S, int C> struct LineSolver {
             for (int s = 0; s < S; ++s) x[s] = scale<T>(v[s][r], inv_n);
             if (prop) {
                 if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
-                apply_r_point<T, S>(x, Rs, m, j);
+                apply_r_point<T, S>(x, Rs, rstride, j);
                 if (fuse_obs) observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f);
             }
 #pragma unroll
@@ -609,11 +612,12 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
     X.bufB = X.bufA + S * X.ldp;
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(X.bufB + S * X.ldp);
     Tab<T>* twc = twm + X.m;
-    Tab<T>* Rs = twc + (C > 1 ? X.m : 0);
-    Tab<T>* eks = Rs + NSYM * X.m;
+    Tab<T>* Rs = J.r_global ? J.R + X.base : twc + (C > 1 ? X.m : 0);
+    Tab<T>* eks = twc + (C > 1 ? X.m : 0) + (J.r_global ? 0 : NSYM * X.m);
     X.twm = twm;
     X.twc = twc;
     X.Rs = Rs;
+    X.rstride = J.r_global ? J.n : J.m;
     X.eks = eks;
     X.capw = J.capw ? J.capw + X.base : nullptr;
     X.Ug = J.U ? J.U + X.base : nullptr;
@@ -632,10 +636,11 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
         if (C > 1) twc[t] = J.tw[cta * t];
         eks[t] = J.expk[X.base + t];
     }
-    for (int e = threadIdx.x; e < NSYM * m; e += blockDim.x) {
-        const int c = e / m, j = e - c * m;
-        Rs[e] = J.R[(size_t)c * n + X.base + j];
-    }
+    if (!J.r_global)
+        for (int e = threadIdx.x; e < NSYM * m; e += blockDim.x) {
+            const int c = e / m, j = e - c * m;
+            Rs[e] = J.R[(size_t)c * n + X.base + j];
+        }
     __syncthreads();
 
     LineCtx<T> ctx{&J, X.cur, nullptr, &rs, m, n, X.logm, X.q, X.ldp, cta, X.base};
@@ -649,7 +654,7 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
         X.zero_acc();
         X.fuse_obs = i > 0 && !J.itp && !J.td;
         if (i > 0) { // Propagator.step (quantum_dynamics.zig:417-427)
-            if (J.td) line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.lo, X.span);
+            if (J.td) line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.rstride, X.lo, X.span);
             X.prop = true;
             X.inverse(X.forward());
             ctx.psi = X.cur;
@@ -658,7 +663,7 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
             line_orthogonalize<T, S, C>(ctx);
             line_normalize<T, S, C>(ctx);
         }
-        if (J.td) line_ham_update<T, S, C>(ctx, (double)i * J.tstep, false, Rs, X.lo, X.span);
+        if (J.td) line_ham_update<T, S, C>(ctx, (double)i * J.tstep, false, Rs, X.rstride, X.lo, X.span);
         if (!X.fuse_obs) X.observe_x();
         if (X.f.mom || X.f.ekin) {
             X.roundtrip();

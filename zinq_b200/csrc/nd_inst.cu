@@ -324,6 +324,15 @@ int enqueue(zqd_job* J) {
 // A run is a fixed sequence of launches: it is captured into a CUDA graph on the
 // first call and the graph is replayed by every later call on the job.
 int ZQD_ND_RUN(zqd_job* J) {
+    if (!J->nd_use_graph) {
+        ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+        const int rc = enqueue(J);
+        if (rc) return rc;
+        ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
+        return ZQD_OK;
+    }
     if (!J->nd_graph) {
         ZQD_CUDA(cudaStreamBeginCapture(J->stream, cudaStreamCaptureModeThreadLocal));
         const int rc = enqueue(J);

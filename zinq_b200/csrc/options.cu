@@ -2,6 +2,7 @@
 // src/quantum_dynamics.zig:606-710), potential upload and twiddle tables.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "internal.h"
 
@@ -178,11 +179,37 @@ int validate(const Opts& o) {
     return ZQD_OK;
 }
 
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    static std::mutex mu;
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64 && !configured[dev]) { // keep freed blocks for reuse instead of releasing them
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            configured[dev] = true;
+        }
+    }
+    e = cudaMallocAsync(p, bytes, cudaStreamPerThread);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread); // usable from any stream after this
+    return e;
+}
+
+void dev_free(void* p) {
+    if (p) cudaFreeAsync(p, cudaStreamPerThread);
+}
+
 PotStore::~PotStore() {
-    if (d_code) cudaFree(d_code);
-    if (d_consts) cudaFree(d_consts);
-    if (d_lvc) cudaFree(d_lvc);
-    if (d_file) cudaFree(d_file);
+    dev_free(d_code);
+    dev_free(d_consts);
+    dev_free(d_lvc);
+    dev_free(d_file);
 }
 
 int build_potential(const Opts& o, PotStore& ps) {
@@ -218,9 +245,9 @@ int build_potential(const Opts& o, PotStore& ps) {
             consts.insert(consts.end(), prog.consts.begin(), prog.consts.end());
         }
         if (consts.empty()) consts.push_back(0.0);
-        ZQD_CUDA(cudaMalloc(&ps.d_code, code.size() * sizeof(uint32_t)));
+        ZQD_CUDA(dev_alloc((void**)&ps.d_code, code.size() * sizeof(uint32_t)));
         ZQD_CUDA(cudaMemcpy(ps.d_code, code.data(), code.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        ZQD_CUDA(cudaMalloc(&ps.d_consts, consts.size() * sizeof(double)));
+        ZQD_CUDA(dev_alloc((void**)&ps.d_consts, consts.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(ps.d_consts, consts.data(), consts.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.code = ps.d_code;
         P.consts = ps.d_consts;
@@ -233,7 +260,7 @@ int build_potential(const Opts& o, PotStore& ps) {
         packed.insert(packed.end(), o.lvc_exc.begin(), o.lvc_exc.end());
         packed.insert(packed.end(), o.lvc_kappa.begin(), o.lvc_kappa.end());
         packed.insert(packed.end(), o.lvc_lambda.begin(), o.lvc_lambda.end());
-        ZQD_CUDA(cudaMalloc(&ps.d_lvc, packed.size() * sizeof(double)));
+        ZQD_CUDA(dev_alloc((void**)&ps.d_lvc, packed.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(ps.d_lvc, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.lvc = ps.d_lvc;
         ps.bytes += packed.size() * sizeof(double);
@@ -241,7 +268,7 @@ int build_potential(const Opts& o, PotStore& ps) {
         break;
     }
     case ZQD_POT_FILE: {
-        ZQD_CUDA(cudaMalloc(&ps.d_file, o.file_table.size() * sizeof(double)));
+        ZQD_CUDA(dev_alloc((void**)&ps.d_file, o.file_table.size() * sizeof(double)));
         ZQD_CUDA(cudaMemcpy(ps.d_file, o.file_table.data(), o.file_table.size() * sizeof(double), cudaMemcpyHostToDevice));
         P.file = ps.d_file;
         ps.bytes += o.file_table.size() * sizeof(double);

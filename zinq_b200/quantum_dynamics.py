@@ -386,3 +386,139 @@ def run_file(path: str, precision: str = "fp64"):
                 raise ZqdError(-7, f"method {tag!r} is outside this library")
             out.append(run(opt, precision, log=True))
     return out
+
+
+class Server:
+    """Request loop for streams of independent jobs (zqd_server_*): submit() returns a ticket at once,
+    wait() returns (Result, latency in ms from submission to completion)."""
+
+    def __init__(self, workers: int = 4, max_batch: int = 16, device_budget_bytes: int = 0):
+        self._L = _abi.load()
+        cfg = _abi.ZqdServerConfig()
+        self._L.zqd_server_config_init(C.byref(cfg))
+        cfg.workers, cfg.max_batch, cfg.device_budget_bytes = workers, max_batch, device_budget_bytes
+        self._h = C.c_void_p()
+        check(self._L.zqd_server_create(C.byref(cfg), C.byref(self._h)))
+        self._shapes = {}
+
+    def submit(self, opt: dict, precision: str = "fp32", initial_wavefunction=None) -> int:
+        o, keep = to_struct(opt, precision, False, initial_wavefunction)
+        t = C.c_uint64()
+        check(self._L.zqd_server_submit(self._h, C.byref(o), C.byref(t)))
+        self._shapes[t.value] = _shape(opt)
+        return t.value
+
+    def wait(self, ticket: int, want_wavefunction: bool = False):
+        res, lat = C.c_void_p(), C.c_double()
+        npt = self._shapes.pop(ticket, None)
+        check(self._L.zqd_server_wait(self._h, ticket, C.byref(res), C.byref(lat)))
+        try:
+            obs = _collect(res)
+            if want_wavefunction and obs:
+                _attach_wavefunctions(res, obs, npt, len(obs[0].pop))
+            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res)), lat.value
+        finally:
+            self._L.zqd_result_destroy(res)
+
+    def stats(self) -> dict:
+        s = _abi.ZqdServerStats()
+        check(self._L.zqd_server_stats_get(self._h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def close(self):
+        if self._h:
+            self._L.zqd_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers: int = 4, max_batch: int = 16):
+    """Submits opts[i] at arrivals_s[i] seconds after the start (a feeder thread sleeps until each
+    arrival), waits for all; returns (results, latencies_ms, wall_s from the first arrival to the
+    last completion, server stats)."""
+    import threading
+    import time
+
+    srv = Server(workers=workers, max_batch=max_batch)
+    tickets = [None] * len(opts)
+    errors = []
+    t0 = time.perf_counter()
+
+    def feed():
+        try:
+            for i, (o, a) in enumerate(zip(opts, arrivals_s)):
+                dt = a - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = srv.submit(o, precision)
+        except Exception as e:  # surfaced after the join
+            errors.append(e)
+
+    th = threading.Thread(target=feed)
+    th.start()
+    results, lats = [None] * len(opts), [0.0] * len(opts)
+    for i in range(len(opts)):
+        while tickets[i] is None and th.is_alive():
+            time.sleep(0.0005)
+        if tickets[i] is None:
+            break
+        results[i], lats[i] = srv.wait(tickets[i])
+    th.join()
+    wall = time.perf_counter() - t0 - (arrivals_s[0] if arrivals_s else 0.0)
+    st = srv.stats()
+    srv.close()
+    if errors:
+        raise errors[0]
+    return results, lats, wall, st
+
+
+def serving_stream(njobs: int, seed: int = 7, rate_per_s: float = 200.0, max_steps: int = 5000):
+    """The serving workload: njobs jobs with Poisson arrivals, parameters drawn from `seed`.
+    dims in {1, 2}; 1-D grids of 2^8..2^14 points on [-L, L], L ~ U(8, 32); 2-D grids of
+    2^6..2^9 points per axis on [-L, L]^2, L ~ U(8, 16); states in {1, 2, 3}; harmonic
+    (V_ii = 0.5 w^2 r^2 + c_i) or tanh-crossing (V_ii = +-A tanh(B r)) diabatic surfaces with
+    couplings C exp(-r^2); A, C, c_i ~ U(-0.02, 0.02); mass ~ U(1, 2000); steps ~ U{100..max_steps};
+    dt = 0.05 sqrt(mass); Gaussian at x0 = -L/3, p0 ~ U(0, 10), gamma 1.  Returns (opts, arrivals)."""
+    rng = np.random.default_rng(seed)
+    opts, arrivals, t = [], [], 0.0
+    for _ in range(njobs):
+        t += rng.exponential(1.0 / rate_per_s)
+        d = int(rng.integers(1, 3))
+        if d == 1:
+            n, L = 2 ** int(rng.integers(8, 15)), float(rng.uniform(8, 32))
+        else:
+            n, L = 2 ** int(rng.integers(6, 10)), float(rng.uniform(8, 16))
+        S = int(rng.integers(1, 4))
+        family = "harmonic" if rng.uniform() < 0.5 else "tanh"
+        A, Cc = rng.uniform(-0.02, 0.02), rng.uniform(-0.02, 0.02)
+        c = rng.uniform(-0.02, 0.02, S)
+        mass = float(rng.uniform(1, 2000))
+        steps = int(rng.integers(100, max_steps + 1))
+        p0 = float(rng.uniform(0, 10))
+        r2 = "r1^2" if d == 1 else "(r1^2+r2^2)"
+        w2 = 1.0 / mass  # omega^2: a well of the packet's own time scale
+        mat = []
+        for i in range(S):
+            row = []
+            for j in range(S):
+                if i == j:
+                    if family == "harmonic":
+                        row.append(f"0.5*{w2:.17g}*{r2}+{c[i]:.17g}")
+                    else:
+                        row.append(f"{(A if i % 2 == 0 else -A):.17g}*tanh(1.6*r1)")
+                else:
+                    row.append(f"{Cc:.17g}*exp(-{r2})")
+            mat.append(row)
+        opts.append({"grid": {"bounds": [[-L, L]] * d, "npoint": n},
+                     "initial_conditions": {"position": [-L / 3] + [0.0] * (d - 1), "momentum": [p0] + [0.0] * (d - 1),
+                                            "gamma": [1.0] * d, "state": 0, "adiabatic": False},
+                     "potential": {"custom": {"ndim": d, "matrix": mat}}, "mass": [mass] * d,
+                     "iterations": steps, "time_step": 0.05 * float(np.sqrt(mass)), "adiabatic": False,
+                     "write": {"population": "P"}})
+        arrivals.append(t)
+    return opts, arrivals
