@@ -15,7 +15,11 @@ Legs printed in one JSON line:
   e2e        zqd_run_batch through the public API from host options to host
              results (table setup, H2D, D2H inside the timed region);
   roofline   the resident line kernel against the measured HBM copy bandwidth;
-  cpu_baseline  the oracle port, single thread, on a bounded sample.
+  cpu_baseline  the oracle port, single thread, on a bounded sample;
+  nd         2-D 512^2 x 3 states, 3-D 128^3 (ITP and real time), 2-D 2048^2 x 2
+             states (larger than L2): FP32 and FP64 device time, HBM roofline;
+  serving    a seeded stream of 600 jobs (Poisson arrivals, 200 jobs/s) through
+             the job server: p50/p99 latency, throughput, FP32 vs FP64 error.
 `--impl reference` times the CPU restatement of the reference path (the
 oracle) with all host threads on the same workload.
 """
@@ -266,6 +270,42 @@ def nd_legs(qd, torch, flush, reps=2):
     return out
 
 
+SERVE_JOBS, SERVE_RATE, SERVE_MAX_STEPS = 600, 200.0, 1000
+
+
+def serving_leg(qd):
+    """The serving stream (seeded generator, Poisson arrivals at 200 jobs/s) through the job server:
+    p50/p99 submit-to-completion latency and throughput at that rate, throughput with every job
+    submitted at once (capacity), FP32 population error against the FP64 form job by job."""
+    import numpy as np
+
+    opts, arrivals = qd.serving_stream(SERVE_JOBS, seed=7, rate_per_s=SERVE_RATE, max_steps=SERVE_MAX_STEPS)
+    units = sum(o["grid"]["npoint"] ** len(o["grid"]["bounds"]) * len(o["potential"]["custom"]["matrix"]) * o["iterations"]
+                for o in opts)
+    w_opts, w_arr = qd.serving_stream(60, seed=8, rate_per_s=2000.0, max_steps=200)
+    qd.serve_stream(w_opts, w_arr, "fp32")  # warm-up: module loading, memory pool
+    qd.serve_stream(w_opts, w_arr, "fp64")
+    out = {"jobs": SERVE_JOBS, "arrival_rate_per_s": SERVE_RATE, "steps": f"100..{SERVE_MAX_STEPS}",
+           "workload": "seeded stream: 1-D 256..16384 pts or 2-D 64^2..512^2, 1-3 states, harmonic or tanh-crossing",
+           "units": units}
+    pops = {}
+    for prec in ("fp32", "fp64"):
+        res, lat, wall, st = qd.serve_stream(opts, arrivals, prec)
+        lat = np.asarray(lat)
+        _, lat_b, wall_b, _ = qd.serve_stream(opts, [0.0] * len(opts), prec)
+        out[prec] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "throughput": units / wall, "unit": UNIT, "wall_s": wall,
+                     "burst_throughput": units / wall_b, "burst_wall_s": wall_b,
+                     "grouped_launches": st["grouped_launches"], "grouped_jobs": st["grouped_jobs"],
+                     "peak_device_bytes": st["peak_device_bytes"]}
+        pops[prec] = [r.observables[0].history["population"] for r in res]
+    errs = [float(np.max(np.abs(a - b))) for a, b in zip(pops["fp32"], pops["fp64"])]
+    out["pop_err_fp32_vs_fp64"] = max(errs)
+    out["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs)
+    out["burst_fp32_over_fp64"] = out["fp32"]["burst_throughput"] / out["fp64"]["burst_throughput"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -274,6 +314,7 @@ def main():
     ap.add_argument("--impl", default="zinq_b200", choices=["zinq_b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-nd", action="store_true", help="skip the 2-D / 3-D legs")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
                     help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
     ap.add_argument("--nd-case", nargs=3, metavar=("WORKLOAD", "PRECISION", "STEPS"), default=None,
@@ -420,6 +461,8 @@ def main():
     }
     if not args.no_nd:
         line["nd"] = nd_legs(qd, torch, flush)
+    if not args.no_serve:
+        line["serving"] = serving_leg(qd)
     if not args.no_cpu:
         sample = workload(ITERS)[2:4]
         dt, _ = oracle_sample(sample, 1)
