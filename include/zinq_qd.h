@@ -203,6 +203,26 @@ int zqd_result_spectrum(const zqd_result* res, uint32_t solve, const double** ac
                         const double** sigma, size_t* nsigma);
 /* GPU time of the propagation kernels of the whole run, milliseconds (CUDA events) */
 double zqd_result_device_ms(const zqd_result* res);
+
+/* History.exportWrite (src/quantum_dynamics.zig:218-277): the recorded time series of solve
+   `solve` written as the reference's .mat text (writeMatrixLspace, src/read_write.zig:115-136:
+   a "rows cols" line, then per row the time 0 .. dt (rows - 1) and the values, each "%20.14f",
+   space-separated), and with the spectrum option the padded autocorrelation (time 0 .. dt
+   (rows - 1 + padding)) and the spectrum (frequency -pi/dt .. pi/dt (M - 2)/M).  A NULL path
+   skips that file; a series that was not recorded returns ZQD_ERR_NOT_FOUND. */
+typedef struct {
+    const char* acf;
+    const char* position;
+    const char* momentum;
+    const char* population;
+    const char* potential_energy;
+    const char* kinetic_energy;
+    const char* norm;
+    const char* total_energy;
+    const char* spectrum_acf;
+    const char* spectrum;
+} zqd_write_paths;
+int zqd_result_export(const zqd_result* res, uint32_t solve, const zqd_write_paths* paths);
 void zqd_result_destroy(zqd_result* res);
 
 /* --------------------------------------------------------------- method API
@@ -290,6 +310,15 @@ void zqd_expr_destroy(zqd_expr* e);
  * W ascending, U[k*n+m] = component k of eigenvector m.
  */
 int zqd_eigh_batch(uint32_t n, size_t count, const double* host_V, double* host_W, double* host_U);
+
+/* ------------------------------------------------------------ potential plot
+ * potential_plot.run (src/potential_plot.zig:48-106) on the device: V(r, time) at every point of
+ * the grid of opt (grid_bounds, npoint, potential; `adiabatic` puts the eigenvalues on the
+ * diagonal and zeros elsewhere).  host_U: npoint^ndim x nstate^2 values (may be NULL);
+ * write_path: the reference's .mat file (coordinates, then the matrix, "%20.14f"), or NULL.
+ * Only the grid, potential and adiabatic fields of opt are read.
+ */
+int zqd_potential_plot(const zqd_options* opt, double time, double* host_U, size_t capacity, const char* write_path);
 
 /* ------------------------------------------------------------------ server
  * A request loop around quantum_dynamics.run for streams of independent jobs

@@ -226,3 +226,41 @@ def test_longest_lines_read_the_propagator_table_from_global_memory(nstate, prec
         compare(opt)
     else:
         compare(opt, precision="fp32", pop_tol=FP32_POP_TOL, obs_tol=1e-4)
+
+
+# ---------------------------------------------------------------- .mat writers (History.exportWrite)
+def _read_mat(path):
+    with open(path) as f:
+        lines = f.read().splitlines()
+    rows, cols = map(int, lines[0].split())
+    body = lines[1:]
+    assert len(body) == rows
+    for line in body:  # every value "%20.14f": width 20, 14 decimals, one space apart
+        fields = [line[i:i + 20] for i in range(0, len(line), 21)]
+        assert len(fields) == cols and all(len(x) == 20 and x[-15] == "." for x in fields), line
+    return np.array([[float(x) for x in line.split()] for line in body])
+
+
+def test_history_files_match_the_result(tmp_path):
+    names = ["acf", "position", "momentum", "population", "potential_energy", "kinetic_energy", "norm", "total_energy"]
+    opt = tully("tully_1", False, npoint=256, iters=120)
+    opt["write"] = {n: str(tmp_path / f"{n}.mat") for n in names}
+    opt["spectrum"] = {"padding": 30, "threshold": 1e-4,
+                       "write": {"acf": str(tmp_path / "spec_acf.mat"), "spectrum": str(tmp_path / "spec.mat")}}
+    res = qd.run(opt, export=True).observables[0]
+    dt, rows = opt["time_step"], 121
+    for n in names:
+        m = _read_mat(tmp_path / f"{n}.mat")
+        np.testing.assert_allclose(m[:, 0], np.arange(rows) * dt, rtol=0, atol=1e-13)
+        h = res.history[n]
+        h = np.stack([h.real, h.imag], 1) if n == "acf" else h.reshape(rows, -1)
+        np.testing.assert_allclose(m[:, 1:], h, rtol=0, atol=6e-15)
+    acfp, sigma = res.spectrum
+    m = _read_mat(tmp_path / "spec_acf.mat")
+    assert m.shape == (len(acfp), 3)
+    np.testing.assert_allclose(m[-1, 0], (rows - 1 + 30) * dt, rtol=1e-14)
+    np.testing.assert_allclose(m[:, 1:], np.stack([acfp.real, acfp.imag], 1), rtol=0, atol=6e-15)
+    m = _read_mat(tmp_path / "spec.mat")
+    nt = len(sigma)
+    np.testing.assert_allclose(m[[0, -1], 0], [-np.pi / dt, np.pi / dt * (nt - 2) / nt], rtol=1e-14)
+    np.testing.assert_allclose(m[:, 1], sigma, rtol=0, atol=6e-15 * max(1.0, np.max(np.abs(sigma))))

@@ -103,3 +103,28 @@ def test_expression_vm_matches_oracle(text):
     ref = np.array([qd_ref.expr_eval(text, p, 0.7) for p in pts])
     # CUDA's and glibc's libm agree to a few ulp; the interpreter itself rounds every operation like the oracle
     np.testing.assert_allclose(out, ref, rtol=1e-13, atol=1e-14)
+
+
+def test_potential_plot_matches_expression_oracle_and_lapack(tmp_path):
+    from oracle import qd_ref
+    from zinq_b200 import quantum_dynamics as qd
+
+    mat = [["0.02*tanh(1.2*r1)+0.01*r2^2", "0.01*exp(-r1^2-r2^2)+0.001*t"],
+           ["0.01*exp(-r1^2-r2^2)+0.001*t", "-0.02*tanh(1.2*r1)+0.01*r2^2"]]
+    opt = {"potential": {"custom": {"ndim": 2, "matrix": mat, "time_dependent": True}},
+           "grid": {"bounds": [[-6, 6], [-4, 4]], "npoint": 16}, "time": 1.5,
+           "write": {"potential": str(tmp_path / "pot.mat")}}
+    U = qd.potential_plot(opt, write=True)
+    n = 16
+    r = np.array([[-6 + i * 12 / n, -4 + j * 8 / n] for i in range(n) for j in range(n)])
+    ref = np.array([[[qd_ref.expr_eval(mat[a][b], p, 1.5) for b in range(2)] for a in range(2)] for p in r])
+    np.testing.assert_allclose(U, ref, rtol=1e-13, atol=1e-15)
+    lines = open(tmp_path / "pot.mat").read().splitlines()
+    assert lines[0] == f"{n * n} 6"
+    rows = np.array([[float(x) for x in l.split()] for l in lines[1:]])
+    np.testing.assert_allclose(rows[:, :2], r, atol=1e-13)
+    np.testing.assert_allclose(rows[:, 2:], ref.reshape(-1, 4), atol=6e-15)
+    Ua = qd.potential_plot({**opt, "adiabatic": True})
+    w = np.linalg.eigvalsh(ref)
+    np.testing.assert_allclose(Ua[:, [0, 1], [0, 1]], w, rtol=1e-13, atol=1e-15)
+    assert np.all(Ua[:, 0, 1] == 0) and np.all(Ua[:, 1, 0] == 0)

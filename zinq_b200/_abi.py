@@ -72,6 +72,14 @@ class ZqdObservables(C.Structure):
     ]
 
 
+WRITE_PATH_FIELDS = ("acf", "position", "momentum", "population", "potential_energy", "kinetic_energy", "norm",
+                     "total_energy", "spectrum_acf", "spectrum")
+
+
+class ZqdWritePaths(C.Structure):
+    _fields_ = [(n, C.c_char_p) for n in WRITE_PATH_FIELDS]
+
+
 class ZqdServerConfig(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
                 ("device_budget_bytes", C.c_uint64)]
@@ -98,6 +106,7 @@ SIGNATURES = [
     ("zqd_result_spectrum", C.c_int, [VP, C.c_uint32, C.POINTER(DP), C.POINTER(C.c_size_t), C.POINTER(DP),
                                       C.POINTER(C.c_size_t)]),
     ("zqd_result_device_ms", C.c_double, [VP]),
+    ("zqd_result_export", C.c_int, [VP, C.c_uint32, C.POINTER(ZqdWritePaths)]),
     ("zqd_result_destroy", None, [VP]),
     ("zqd_run", C.c_int, [C.POINTER(ZqdOptions), C.POINTER(VP)]),
     ("zqd_job_create", C.c_int, [C.POINTER(ZqdOptions), C.POINTER(VP)]),
@@ -123,6 +132,7 @@ SIGNATURES = [
     ("zqd_expr_eval_points", C.c_int, [VP, DP, C.c_size_t, C.c_double, DP]),
     ("zqd_expr_destroy", None, [VP]),
     ("zqd_eigh_batch", C.c_int, [C.c_uint32, C.c_size_t, DP, DP, DP]),
+    ("zqd_potential_plot", C.c_int, [C.POINTER(ZqdOptions), C.c_double, DP, C.c_size_t, C.c_char_p]),
     ("zqd_server_config_init", None, [C.POINTER(ZqdServerConfig)]),
     ("zqd_server_create", C.c_int, [C.POINTER(ZqdServerConfig), C.POINTER(VP)]),
     ("zqd_server_submit", C.c_int, [VP, C.POINTER(ZqdOptions), C.POINTER(C.c_uint64)]),

@@ -98,6 +98,7 @@ struct zqd_result {
     std::vector<std::vector<double>> series_cache; // per (solve, series)
     double device_ms = 0;
     uint32_t write_mask = 0;
+    double time_step = 0;
     int hc = 0;
     uint64_t h2d = 0, d2h = 0;
 };

@@ -390,6 +390,7 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     R->npoint_total = J->N;
     R->hc = J->hc;
     R->write_mask = J->o.write_mask;
+    R->time_step = J->o.time_step;
     R->device_ms = J->last_ms;
     R->solves.resize(J->nsolve);
     for (int s = 0; s < J->nsolve; ++s) {

@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <cstdio>
+
 #include "internal.h"
 #include "line_kernel.cuh"
 
@@ -94,6 +96,67 @@ extern "C" int zqd_result_spectrum(const zqd_result* r, uint32_t s, const double
 
 extern "C" double zqd_result_device_ms(const zqd_result* r) { return r ? r->device_ms : 0.0; }
 
+namespace {
+// writeMatrixLspace (src/read_write.zig:115-136): "rows cols+1", then per row the grid value
+// start + step i (step = (end - start) / (rows - 1), 0 for one row) and the row's values
+int write_lspace(const char* path, const double* v, size_t rows, size_t cols, double start, double end) {
+    FILE* f = std::fopen(path, "w");
+    if (!f) return zqd::fail(ZQD_ERR_INVALID_INPUT, std::string("CANNOT OPEN ") + path);
+    std::vector<char> buf(1 << 16);
+    std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    std::fprintf(f, "%zu %zu\n", rows, cols + 1);
+    const double step = rows > 1 ? (end - start) / (double)(rows - 1) : 0.0;
+    for (size_t i = 0; i < rows; ++i) {
+        std::fprintf(f, "%20.14f ", start + step * (double)i);
+        for (size_t c = 0; c < cols; ++c) std::fprintf(f, "%20.14f%s", v[i * cols + c], c + 1 == cols ? "\n" : " ");
+    }
+    const bool ok = std::fflush(f) == 0;
+    std::fclose(f);
+    return ok ? ZQD_OK : zqd::fail(ZQD_ERR_INVALID_INPUT, std::string("WRITE FAILED: ") + path);
+}
+} // namespace
+
+extern "C" int zqd_result_export(const zqd_result* r, uint32_t s, const zqd_write_paths* paths) {
+    if (!r || !paths) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    if (s >= r->solves.size()) return fail(ZQD_ERR_NOT_FOUND, "SOLVE INDEX OUT OF RANGE");
+    const SolveOut& so = r->solves[s];
+    const double end = r->time_step * (double)(so.rows > 0 ? so.rows - 1 : 0);
+    const struct {
+        const char* path;
+        zqd_series which;
+    } series[] = {{paths->acf, ZQD_SERIES_ACF},
+                  {paths->position, ZQD_SERIES_POSITION},
+                  {paths->momentum, ZQD_SERIES_MOMENTUM},
+                  {paths->population, ZQD_SERIES_POPULATION},
+                  {paths->potential_energy, ZQD_SERIES_POTENTIAL_ENERGY},
+                  {paths->kinetic_energy, ZQD_SERIES_KINETIC_ENERGY},
+                  {paths->norm, ZQD_SERIES_NORM},
+                  {paths->total_energy, ZQD_SERIES_TOTAL_ENERGY}};
+    int rc;
+    for (const auto& e : series) {
+        if (!e.path) continue;
+        const double* data = nullptr;
+        size_t rows = 0, cols = 0;
+        if ((rc = zqd_result_series(r, s, e.which, &data, &rows, &cols))) return rc;
+        if ((rc = write_lspace(e.path, data, rows, cols, 0.0, end))) return rc;
+    }
+    if (paths->spectrum_acf || paths->spectrum) {
+        if (so.acfpad.empty()) return fail(ZQD_ERR_NOT_FOUND, "NO SPECTRUM WAS COMPUTED");
+        const size_t lp = so.acfpad.size() / 2;
+        if (paths->spectrum_acf) { // time axis extended by the padding (quantum_dynamics.zig:267-270)
+            const double pad = r->time_step * (double)(lp - so.rows);
+            if ((rc = write_lspace(paths->spectrum_acf, so.acfpad.data(), lp, 2, 0.0, end + pad))) return rc;
+        }
+        if (paths->spectrum) { // frequency axis from -pi/dt (quantum_dynamics.zig:271-275)
+            const double nyquist = 3.14159265358979323846 / r->time_step, nt = (double)so.sigma.size();
+            if ((rc = write_lspace(paths->spectrum, so.sigma.data(), so.sigma.size(), 1, -nyquist,
+                                   nyquist * (nt - 2) / nt)))
+                return rc;
+        }
+    }
+    return ZQD_OK;
+}
+
 extern "C" int zqd_result_transfer_bytes(const zqd_result* r, uint64_t* h2d, uint64_t* d2h) {
     if (!r) return fail(ZQD_ERR_INVALID_INPUT, "NULL RESULT");
     if (h2d) *h2d = r->h2d;
@@ -169,6 +232,103 @@ template <int S> __global__ void eigh_batch_kernel(const double* V, double* W, d
     eigh_dev<S>(v, w, u);
     for (int e = 0; e < S; ++e) W[i * S + e] = w[e];
     for (int e = 0; e < S * S; ++e) U[i * S * S + e] = u[e];
+}
+
+// potential_plot.run (src/potential_plot.zig:48-106): V(r, t) at every point of Grid.init's grid
+// (wavepacket.zig:55-74), or with `adiabatic` the eigenvalues on the diagonal and zeros elsewhere
+template <int S>
+static __global__ void potential_plot_kernel(PotDev pot, int d, int n, size_t N, double3 lo, double3 span, double t,
+                                             int adiabatic, double* __restrict__ U, double* __restrict__ R) {
+    const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    double r[3] = {0, 0, 0};
+    const double los[3] = {lo.x, lo.y, lo.z}, sps[3] = {span.x, span.y, span.z};
+    size_t q = g;
+    for (int l = 0; l < d; ++l) {
+        const int j = d - l - 1;
+        r[j] = __dadd_rn(los[j], __dmul_rn((double)(q % (size_t)n), sps[j]) / (double)n);
+        q /= (size_t)n;
+    }
+    for (int j = 0; j < d; ++j) R[g * d + j] = r[j];
+    double V[S * S];
+    pot_eval(pot, r, t, V);
+    if (adiabatic) {
+        double Vu[S * S], W[S], Uv[S * S];
+        for (int a = 0; a < S; ++a)
+            for (int b = 0; b < S; ++b) Vu[a * S + b] = V[(a < b ? a : b) * S + (a < b ? b : a)];
+        eigh_dev<S>(Vu, W, Uv);
+        for (int e = 0; e < S * S; ++e) V[e] = 0.0;
+        for (int a = 0; a < S; ++a) V[a * S + a] = W[a];
+    }
+    for (int e = 0; e < S * S; ++e) U[g * S * S + e] = V[e];
+}
+
+extern "C" int zqd_potential_plot(const zqd_options* opt, double time, double* host_U, size_t capacity,
+                                  const char* write_path) {
+    if (!opt) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    // only the grid and the potential are read; the propagation fields may be left unset
+    static const double zeros[3] = {0, 0, 0}, ones[3] = {1, 1, 1};
+    zqd_options in = *opt;
+    if (!in.ic_position) in.ic_position = zeros;
+    if (!in.ic_momentum) in.ic_momentum = zeros;
+    if (!in.ic_gamma) in.ic_gamma = ones;
+    if (!in.mass) in.mass = ones;
+    Opts o;
+    int rc = copy_options(&in, o);
+    if (rc) return rc;
+    if (o.ndim == 0 || o.ndim > ZQD_MAX_NDIM) return fail(ZQD_ERR_UNSUPPORTED, "GRID DIMENSION MUST BE 1..3");
+    if (o.npoint == 0) return fail(ZQD_ERR_INVALID_INPUT, "GRID POINT COUNT MUST BE GREATER THAN 0");
+    if ((uint32_t)o.pot_nd != o.ndim) return fail(ZQD_ERR_INVALID_INPUT, "POTENTIAL DIMENSION DOES NOT MATCH GRID DIMENSION");
+    if (o.pot_ns < 1 || o.pot_ns > ZQD_MAX_NSTATE) return fail(ZQD_ERR_UNSUPPORTED, "MORE THAN 4 ELECTRONIC STATES ARE NOT SUPPORTED");
+    const int d = (int)o.ndim, S = o.pot_ns, n = (int)o.npoint;
+    size_t N = 1;
+    for (int j = 0; j < d; ++j) N *= (size_t)n;
+    if (host_U && capacity < N * S * S) return fail(ZQD_ERR_INVALID_INPUT, "OUTPUT BUFFER TOO SMALL");
+    PotStore ps;
+    if ((rc = build_potential(o, ps))) return rc;
+    double3 lo = make_double3(0, 0, 0), span = make_double3(0, 0, 0);
+    double* los = &lo.x;
+    double* sps = &span.x;
+    for (int j = 0; j < d; ++j) {
+        los[j] = o.bounds[2 * j];
+        sps[j] = o.bounds[2 * j + 1] - o.bounds[2 * j];
+    }
+    double *dU = nullptr, *dR = nullptr;
+    cudaError_t err = dev_alloc((void**)&dU, N * S * S * sizeof(double));
+    if (!err) err = dev_alloc((void**)&dR, N * d * sizeof(double));
+    std::vector<double> U(N * S * S), R(N * d);
+    if (!err) {
+        const unsigned b = (unsigned)((N + 127) / 128);
+        const int adia = o.adiabatic ? 1 : 0;
+        switch (S) {
+        case 1: potential_plot_kernel<1><<<b, 128>>>(ps.dev, d, n, N, lo, span, time, adia, dU, dR); break;
+        case 2: potential_plot_kernel<2><<<b, 128>>>(ps.dev, d, n, N, lo, span, time, adia, dU, dR); break;
+        case 3: potential_plot_kernel<3><<<b, 128>>>(ps.dev, d, n, N, lo, span, time, adia, dU, dR); break;
+        default: potential_plot_kernel<4><<<b, 128>>>(ps.dev, d, n, N, lo, span, time, adia, dU, dR); break;
+        }
+        err = cudaGetLastError();
+    }
+    if (!err) err = cudaMemcpy(U.data(), dU, U.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    if (!err) err = cudaMemcpy(R.data(), dR, R.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    dev_free(dU);
+    dev_free(dR);
+    if (err) return fail(ZQD_ERR_DEVICE, cudaGetErrorString(err));
+    if (host_U) std::memcpy(host_U, U.data(), U.size() * sizeof(double));
+    if (write_path) { // writeMatrixHjoin(grid.r, U) (src/read_write.zig:79-110)
+        FILE* f = std::fopen(write_path, "w");
+        if (!f) return fail(ZQD_ERR_INVALID_INPUT, std::string("CANNOT OPEN ") + write_path);
+        std::vector<char> buf(1 << 16);
+        std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+        std::fprintf(f, "%zu %zu\n", N, (size_t)(d + S * S));
+        for (size_t g = 0; g < N; ++g) {
+            for (int j = 0; j < d; ++j) std::fprintf(f, "%20.14f ", R[g * d + j]);
+            for (int e = 0; e < S * S; ++e) std::fprintf(f, "%20.14f%s", U[g * S * S + e], e + 1 == S * S ? "\n" : " ");
+        }
+        const bool ok = std::fflush(f) == 0;
+        std::fclose(f);
+        if (!ok) return fail(ZQD_ERR_INVALID_INPUT, std::string("WRITE FAILED: ") + write_path);
+    }
+    return ZQD_OK;
 }
 
 extern "C" int zqd_eigh_batch(uint32_t n, size_t count, const double* hV, double* hW, double* hU) {

@@ -218,8 +218,22 @@ def _shape(opt):
     return int(g["npoint"]) ** len(g["bounds"])
 
 
+def _export(L, res_ptr, opt):
+    """History.exportWrite: writes the files named by opt["write"] and opt["spectrum"]["write"]; solve by
+    solve to the same paths, so the last solve's history remains, as in the reference."""
+    w = opt.get("write") or {}
+    sw = (opt.get("spectrum") or {}).get("write") or {}
+    vals = {n: w.get(n) for n in _abi.WRITE_PATH_FIELDS[:8]}
+    vals["spectrum_acf"], vals["spectrum"] = sw.get("acf"), sw.get("spectrum")
+    if not any(vals.values()):
+        return
+    paths = _abi.ZqdWritePaths(**{k: str(v).encode() for k, v in vals.items() if v})
+    for s in range(L.zqd_result_nsolve(res_ptr)):
+        check(L.zqd_result_export(res_ptr, s, C.byref(paths)))
+
+
 def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction: bool = True,
-        initial_wavefunction=None) -> Result:
+        initial_wavefunction=None, export: bool = False) -> Result:
     """quantum_dynamics.run on the GPU (src/quantum_dynamics.zig:567-603).
 
     initial_wavefunction replaces the initial Gaussian (e.g. the relaxed state of an
@@ -229,6 +243,8 @@ def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction
     res = C.c_void_p()
     check(L.zqd_run(C.byref(o), C.byref(res)))
     try:
+        if export:
+            _export(L, res, opt)
         obs = _collect(res)
         if want_wavefunction and obs:
             S = len(obs[0].pop)
@@ -375,8 +391,9 @@ def run_batch_e2e(opts: list, precision: str = "fp64"):
     return out, h2d, d2h
 
 
-def run_file(path: str, precision: str = "fp64"):
-    """Runs every quantum_dynamics job of a Zinq input file ({"zinq": [...]}, src/main.zig:63-73,122-135)."""
+def run_file(path: str, precision: str = "fp64", export: bool = True):
+    """Runs every quantum_dynamics job of a Zinq input file ({"zinq": [...]}, src/main.zig:63-73,122-135),
+    writing the files its `write` options name, like the reference."""
     with open(path) as f:
         doc = json.load(f)
     out = []
@@ -384,7 +401,7 @@ def run_file(path: str, precision: str = "fp64"):
         for tag, opt in entry.items():
             if tag != "quantum_dynamics":
                 raise ZqdError(-7, f"method {tag!r} is outside this library")
-            out.append(run(opt, precision, log=True))
+            out.append(run(opt, precision, log=True, export=export))
     return out
 
 
@@ -522,3 +539,31 @@ def serving_stream(njobs: int, seed: int = 7, rate_per_s: float = 200.0, max_ste
                      "write": {"population": "P"}})
         arrivals.append(t)
     return opts, arrivals
+
+
+def potential_plot(opt: dict, write: bool = False) -> np.ndarray:
+    """potential_plot.run (src/potential_plot.zig:48-106) on the device: the reference's options
+    {potential, grid, adiabatic, time, write: {potential: path}}; returns V (or the adiabatic
+    diagonal) as an array of npoint^ndim x nstate x nstate and, with write, writes the .mat file."""
+    L = _abi.load()
+    d = len(opt["grid"]["bounds"])
+    full = {"grid": opt["grid"], "potential": opt["potential"], "adiabatic": bool(opt.get("adiabatic", False)),
+            "initial_conditions": {"position": [0.0] * d, "momentum": [0.0] * d, "gamma": [1.0] * d, "state": 0},
+            "mass": [1.0] * d, "time_step": 1.0, "iterations": 0}
+    o, keep = to_struct(full)
+    (pname, pval), = opt["potential"].items()
+    if pname == "custom":
+        S = len(pval["matrix"])
+    elif pname == "lvc":
+        S = len(pval["excitation_energies"])
+    elif pname == "file":
+        table = pval["data"] if "data" in pval else read_matrix(pval["path"])
+        S = int(round(np.sqrt(np.asarray(table).shape[1] - int(pval["ndim"]))))
+    else:
+        S = 1 if pname in ("harmonic",) else 2
+    N = int(opt["grid"]["npoint"]) ** d
+    U = np.zeros(N * S * S)
+    path = ((opt.get("write") or {}).get("potential") if write else None)
+    check(L.zqd_potential_plot(C.byref(o), float(opt.get("time", 0.0)), U.ctypes.data_as(_abi.DP), U.size,
+                               path.encode() if path else None))
+    return U.reshape(N, S, S)
