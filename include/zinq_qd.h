@@ -221,8 +221,15 @@ typedef struct {
     const char* total_energy;
     const char* spectrum_acf;
     const char* spectrum;
+    const char* wavefunction; /* writeMatrixHjoin(grid.r, History.wfn): per grid point its coordinates, then
+                                 re, im of every state at every recorded step */
 } zqd_write_paths;
 int zqd_result_export(const zqd_result* res, uint32_t solve, const zqd_write_paths* paths);
+/* write.wavefunction history of solve `solve` (History.append, src/quantum_dynamics.zig:176-180; in
+   the adiabatic basis when `adiabatic`): rows x nstate x npoint_total complex values (re, im),
+   copied into out when capacity (doubles) suffices; out may be NULL to query the shape. */
+int zqd_result_wavefunction_series(const zqd_result* res, uint32_t solve, double* out, size_t capacity, size_t* rows,
+                                   size_t* npoint_total);
 void zqd_result_destroy(zqd_result* res);
 
 /* --------------------------------------------------------------- method API

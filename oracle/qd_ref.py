@@ -264,6 +264,11 @@ def run(opt: dict, nthreads: int = 1, want_wavefunction: bool = True, initial_wa
                     hist[name] = buf.reshape(rows, cols)
             if "acf" in hist:
                 hist["acf"] = hist["acf"][:, 0] + 1j * hist["acf"][:, 1]
+            cols = L.qr_hist(h, s, b"wfn", None)
+            if cols > 0:  # History.wfn: rows x S x N complex
+                buf = np.zeros(rows * cols)
+                L.qr_hist(h, s, b"wfn", _dptr(buf))
+                hist["wfn"] = (buf[0::2] + 1j * buf[1::2]).reshape(rows, S, N)
             wf = None
             if want_wavefunction:
                 buf = np.zeros(2 * S * N)

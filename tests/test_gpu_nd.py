@@ -205,3 +205,14 @@ def test_3d_spectrum_of_real_time_leg():
     r = qd_ref.run(opt, want_wavefunction=False)[0].spectrum
     np.testing.assert_allclose(g[0], r[0], rtol=0, atol=1e-10)
     assert float(np.max(np.abs(g[1] - r[1]))) <= 1e-9 * max(1.0, float(np.max(np.abs(r[1]))))
+
+
+def test_2d_wavefunction_history_adiabatic():
+    opt = {"grid": {"bounds": [[-10, 10], [-6, 6]], "npoint": 32},
+           "initial_conditions": {"position": [-3, 0], "momentum": [4, 0.5], "gamma": [1, 2], "state": 1,
+                                  "adiabatic": True},
+           "potential": {"custom": {"ndim": 2, "matrix": [["0.02*tanh(1.2*r1)+0.01*r2^2", "0.01*exp(-r1^2-r2^2)"],
+                                                          ["0.01*exp(-r1^2-r2^2)", "-0.02*tanh(1.2*r1)+0.01*r2^2"]]}},
+           "mass": [100, 50], "iterations": 40, "time_step": 0.5, "adiabatic": True,
+           "write": {"population": "P", "wavefunction": "W", "kinetic_energy": "T"}}
+    compare(opt)

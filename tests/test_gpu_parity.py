@@ -22,7 +22,7 @@ POP_TOL = 1e-12
 FP32_POP_TOL = 1e-5
 
 ORACLE_NAMES = {"position": "pos", "momentum": "mom", "population": "pop", "potential_energy": "epot",
-                "kinetic_energy": "ekin", "total_energy": "etot", "norm": "norm", "acf": "acf"}
+                "kinetic_energy": "ekin", "total_energy": "etot", "norm": "norm", "acf": "acf", "wavefunction": "wfn"}
 
 
 def psi_rel(g, r):
@@ -264,3 +264,19 @@ def test_history_files_match_the_result(tmp_path):
     nt = len(sigma)
     np.testing.assert_allclose(m[[0, -1], 0], [-np.pi / dt, np.pi / dt * (nt - 2) / nt], rtol=1e-14)
     np.testing.assert_allclose(m[:, 1], sigma, rtol=0, atol=6e-15 * max(1.0, np.max(np.abs(sigma))))
+
+
+# ---------------------------------------------------------------- wavefunction history (write.wavefunction)
+@pytest.mark.parametrize("adia", [False, True])
+def test_wavefunction_history_matches_oracle(adia, tmp_path):
+    opt = tully("tully_2", adia, npoint=256, iters=60)
+    opt["write"] = {"wavefunction": str(tmp_path / "wfn.mat"), "population": "P"}
+    gpu, ref, _ = compare(opt)
+    w = gpu.observables[0].history["wavefunction"]
+    assert w.shape == (61, 2, 256)
+    qd.run(opt, export=True)
+    lines = open(tmp_path / "wfn.mat").read().splitlines()
+    assert lines[0] == f"256 {1 + 2 * 2 * 61}"
+    row = np.array([float(x) for x in lines[5].split()])
+    np.testing.assert_allclose(row[0], -24 + 4 * 56 / 256, atol=1e-13)
+    np.testing.assert_allclose(row[1::2] + 1j * row[2::2], w[:, :, 4].ravel(), atol=6e-15 * 1.5)

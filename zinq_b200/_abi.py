@@ -73,7 +73,7 @@ class ZqdObservables(C.Structure):
 
 
 WRITE_PATH_FIELDS = ("acf", "position", "momentum", "population", "potential_energy", "kinetic_energy", "norm",
-                     "total_energy", "spectrum_acf", "spectrum")
+                     "total_energy", "spectrum_acf", "spectrum", "wavefunction")
 
 
 class ZqdWritePaths(C.Structure):
@@ -107,6 +107,8 @@ SIGNATURES = [
                                       C.POINTER(C.c_size_t)]),
     ("zqd_result_device_ms", C.c_double, [VP]),
     ("zqd_result_export", C.c_int, [VP, C.c_uint32, C.POINTER(ZqdWritePaths)]),
+    ("zqd_result_wavefunction_series", C.c_int, [VP, C.c_uint32, DP, C.c_size_t, C.POINTER(C.c_size_t),
+                                                 C.POINTER(C.c_size_t)]),
     ("zqd_result_destroy", None, [VP]),
     ("zqd_run", C.c_int, [C.POINTER(ZqdOptions), C.POINTER(VP)]),
     ("zqd_job_create", C.c_int, [C.POINTER(ZqdOptions), C.POINTER(VP)]),

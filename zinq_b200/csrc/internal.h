@@ -83,6 +83,7 @@ struct SolveOut {
     std::vector<double> fin;  // HC
     std::vector<double> psi;  // S x N complex, natural order
     std::vector<double> acfpad, sigma;
+    std::vector<double> wfn; // write.wavefunction: rows x S x N complex, natural order
 };
 
 // calcSpectrum of one solve from its device history (spectrum.cu)
@@ -99,6 +100,7 @@ struct zqd_result {
     double device_ms = 0;
     uint32_t write_mask = 0;
     double time_step = 0;
+    std::vector<double> grid; // bounds [ndim][2] and npoint, for the wavefunction file's coordinates
     int hc = 0;
     uint64_t h2d = 0, d2h = 0;
 };

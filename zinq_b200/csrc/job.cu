@@ -262,6 +262,9 @@ template <typename T> static int create_line(zqd_job* J) {
     if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
     if ((rc = J->jobs.alloc((size_t)J->nsolve * sizeof(LineJob<T>)))) return rc;
     if ((rc = J->scratch.alloc(n + 16))) return rc;
+    if ((J->o.write_mask & ZQD_WRITE_WAVEFUNCTION) &&
+        (rc = J->wfn_hist.alloc((size_t)J->nsolve * ((size_t)J->o.iterations + 1) * S * n * c)))
+        return rc;
     if (!J->o.ic_wfn.empty()) { // initial wavefunction in the cluster-permuted layout
         if ((rc = J->psi_init.alloc(S * n * c))) return rc;
         std::vector<cx<T>> h(S * n);
@@ -329,6 +332,7 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
     L.R = J->R.as<Tab<T>>();
     L.psi_init = J->psi_init.as<cx<T>>();
     L.r_global = J->r_global ? 1 : 0;
+    L.wfn_hist = J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + (size_t)s * ((size_t)o.iterations + 1) * J->S * J->n : nullptr;
     L.expk = J->expk.as<Tab<T>>();
     L.V = J->V.as<double>();
     L.U = J->U.as<double>();
@@ -391,6 +395,8 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     R->hc = J->hc;
     R->write_mask = J->o.write_mask;
     R->time_step = J->o.time_step;
+    R->grid = J->o.bounds;
+    R->grid.push_back((double)J->o.npoint);
     R->device_ms = J->last_ms;
     R->solves.resize(J->nsolve);
     for (int s = 0; s < J->nsolve; ++s) {
@@ -403,6 +409,24 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
                                            RowLayout{J->d, J->S}.acf(), so.rows, J->o, so, J->d2h);
             if (rc) return rc;
             R->d2h = J->d2h;
+        }
+        if (J->wfn_hist.p && so.rows) { // History.wfn of this solve
+            std::vector<cx<T>> w(so.rows * SN);
+            ZQD_CUDA(cudaMemcpy(w.data(), J->wfn_hist.as<cx<T>>() + (size_t)s * rows * SN, w.size() * sizeof(cx<T>),
+                                cudaMemcpyDeviceToHost));
+            J->d2h += w.size() * sizeof(cx<T>);
+            R->d2h = J->d2h;
+            so.wfn.resize(2 * w.size());
+            for (size_t st = 0; st < so.rows * J->S; ++st)
+                for (size_t p = 0; p < J->N; ++p) {
+                    size_t x = p;
+                    if (J->d == 1) { // position p = c*m + j holds grid index c + C*j
+                        const size_t c = p / J->m, j = p - c * J->m;
+                        x = c + (size_t)J->C * j;
+                    }
+                    so.wfn[2 * (st * J->N + x)] = (double)w[st * J->N + p].x;
+                    so.wfn[2 * (st * J->N + x) + 1] = (double)w[st * J->N + p].y;
+                }
         }
         const cx<T>* src = (s + 1 < J->nsolve) ? orth.data() + (size_t)s * SN : save.data();
         so.psi.resize(2 * SN);

@@ -51,6 +51,7 @@ struct zqd_job {
     zqd::DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
     zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
     zqd::DevBuf psi_init;               // initial wavefunction replacing the Gaussian (1-D: permuted layout)
+    zqd::DevBuf wfn_hist;               // write.wavefunction: [solve][step][S][N] (1-D: permuted layout)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)

@@ -670,6 +670,30 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
             ctx.psi = X.cur;
         }
         const double nrm = X.finish_row(J.hist + (size_t)i * HC);
+        if (J.wfn_hist) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
+            cx<T>* __restrict__ dst = J.wfn_hist + (size_t)i * S * n;
+            for (int j = threadIdx.x; j < m; j += blockDim.x) {
+                cx<T> x[S];
+#pragma unroll
+                for (int s = 0; s < S; ++s) x[s] = X.cur[s * X.ldp + padx<T>(j)];
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    cx<T> y = x[s];
+                    if (J.adiabatic && S > 1) {
+                        double re = 0, im = 0;
+#pragma unroll
+                        for (int k = 0; k < S; ++k) {
+                            const double u = J.U[(size_t)(k * S + s) * n + X.base + j];
+                            re += (double)x[k].x * u;
+                            im += (double)x[k].y * u;
+                        }
+                        y = mk<T>((T)re, (T)im);
+                    }
+                    dst[(size_t)s * n + X.base + j] = y;
+                }
+            }
+            __syncthreads(); // the next step's passes overwrite the buffers read here
+        }
         if (J.has_stop && nrm < J.stop_norm) { // stop_norm (quantum_dynamics.zig:933-944)
             rows = i + 1;
             break;

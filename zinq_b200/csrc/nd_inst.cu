@@ -84,8 +84,9 @@ struct Launch {
     // partial-sum regions (in blocks)
     size_t R0, R1, R2, K, G;
 
-    int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false, NdFin f = NdFin{}) {
+    int row(uint32_t mode, uint32_t obs, size_t region, bool nostop = false, NdFin f = NdFin{}, cx<T>* wout = nullptr) {
         NdJob<T> d = D;
+        d.wfn_out = wout;
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
         const size_t smem = nd_smem_bytes<T>(2, S * J->nd_rows, J->n);
         if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
@@ -174,6 +175,9 @@ int ZQD_ND_CREATE(zqd_job* J) {
     if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
     if ((rc = J->expk.alloc((size_t)J->d * n * (sizeof(double2) + sizeof(double4))))) return rc; // phases, axis table
     if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
+    if ((o.write_mask & ZQD_WRITE_WAVEFUNCTION) &&
+        (rc = J->wfn_hist.alloc((size_t)J->nsolve * (o.iterations + 1) * S * N * c)))
+        return rc;
     if (!o.ic_wfn.empty()) { // initial wavefunction, natural order
         if ((rc = J->psi_init.alloc((size_t)S * N * c))) return rc;
         std::vector<cx<T>> h((size_t)S * N);
@@ -243,6 +247,10 @@ int enqueue(zqd_job* J) {
         if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc;
         nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
         ZQD_CUDA(cudaGetLastError());
+        // this solve's wavefunction history entry of step i (write.wavefunction), or null
+        auto whist = [&](int i) -> cx<T>* {
+            return J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + ((size_t)s * (iters + 1) + i) * S * N : nullptr;
+        };
         // finalize descriptors, run by the last CTA of the launch that ends a step
         auto fin = [&](int kind, size_t x0, size_t x1, bool k, uint32_t mask, double* row, int i) {
             NdFin f{};
@@ -285,7 +293,7 @@ int enqueue(zqd_job* J) {
                 if (i > 0) mode |= RM_INV | RM_REND;
                 if (i < iters) mode |= RM_RSTART | RM_FWD;
                 const NdFin f = fin(0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
-                if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f))) return rc;
+                if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f, whist(i)))) return rc;
                 if (needk && (rc = Lc.kobs(false, f))) return rc;
             } else {
                 if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
@@ -296,7 +304,7 @@ int enqueue(zqd_job* J) {
                 }
                 // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
                 const NdFin f = fin(0, i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
-                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f))) return rc;
+                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f, whist(i)))) return rc;
                 if (needk && (rc = Lc.kobs(false, f))) return rc;
                 if (i < iters) {
                     if (o.pot_td) {

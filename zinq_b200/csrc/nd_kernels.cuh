@@ -53,6 +53,7 @@ template <typename T> struct NdJob {
     cx<T>* phi;   // [S][N] scratch: the forward transform of the end-of-step psi
     cx<T>* psi0;  // [S][N] autocorrelation reference
     const cx<T>* psi_init; // [S][N] initial wavefunction replacing the Gaussian, or null
+    cx<T>* wfn_out;        // [S][N] this launch's entry of the wavefunction history, or null
     const cx<T>* orth; // [northo][S][N] relaxed states (imaginary time)
     Tab<T>* R;    // [NSYM][N]
     double* V;    // [S*S][N]
@@ -620,6 +621,23 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
             R.apply(v);
         }
         if (mode & RM_OBS) nd_observe<T, D, S>(J, v, g, obs, acc);
+        if (J.wfn_out) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                cx<T> y = v[i];
+                if (J.adiabatic && S > 1) {
+                    double re = 0, im = 0;
+#pragma unroll
+                    for (int k = 0; k < S; ++k) {
+                        const double u = J.U[(size_t)(k * S + i) * J.N + g];
+                        re += (double)v[k].x * u;
+                        im += (double)v[k].y * u;
+                    }
+                    y = mk<T>((T)re, (T)im);
+                }
+                J.wfn_out[(size_t)i * J.N + g] = y;
+            }
+        }
         if (phi_src)
 #pragma unroll
             for (int s = 0; s < S; ++s) phi_src[(s * L + l) * ldp + padx<T>(x)] = v[s];

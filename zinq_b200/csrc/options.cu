@@ -174,8 +174,13 @@ int validate(const Opts& o) {
             return fail(ZQD_ERR_EXPRESSION, "EXPRESSION V[" + std::to_string(e / o.custom_ns) + "][" +
                                                  std::to_string(e % o.custom_ns) + "] \"" + o.custom[e] + "\": " + err);
     }
-    if (o.write_mask & ZQD_WRITE_WAVEFUNCTION)
-        return fail(ZQD_ERR_UNSUPPORTED, "WAVEFUNCTION TIME SERIES OUTPUT IS NOT SUPPORTED");
+    if (o.write_mask & ZQD_WRITE_WAVEFUNCTION) { // History.wfn: (iterations + 1) x nstate x N complex per solve
+        double N = 1;
+        for (uint32_t i = 0; i < o.ndim; ++i) N *= (double)o.npoint;
+        const double bytes = ((double)o.iterations + 1) * o.pot_ns * N * 16.0 * (o.imag_nstate ? o.imag_nstate : 1);
+        if (bytes > 32.0 * 1024 * 1024 * 1024)
+            return fail(ZQD_ERR_UNSUPPORTED, "WAVEFUNCTION TIME SERIES LARGER THAN 32 GiB");
+    }
     return ZQD_OK;
 }
 

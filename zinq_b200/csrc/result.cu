@@ -116,6 +116,21 @@ int write_lspace(const char* path, const double* v, size_t rows, size_t cols, do
 }
 } // namespace
 
+extern "C" int zqd_result_wavefunction_series(const zqd_result* r, uint32_t s, double* out, size_t capacity, size_t* rows,
+                                              size_t* npoint_total) {
+    if (!r) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    if (s >= r->solves.size()) return fail(ZQD_ERR_NOT_FOUND, "SOLVE INDEX OUT OF RANGE");
+    const SolveOut& so = r->solves[s];
+    if (so.wfn.empty()) return fail(ZQD_ERR_NOT_FOUND, "SERIES WAS NOT RECORDED (write option not set)");
+    if (rows) *rows = so.rows;
+    if (npoint_total) *npoint_total = r->npoint_total;
+    if (out) {
+        if (capacity < so.wfn.size()) return fail(ZQD_ERR_INVALID_INPUT, "OUTPUT BUFFER TOO SMALL");
+        std::memcpy(out, so.wfn.data(), so.wfn.size() * sizeof(double));
+    }
+    return ZQD_OK;
+}
+
 extern "C" int zqd_result_export(const zqd_result* r, uint32_t s, const zqd_write_paths* paths) {
     if (!r || !paths) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
     if (s >= r->solves.size()) return fail(ZQD_ERR_NOT_FOUND, "SOLVE INDEX OUT OF RANGE");
@@ -139,6 +154,35 @@ extern "C" int zqd_result_export(const zqd_result* r, uint32_t s, const zqd_writ
         size_t rows = 0, cols = 0;
         if ((rc = zqd_result_series(r, s, e.which, &data, &rows, &cols))) return rc;
         if ((rc = write_lspace(e.path, data, rows, cols, 0.0, end))) return rc;
+    }
+    if (paths->wavefunction) { // writeMatrixHjoin(grid.r, wfn, 2 nstate index) (quantum_dynamics.zig:253-255)
+        if (so.wfn.empty()) return fail(ZQD_ERR_NOT_FOUND, "SERIES WAS NOT RECORDED (write option not set)");
+        const size_t N = r->npoint_total, S = r->nstate, d = r->ndim, n = (size_t)r->grid[2 * d];
+        FILE* f = std::fopen(paths->wavefunction, "w");
+        if (!f) return fail(ZQD_ERR_INVALID_INPUT, std::string("CANNOT OPEN ") + paths->wavefunction);
+        std::vector<char> buf(1 << 16);
+        std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+        std::fprintf(f, "%zu %zu\n", N, d + 2 * S * so.rows);
+        for (size_t g = 0; g < N; ++g) {
+            size_t q = g;
+            double x[3];
+            for (size_t l = 0; l < d; ++l) { // Grid.init (wavepacket.zig:55-74)
+                const size_t j = d - l - 1;
+                const double lo = r->grid[2 * j], hi = r->grid[2 * j + 1];
+                x[j] = lo + (double)(q % n) * (hi - lo) / (double)n;
+                q /= n;
+            }
+            for (size_t j = 0; j < d; ++j) std::fprintf(f, "%20.14f ", x[j]);
+            for (size_t t = 0; t < so.rows; ++t)
+                for (size_t s2 = 0; s2 < S; ++s2) {
+                    const size_t e = (t * S + s2) * N + g;
+                    const bool last = t + 1 == so.rows && s2 + 1 == S;
+                    std::fprintf(f, "%20.14f %20.14f%s", so.wfn[2 * e], so.wfn[2 * e + 1], last ? "\n" : " ");
+                }
+        }
+        const bool ok = std::fflush(f) == 0;
+        std::fclose(f);
+        if (!ok) return fail(ZQD_ERR_INVALID_INPUT, std::string("WRITE FAILED: ") + paths->wavefunction);
     }
     if (paths->spectrum_acf || paths->spectrum) {
         if (so.acfpad.empty()) return fail(ZQD_ERR_NOT_FOUND, "NO SPECTRUM WAS COMPUTED");

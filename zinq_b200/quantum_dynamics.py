@@ -194,6 +194,12 @@ def _collect(res_ptr):
                 a = np.ctypeslib.as_array(ptr, shape=(rows.value * cols.value,)).copy().reshape(rows.value, cols.value)
                 hist[name] = a[:, 0] + 1j * a[:, 1] if name == "acf" else a
         acf = None if np.isnan(ob.acf_re) else complex(ob.acf_re, ob.acf_im)
+        nr, nt = C.c_size_t(), C.c_size_t()
+        if L.zqd_result_wavefunction_series(res_ptr, s, None, 0, C.byref(nr), C.byref(nt)) == 0:
+            buf = np.zeros(2 * nr.value * S * nt.value)
+            check(L.zqd_result_wavefunction_series(res_ptr, s, buf.ctypes.data_as(_abi.DP), buf.size, C.byref(nr),
+                                                   C.byref(nt)))
+            hist["wavefunction"] = (buf[0::2] + 1j * buf[1::2]).reshape(nr.value, S, nt.value)
         spec = None
         ap, na, sg, ns = _abi.DP(), C.c_size_t(), _abi.DP(), C.c_size_t()
         if L.zqd_result_spectrum(res_ptr, s, C.byref(ap), C.byref(na), C.byref(sg), C.byref(ns)) == 0:
@@ -224,6 +230,7 @@ def _export(L, res_ptr, opt):
     w = opt.get("write") or {}
     sw = (opt.get("spectrum") or {}).get("write") or {}
     vals = {n: w.get(n) for n in _abi.WRITE_PATH_FIELDS[:8]}
+    vals["wavefunction"] = w.get("wavefunction")
     vals["spectrum_acf"], vals["spectrum"] = sw.get("acf"), sw.get("spectrum")
     if not any(vals.values()):
         return
