@@ -44,6 +44,7 @@ struct zqd_job {
     size_t smem = 0;
     bool fp32 = false;
     bool r_global = false; // 1-D: R read from global memory (the largest lines)
+    int lrmax = 3;         // 1-D: log2 of the largest local radix
     int nsolve = 1, hc = 0;
     zqd::PotStore pot;
     cudaStream_t stream = nullptr;

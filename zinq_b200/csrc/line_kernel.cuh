@@ -75,6 +75,7 @@ template <typename T> struct LineJob {
     const cx<T>* orth;
     const cx<T>* psi_init; // [S][n] permuted initial wavefunction replacing the Gaussian, or null
     int r_global;          // R read from global memory instead of shared memory
+    int lrmax;             // log2 of the largest local radix (threads per CTA = m >> lrmax)
     cx<T>* wfn_hist;       // [step][S][n] permuted wavefunction history of this solve, or null
     int northo;
     double* hist;

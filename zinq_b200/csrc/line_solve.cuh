@@ -314,6 +314,7 @@ template <typename T, int S, int C> struct LineSolver {
     const double* Vg;
     const cx<T>* psi0;
     int m, n, logm, q, ldp, cta;
+    int lrmax; // log2 of the largest radix of the local passes (3: radix 8, 2: radix 4 with twice the threads)
     size_t base;
     double lo, span, dr, dk, dkunit, mass;
     T inv_n;
@@ -445,7 +446,7 @@ template <typename T, int S, int C> struct LineSolver {
         cx<T>* in = a;
         cx<T>* out = b;
         while (rem > 0) {
-            const int LR = rem >= 3 ? 3 : rem;
+            const int LR = rem >= lrmax ? lrmax : rem; // radix 8 (lrmax 3) or 4 (lrmax 2), smaller at the end
             const bool last = rem == LR;
             if (LR == 3) {
                 if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
@@ -453,8 +454,10 @@ template <typename T, int S, int C> struct LineSolver {
                 else if (last) pass<8, SIGN, KL>(in, out, p, logp, xbuf);
                 else pass<8, SIGN, 0>(in, out, p, logp, xbuf);
             } else if (LR == 2) {
-                if (first) pass<4, SIGN, KF | KL>(in, out, p, logp, xbuf);
-                else pass<4, SIGN, KL>(in, out, p, logp, xbuf);
+                if (first && last) pass<4, SIGN, KF | KL>(in, out, p, logp, xbuf);
+                else if (first) pass<4, SIGN, KF>(in, out, p, logp, xbuf);
+                else if (last) pass<4, SIGN, KL>(in, out, p, logp, xbuf);
+                else pass<4, SIGN, 0>(in, out, p, logp, xbuf);
             } else {
                 if (first) pass<2, SIGN, KF | KL>(in, out, p, logp, xbuf);
                 else pass<2, SIGN, KL>(in, out, p, logp, xbuf);
@@ -597,6 +600,7 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
     X.m = J.m;
     X.n = J.n;
     X.logm = J.logm;
+    X.lrmax = J.lrmax;
     X.q = J.q;
     X.ldp = padded_len<T>(J.m);
     X.cta = cta;
