@@ -273,6 +273,61 @@ def nd_legs(qd, torch, flush, reps=2):
 SERVE_JOBS, SERVE_RATE, SERVE_MAX_STEPS = 600, 200.0, 1000
 
 
+def harmonic_1d():
+    """1-D harmonic oscillator, 1024 points on [-16, 16], psi0 ~ exp(-(x-1)^2/2), dt 0.1, 1000 steps."""
+    return {"grid": {"bounds": [[-16, 16]], "npoint": 1024},
+            "initial_conditions": {"position": [1], "momentum": [0], "gamma": [1], "state": 0},
+            "potential": {"harmonic": {"k": [1]}}, "mass": [1], "iterations": 1000, "time_step": 0.1,
+            "write": {"norm": "N", "total_energy": "E", "position": "X"}}
+
+
+def config_table(qd):
+    """Per-configuration rates in grid-pt*state*steps/s: the oracle on the host (one thread and all
+    threads, bounded samples of each workload) and the GPU forms, for the comparison table."""
+    import numpy as np
+
+    from oracle import qd_ref
+
+    nproc = os.cpu_count() or 1
+
+    def rate(opt, **kw):
+        d = len(opt["grid"]["bounds"])
+        S = 1 if "harmonic" in opt["potential"] else len(opt["potential"]["custom"]["matrix"])
+        u = opt["grid"]["npoint"] ** d * S * opt["iterations"] * max(1, (opt.get("imaginary") or {}).get("nstate", 1))
+        t0 = time.perf_counter()
+        qd_ref.run(opt, want_wavefunction=False, **kw)
+        return u / (time.perf_counter() - t0)
+
+    def sample(opt, iters):
+        o = dict(opt)
+        o["iterations"] = iters
+        return o
+
+    cases = [("1_harmonic_1d", harmonic_1d(), 1000), ("2_tanh_crossing_1d_p20", workload()[2], 1000),
+             ("3_coupled_2d_512sq", coupled_harmonic_2d(), 10), ("4_anharmonic_3d_128cube_itp", anharmonic_3d(500, True), 6),
+             ("4_anharmonic_3d_128cube_rt", anharmonic_3d(2000, False), 6)]
+    out = {"host_threads": nproc}
+    for name, opt, iters in cases:
+        o = sample(opt, iters)
+        row = {"cpu_1thread": rate(o, nthreads=1), "cpu_all": rate(o, nthreads=nproc), "cpu_sample_steps": iters}
+        for prec in ("fp64", "fp32"):
+            job = qd.Job(opt, prec)
+            job.run()
+            ms = statistics.mean([job.run() for _ in range(2)])
+            d = len(opt["grid"]["bounds"])
+            S = 1 if "harmonic" in opt["potential"] else len(opt["potential"]["custom"]["matrix"])
+            row["gpu_" + prec] = opt["grid"]["npoint"] ** d * S * opt["iterations"] / (ms / 1e3)
+            job.close()
+        out[name] = row
+    # serving: the oracle on a 50-job subset of the stream (steps <= 300), all threads, one job per thread
+    sub, _ = qd.serving_stream(50, seed=7, max_steps=300)
+    u = sum(o["grid"]["npoint"] ** len(o["grid"]["bounds"]) * len(o["potential"]["custom"]["matrix"]) * o["iterations"]
+            for o in sub)
+    dt, _ = oracle_sample(sub, nproc)
+    out["5_serving_subset_50jobs"] = {"cpu_all": u / dt}
+    return out
+
+
 def serving_leg(qd):
     """The serving stream (seeded generator, Poisson arrivals at 200 jobs/s) through the job server:
     p50/p99 submit-to-completion latency and throughput at that rate, throughput with every job
@@ -320,7 +375,15 @@ def main():
     ap.add_argument("--nd-case", nargs=3, metavar=("WORKLOAD", "PRECISION", "STEPS"), default=None,
                     help="run one 2-D/3-D workload (c3 | c4 | c4itp | wide) for STEPS steps twice and exit; "
                          "for ncu captures")
+    ap.add_argument("--table", action="store_true",
+                    help="print per-configuration CPU (oracle) and GPU rates as one JSON line and exit")
     args = ap.parse_args()
+
+    if args.table:
+        from zinq_b200 import quantum_dynamics as qd
+
+        print(json.dumps(config_table(qd)), flush=True)
+        return
 
     if args.nd_case:
         from zinq_b200 import quantum_dynamics as qd

@@ -142,14 +142,14 @@ template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
 // Cluster shape of a 1-D job: C CTAs of m = n/C points each, m/4 threads per CTA (one
 // radix-4 butterfly of every state per thread; radix 8 and m/8 threads where m/4 threads
 // exceed the kernel's limit).  The default is the smallest C whose CTA fits in shared memory
-// and holds at most `target` points (512: at 8192 points a cluster of 16 CTAs, measured
-// 18 % faster per step than 8 CTAs of 1024 points); ZQD_LINE_CLUSTER forces C and
-// ZQD_LINE_RADIX=8 the radix-8 passes (tuning sweeps).
+// and holds at most `target` points (256; measured per step: 8192 points on 16 CTAs 18 %
+// faster than on 8, 1024 points on 4 CTAs 15 % faster than on 2); ZQD_LINE_CLUSTER forces C
+// and ZQD_LINE_RADIX=8 the radix-8 passes (tuning sweeps).
 static int choose_line_shape(zqd_job* J) {
     const size_t budget = 205 * 1024; // dynamic shared memory per CTA
     int forced = 0;
     if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
-    const int target = 512;
+    const int target = 256;
     int fallback = -1;
     // pass 0: at most `target` points per CTA; 1: any size; 2: R read from global memory
     for (int pass = 0; pass < 3; ++pass) {
