@@ -137,8 +137,8 @@ int ZQD_ND_CREATE(zqd_job* J) {
     const Opts& o = J->o;
     const int n = J->n;
     // Launch shapes.  Row pass: L rows (all S states) per CTA, about 2048 points a CTA, at
-    // least two CTAs per SM where the grid allows, within the shared-memory budget (three
-    // line buffers: the final observables always need the momentum-space copy).
+    // least two CTAs per SM where the grid allows, within the shared-memory budget (two line
+    // buffers; one thread per 8-point group).
     // Tile pass: Tn lines per CTA, rows of Tn * c >= 32 bytes (one sector), shrunk from
     // 128 bytes until the grid has two CTAs per SM.
     const int budget = 200 * 1024, sms2 = 2 * 148;
@@ -154,8 +154,9 @@ int ZQD_ND_CREATE(zqd_job* J) {
     J->nd_row_threads = std::max(32, (S * L * n / 8 + 31) / 32 * 32);
     const int tmin = std::max(1, (int)(32 / c));
     int Tn = std::min(n, (int)(128 / c));
-    while (Tn > 1 && (Tn * n / 8 > 256 || nd_smem_bytes<T>(2, Tn, n) > (size_t)budget ||
-                      (Tn > tmin && (size_t)S * (N / n / Tn) < (size_t)sms2)))
+    // at most 256 threads, except that long lines keep one 32-byte sector per row (up to 512 threads)
+    while (Tn > 1 && ((Tn * n / 8 > 256 && (Tn > tmin || Tn * n / 8 > max_items)) ||
+                      nd_smem_bytes<T>(2, Tn, n) > (size_t)budget || (Tn > tmin && (size_t)S * (N / n / Tn) < (size_t)sms2)))
         Tn >>= 1;
     if (nd_smem_bytes<T>(2, Tn, n) > (size_t)budget || Tn * n / 8 > max_items)
         return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE TILE PASS");
