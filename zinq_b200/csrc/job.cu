@@ -150,11 +150,12 @@ static int choose_line_shape(zqd_job* J) {
     int forced = 0;
     if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
     const int target = 256;
-    int fallback = -1;
-    // pass 0: at most `target` points per CTA; 1: any size; 2: R read from global memory
+    // pass 0: the smallest C with at most `target` points per CTA; 1: the largest C that fits
+    // (fewest points per CTA); 2: the same with R read from global memory
     for (int pass = 0; pass < 3; ++pass) {
         const bool rg = pass == 2;
-        for (int C = 1; C <= 16; C <<= 1) {
+        for (int k = 0; k < 5; ++k) {
+            const int C = pass == 0 ? 1 << k : 16 >> k;
             if (forced && C != forced) continue;
             if (J->n % C) continue;
             const int m = J->n / C;
@@ -168,10 +169,7 @@ static int choose_line_shape(zqd_job* J) {
             if (lrmax == 2 && ((m >> 2) + 31) / 32 * 32 > tmax) lrmax = 3;
             const int threads = std::max(32, ((m >> lrmax) + 31) / 32 * 32);
             if (threads > tmax) continue;
-            if (pass == 0 && !forced && m > target) {
-                if (fallback < 0) fallback = C;
-                continue;
-            }
+            if (pass == 0 && !forced && m > target) continue;
             J->C = C;
             J->m = m;
             J->q = m / C;
