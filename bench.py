@@ -361,6 +361,22 @@ def serving_leg(qd):
     return out
 
 
+def max_over_ranks(x, dist, device):
+    """The largest of every rank's x (the timed region of the slowest replica); x itself without a group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank, world, steps, seconds_max):
+    """Whole-job throughput of `world` replicas: every rank's units over the slowest rank's time."""
+    return world * units_per_rank * steps / seconds_max
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -480,11 +496,7 @@ def main():
     barrier()
 
     def maxall(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(x, dist, "cuda")
 
     s32 = maxall(sum(t32) / 1e3)
     s64 = maxall(sum(t64) / 1e3)
@@ -494,8 +506,8 @@ def main():
     if rank != 0:
         return
 
-    value = world * U * args.steps / s32
-    v64 = world * U * args.steps / s64
+    value = replica_value(U, world, args.steps, s32)
+    v64 = replica_value(U, world, args.steps, s64)
     peak, peak_kind = measured_peak()
     per_launch = statistics.mean(t32) / 1e3  # one grouped launch runs the whole batch
     achieved = BYTES_PER_UNIT["fp32"] * U / per_launch / 1e9
