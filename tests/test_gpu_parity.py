@@ -280,3 +280,12 @@ def test_wavefunction_history_matches_oracle(adia, tmp_path):
     row = np.array([float(x) for x in lines[5].split()])
     np.testing.assert_allclose(row[0], -24 + 4 * 56 / 256, atol=1e-13)
     np.testing.assert_allclose(row[1::2] + 1j * row[2::2], w[:, :, 4].ravel(), atol=6e-15 * 1.5)
+
+
+def test_radix8_kernel_for_lines_above_the_radix4_thread_limit():
+    # 32768 points: CTAs of 2048 points, whose radix-4 passes would need more threads than allowed
+    opt = {"grid": {"bounds": [[-40, 40]], "npoint": 32768},
+           "initial_conditions": {"position": [-8], "momentum": [10], "gamma": [0.5], "state": 0, "adiabatic": False},
+           "potential": {"harmonic": {"k": [0.01]}}, "mass": [2000], "iterations": 100, "time_step": 1,
+           "adiabatic": False, "write": {"position": "X", "momentum": "K", "total_energy": "E"}}
+    compare(opt)

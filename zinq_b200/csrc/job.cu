@@ -144,7 +144,8 @@ template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
 // exceed the kernel's limit).  The default is the smallest C whose CTA fits in shared memory
 // and holds at most `target` points (256; measured per step: 8192 points on 16 CTAs 18 %
 // faster than on 8, 1024 points on 4 CTAs 15 % faster than on 2); ZQD_LINE_CLUSTER forces C
-// and ZQD_LINE_RADIX=8 the radix-8 passes (tuning sweeps).
+// (tuning sweeps).  Radix-8 kernels exist for 16-CTA clusters only (lines above 16384 points in
+// FP64, 32768 in FP32); radix-4-only kernels keep the instruction footprint small.
 static int choose_line_shape(zqd_job* J) {
     const size_t budget = 205 * 1024; // dynamic shared memory per CTA
     int forced = 0;
@@ -164,9 +165,9 @@ static int choose_line_shape(zqd_job* J) {
             if (smem > budget) continue;
             // radix 4 doubles the threads of a CTA (more warps to hide latency) where the limit allows
             int lrmax = 2;
-            if (const char* env = std::getenv("ZQD_LINE_RADIX")) lrmax = std::atoi(env) == 8 ? 3 : 2;
             const int tmax = J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value;
-            if (lrmax == 2 && ((m >> 2) + 31) / 32 * 32 > tmax) lrmax = 3;
+            if (((m >> 2) + 31) / 32 * 32 > tmax) lrmax = 3;
+            if (lrmax == 3 && C != 16) continue; // radix 8 is built for 16-CTA clusters only
             const int threads = std::max(32, ((m >> lrmax) + 31) / 32 * 32);
             if (threads > tmax) continue;
             if (pass == 0 && !forced && m > target) continue;
@@ -365,6 +366,7 @@ template <typename T> static int run_line(zqd_job* J) {
     J->h2d += descs.size() * sizeof(LineJob<T>);
     ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
     LaunchShape sh{J->S, J->C, J->E, J->threads, J->smem, J->stream};
+    sh.lrmax = J->lrmax;
     for (int s = 0; s < J->nsolve; ++s) {
         int rc = launch_line_s<T>(&sh, J->jobs.as<LineJob<T>>() + s, 1);
         if (rc) return rc;
@@ -625,6 +627,7 @@ extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, 
         g->members.push_back(a);
         g->fp32 = a->fp32;
         g->shape = LaunchShape{a->S, a->C, a->E, 0, 0, B->stream};
+        g->shape.lrmax = a->lrmax;
         for (uint32_t k = i + 1; k < njobs; ++k) {
             zqd_job* b = B->jobs[k].get();
             if (!done[k] && b->d == 1 && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C &&
@@ -677,6 +680,7 @@ int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, floa
             J->lrmax != a->lrmax)
             return fail(ZQD_ERR_INVALID_INPUT, "JOBS OF ONE GROUP MUST SHARE PRECISION, STATES AND CLUSTER SHAPE");
     LaunchShape sh{a->S, a->C, a->E, 0, 0, st};
+    sh.lrmax = a->lrmax;
     for (const zqd_job* J : jobs) {
         sh.threads = std::max(sh.threads, J->threads);
         sh.smem = std::max(sh.smem, J->smem);

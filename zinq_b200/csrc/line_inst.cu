@@ -13,8 +13,8 @@
 
 namespace zqd {
 
-template <int C> static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
-    auto kern = line_solve_kernel<ZQD_T, ZQD_S, C>;
+template <int C, int LRM> static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
+    auto kern = line_solve_kernel<ZQD_T, ZQD_S, C, LRM>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -39,13 +39,19 @@ template <int C> static int launch_one(const LaunchShape* J, const void* d_jobs,
     return ZQD_OK;
 }
 
+// Radix-4 kernels for every cluster size; radix 8 only with 16 CTAs, the one shape whose CTAs can
+// hold more points than radix-4 threads allow (the longest lines)
 int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
+    if (J->lrmax == 3) {
+        if (J->C == 16) return launch_one<16, 3>(J, dj, nj);
+        return fail(ZQD_ERR_UNSUPPORTED, "RADIX-8 LINE PASSES ARE BUILT FOR CLUSTERS OF 16 ONLY");
+    }
     switch (J->C) {
-    case 1: return launch_one<1>(J, dj, nj);
-    case 2: return launch_one<2>(J, dj, nj);
-    case 4: return launch_one<4>(J, dj, nj);
-    case 8: return launch_one<8>(J, dj, nj);
-    case 16: return launch_one<16>(J, dj, nj);
+    case 1: return launch_one<1, 2>(J, dj, nj);
+    case 2: return launch_one<2, 2>(J, dj, nj);
+    case 4: return launch_one<4, 2>(J, dj, nj);
+    case 8: return launch_one<8, 2>(J, dj, nj);
+    case 16: return launch_one<16, 2>(J, dj, nj);
     default: return fail(ZQD_ERR_UNSUPPORTED, "CLUSTER SIZE MUST BE 1, 2, 4, 8 OR 16");
     }
 }

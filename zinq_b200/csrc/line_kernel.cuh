@@ -267,6 +267,7 @@ struct LaunchShape {
     int S, C, E, threads;
     size_t smem;
     cudaStream_t stream;
+    int lrmax = 2; // log2 of the largest local radix: 2 (radix 4) or 3 (radix 8, 16-CTA clusters only)
 };
 
 

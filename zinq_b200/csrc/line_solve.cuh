@@ -295,7 +295,7 @@ enum PassKind : int { FWD_FIRST = 1, FWD_LAST = 2, INV_FIRST = 4, INV_LAST = 8 }
 
 // All state of one CTA's solve.  Every member function is force-inlined into
 // the kernel, so the members stay in registers (no closure objects, no stack).
-template <typename T, int S, int C> struct LineSolver {
+template <typename T, int S, int C, int LRM> struct LineSolver {
     static constexpr int NSYM = S * (S + 1) / 2;
     static constexpr int NV = NAcc<S>::value;
 
@@ -314,7 +314,6 @@ template <typename T, int S, int C> struct LineSolver {
     const double* Vg;
     const cx<T>* psi0;
     int m, n, logm, q, ldp, cta;
-    int lrmax; // log2 of the largest radix of the local passes (3: radix 8, 2: radix 4 with twice the threads)
     size_t base;
     double lo, span, dr, dk, dkunit, mass;
     T inv_n;
@@ -446,13 +445,17 @@ template <typename T, int S, int C> struct LineSolver {
         cx<T>* in = a;
         cx<T>* out = b;
         while (rem > 0) {
-            const int LR = rem >= lrmax ? lrmax : rem; // radix 8 (lrmax 3) or 4 (lrmax 2), smaller at the end
+            // largest radix 2^LRM (8, or 4 with twice the threads and only the radix-4/2 code compiled,
+            // which keeps the kernel's instruction footprint small), smaller at the end
+            const int LR = rem >= LRM ? LRM : rem;
             const bool last = rem == LR;
-            if (LR == 3) {
-                if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
-                else if (first) pass<8, SIGN, KF>(in, out, p, logp, xbuf);
-                else if (last) pass<8, SIGN, KL>(in, out, p, logp, xbuf);
-                else pass<8, SIGN, 0>(in, out, p, logp, xbuf);
+            if (LRM == 3 && LR == 3) {
+                if constexpr (LRM == 3) {
+                    if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
+                    else if (first) pass<8, SIGN, KF>(in, out, p, logp, xbuf);
+                    else if (last) pass<8, SIGN, KL>(in, out, p, logp, xbuf);
+                    else pass<8, SIGN, 0>(in, out, p, logp, xbuf);
+                }
             } else if (LR == 2) {
                 if (first && last) pass<4, SIGN, KF | KL>(in, out, p, logp, xbuf);
                 else if (first) pass<4, SIGN, KF>(in, out, p, logp, xbuf);
@@ -579,9 +582,9 @@ template <typename T, int S, int C> struct LineSolver {
     }
 };
 
-template <typename T, int S, int C>
+template <typename T, int S, int C, int LRM>
 __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel(const LineJob<T>* __restrict__ jobs) {
-    using Solver = LineSolver<T, S, C>;
+    using Solver = LineSolver<T, S, C, LRM>;
     constexpr int NSYM = Solver::NSYM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ LineJob<T> J;
@@ -600,7 +603,6 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
     X.m = J.m;
     X.n = J.n;
     X.logm = J.logm;
-    X.lrmax = J.lrmax;
     X.q = J.q;
     X.ldp = padded_len<T>(J.m);
     X.cta = cta;
