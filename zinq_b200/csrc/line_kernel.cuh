@@ -177,15 +177,21 @@ struct RedSmem {
 
 // Sums NV compensated accumulators over the cluster; every thread of every
 // CTA receives the same totals (fixed combination order: deterministic).
-// Consecutive calls alternate between two slots, so one cluster barrier per
-// call suffices: a CTA can only overwrite a slot after every CTA has passed
-// the barrier of the following call, i.e. after it finished reading.
-template <int NV, int C> __device__ __forceinline__ void cluster_sum(Acc (&a)[NV], double (&out)[NV], RedSmem* rs) {
+// Only the values whose bit is set in `active` (uniform over the cluster) are
+// reduced, the others come back as 0: a step that records one observable
+// pays for that one.  Consecutive calls alternate between two slots, so one
+// cluster barrier per call suffices: a CTA can only overwrite a slot after
+// every CTA has passed the barrier of the following call, i.e. after it
+// finished reading.
+template <int NV, int C>
+__device__ __forceinline__ void cluster_sum(Acc (&a)[NV], double (&out)[NV], RedSmem* rs, uint32_t active = ~0u) {
     static_assert(NV <= NRED, "too many reduction values");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
     const int slot = rs->slot_idx;
+    const bool mine = threadIdx.x < NV && ((active >> threadIdx.x) & 1u);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
+        if (!((active >> v) & 1u)) continue;
         double s = a[v].s, c = a[v].c;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
@@ -205,7 +211,7 @@ template <int NV, int C> __device__ __forceinline__ void cluster_sum(Acc (&a)[NV
         }
     }
     __syncthreads();
-    if (threadIdx.x < NV) {
+    if (mine) {
         Acc t;
         for (int w = 0; w < nw; ++w) {
             t.add(rs->warp[w][threadIdx.x][0]);
@@ -217,7 +223,8 @@ template <int NV, int C> __device__ __forceinline__ void cluster_sum(Acc (&a)[NV
     if constexpr (C > 1) {
         cg::cluster_group cl = cg::this_cluster();
         cl.sync();
-        if (threadIdx.x < NV) {
+        if (threadIdx.x < NV && !mine) rs->res[threadIdx.x] = 0.0;
+        if (mine) {
             Acc t;
             for (int cc = 0; cc < C; ++cc) {
                 const double* rem = cl.map_shared_rank(&rs->slot[slot][threadIdx.x][0], cc);
@@ -228,7 +235,7 @@ template <int NV, int C> __device__ __forceinline__ void cluster_sum(Acc (&a)[NV
         }
     } else {
         __syncthreads();
-        if (threadIdx.x < NV) rs->res[threadIdx.x] = rs->slot[slot][threadIdx.x][0] + rs->slot[slot][threadIdx.x][1];
+        if (threadIdx.x < NV) rs->res[threadIdx.x] = mine ? rs->slot[slot][threadIdx.x][0] + rs->slot[slot][threadIdx.x][1] : 0.0;
     }
     if (threadIdx.x == 0) rs->slot_idx = slot ^ 1; // every thread read slot_idx before the first barrier
     __syncthreads();

@@ -561,8 +561,13 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     }
     // reduce the step's accumulators; the row is written by one thread of the cluster
     __device__ __forceinline__ double finish_row(double* dst) {
+        // the values this step accumulated (the observe_* helpers add to no other slot)
+        uint32_t act = (f.norm ? 1u << A_NORM : 0u) | (f.pos ? 1u << A_POS : 0u) | (f.epot ? 1u << A_EPOT : 0u) |
+                       (f.acf ? 3u << A_ACFR : 0u) | (f.mom ? 1u << A_MOM : 0u) | (f.ekin ? 1u << A_EKIN : 0u);
+        if (f.pop) act |= ((1u << S) - 1u) << A_POP;
+        if (f.track) act |= ((1u << S) - 1u) << (A_POP + S);
         double out[NV];
-        cluster_sum<NV, C>(acc, out, rs);
+        cluster_sum<NV, C>(acc, out, rs, act);
 #pragma unroll
         for (int s = 0; s < S; ++s) pop_abs[s] += out[A_POP + S + s] * dr;
         const double norm = out[A_NORM] * dr;
