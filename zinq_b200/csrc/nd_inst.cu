@@ -77,6 +77,11 @@ NdJob<T> describe(zqd_job* J) {
     return D;
 }
 
+// Row CTAs of at most 256 threads with several states take the 256-thread kernel form (up
+// to 255 registers).  One state keeps the 512-thread form: its sweep fits in 128 registers
+// and two 256-thread CTAs per SM hide more latency than extra registers would.
+inline bool row_narrow(unsigned threads) { return S > 1 && threads <= 256; }
+
 struct Launch {
     zqd_job* J;
     NdJob<T> D;
@@ -89,8 +94,14 @@ struct Launch {
         d.wfn_out = wout;
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
         const size_t smem = nd_smem_bytes<T>(2, S * J->nd_rows, J->n);
-        if (D.d == 2) nd_row_kernel<T, 2, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
-        else nd_row_kernel<T, 3, S><<<(unsigned)nrow_blocks, J->nd_row_threads, smem, J->stream>>>(d, mode, obs, region, f);
+        const unsigned nb = (unsigned)nrow_blocks, nt = (unsigned)J->nd_row_threads;
+        if (row_narrow(nt)) {
+            if (D.d == 2) nd_row_kernel<T, 2, S, 256><<<nb, nt, smem, J->stream>>>(d, mode, obs, region, f);
+            else nd_row_kernel<T, 3, S, 256><<<nb, nt, smem, J->stream>>>(d, mode, obs, region, f);
+        } else {
+            if (D.d == 2) nd_row_kernel<T, 2, S, 512><<<nb, nt, smem, J->stream>>>(d, mode, obs, region, f);
+            else nd_row_kernel<T, 3, S, 512><<<nb, nt, smem, J->stream>>>(d, mode, obs, region, f);
+        }
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -208,7 +219,8 @@ int ZQD_ND_CREATE(zqd_job* J) {
     nd_kphase_kernel<T><<<(unsigned)((J->d * n + 127) / 128), 128, 0, J->stream>>>(
         D, J->expk.as<double2>(), const_cast<double4*>(D.axis));
     ZQD_CUDA(cudaGetLastError());
-    for (auto f : {nd_row_kernel<T, 2, S>, nd_row_kernel<T, 3, S>})
+    for (auto f : {nd_row_kernel<T, 2, S, 256>, nd_row_kernel<T, 3, S, 256>, nd_row_kernel<T, 2, S, 512>,
+                   nd_row_kernel<T, 3, S, 512>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
     for (auto f : {nd_tile_kernel<T, 2>, nd_tile_kernel<T, 3>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));

@@ -202,14 +202,17 @@ template <int D, int S> struct Slots {
 };
 
 // per-CTA reduction of NV compensated sums into slots [first, first + NV) of the
-// slot-major partial array part[NDV][P][2], at column `block` (fixed order)
+// slot-major partial array part[NDV][P][2], at column `block` (fixed order).  Only
+// the values whose bit is set in `active` (uniform over the CTA) are reduced; the
+// others are stored as zero without any work.
 template <int NV>
 __device__ __forceinline__ void block_partials(const double (&a)[NV], int first, double* __restrict__ part, size_t P,
-                                               size_t block) {
+                                               size_t block, uint32_t active = ~0u) {
     __shared__ double red[16][NV][2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
+        if (!((active >> v) & 1u)) continue;
         double s = a[v], c = 0.0; // a thread's plain sum over its few points, then compensated combination
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
@@ -230,10 +233,11 @@ __device__ __forceinline__ void block_partials(const double (&a)[NV], int first,
     __syncthreads();
     if (threadIdx.x < NV) {
         Acc t;
-        for (int w = 0; w < nw; ++w) {
-            t.add(red[w][threadIdx.x][0]);
-            t.c += red[w][threadIdx.x][1];
-        }
+        if ((active >> threadIdx.x) & 1u)
+            for (int w = 0; w < nw; ++w) {
+                t.add(red[w][threadIdx.x][0]);
+                t.c += red[w][threadIdx.x][1];
+            }
         const size_t o = ((size_t)(first + threadIdx.x) * P + block) * 2;
         part[o] = t.s;
         part[o + 1] = t.c;
@@ -653,8 +657,10 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
 
 // L rows of the last axis (all S states) per CTA:
 // global -> [inverse FFT] -> shared -> sweep -> [phi] -> [forward FFT] -> global
-template <typename T, int D, int S>
-__global__ void __launch_bounds__(512)
+// MAXT bounds the CTA size: the 256-thread form gives several states' sweep (R, the
+// observables, their sums) room in registers instead of spilling at 128.
+template <typename T, int D, int S, int MAXT>
+__global__ void __launch_bounds__(MAXT)
     nd_row_kernel(const __grid_constant__ NdJob<T> J, uint32_t mode, uint32_t obs, size_t part_base,
                   const __grid_constant__ NdFin F) {
     if (*J.stopped) return;
@@ -702,7 +708,19 @@ __global__ void __launch_bounds__(512)
 #pragma unroll
         for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
         nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr, ldp, L, row0, mode, obs, acc);
-        if (mode & (RM_OBS | RM_REND | RM_RSTART)) block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
+        if (mode & (RM_OBS | RM_REND | RM_RSTART)) {
+            // the slots this launch accumulates (nd_observe adds norm always, the rest by mask)
+            constexpr uint32_t sm = (1u << S) - 1u;
+            uint32_t act = 1u << SL::norm;
+            if (mode & RM_OBS) {
+                if (obs & WM_POS) act |= ((1u << D) - 1u) << SL::pos;
+                if (obs & (WM_EPOT | WM_ETOT)) act |= 1u << SL::epot;
+                if (obs & WM_ACF) act |= 3u << SL::acf;
+                if (obs & WM_POP) act |= sm << SL::pop;
+            }
+            if (J.track) act |= (sm << SL::abs) | (sm << SL::absn);
+            block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x, act);
+        }
 #pragma unroll
         for (int k = 0; k < ND_IPT; ++k) { // the next step's first-pass inputs; frees cur
             const int it = threadIdx.x + k * blockDim.x;
