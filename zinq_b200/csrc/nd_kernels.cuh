@@ -493,28 +493,6 @@ __device__ __forceinline__ void nd_fft_regs(cx<T> (&v)[ND_IPT][8], cx<T>* a, cx<
 }
 
 // ------------------------------------------------------------ row pass
-// accumAbsorbed at one grid point into slots [SLOT, SLOT + S) (quantum_dynamics.zig:470-500)
-template <typename T, int S, int SLOT, int NV>
-__device__ __forceinline__ void nd_absorbed(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, double (&acc)[NV]) {
-    const double w = J.capw[g];
-#pragma unroll
-    for (int i = 0; i < S; ++i) {
-        double are = 0, aim = 0;
-        if (J.adiabatic && S > 1) {
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const double u = J.U[(size_t)(k * S + i) * J.N + g];
-                are += (double)x[k].x * u;
-                aim += (double)x[k].y * u;
-            }
-        } else {
-            are = (double)x[i].x;
-            aim = (double)x[i].y;
-        }
-        acc[SLOT + i] += w * (are * are + aim * aim);
-    }
-}
-
 // the CTA's R entries of one point (complex symmetric, upper triangle stored)
 template <typename T, int S> struct RPoint {
     Tab<T> r[S * (S + 1) / 2];
@@ -540,10 +518,90 @@ template <typename T, int S> struct RPoint {
     }
 };
 
+// What the per-point stages of a row sweep read from global memory besides psi.  EAGER:
+// loaded for a batch of points before any of them is processed, so that the loads of the
+// batch are in flight together; otherwise each value is read where it is used (fewer live
+// registers, for several states).  R is loaded up front either way.
+template <typename T, int S, bool EAGER> struct NdAux {
+    static constexpr int NU = EAGER && S > 1 ? S * S : 1, NV = EAGER ? S * (S + 1) / 2 : 1, NZ = EAGER ? S : 1;
+    RPoint<T, S> R;
+    double w_;     // CAP weight 1 - decay^2 (accumAbsorbed)
+    double U_[NU]; // adiabatic eigenvectors, U_[k * S + i] = U_ki
+    double V_[NV]; // diabatic potential: row i from the diagonal on
+    cx<T> z_[NZ];  // autocorrelation reference
+    __device__ __forceinline__ double w(const NdJob<T>& J, size_t g) const {
+        if constexpr (EAGER) return w_;
+        else return J.capw[g];
+    }
+    __device__ __forceinline__ double u(const NdJob<T>& J, size_t g, int k, int i) const {
+        if constexpr (EAGER) return U_[NU > 1 ? k * S + i : 0];
+        else return J.U[(size_t)(k * S + i) * J.N + g];
+    }
+    // V_ik (i <= k), entry c of the row-by-row upper triangle
+    __device__ __forceinline__ double v(const NdJob<T>& J, size_t g, int c, int i, int k) const {
+        if constexpr (EAGER) return V_[NV > 1 ? c : 0];
+        else return J.V[(size_t)(i * S + k) * J.N + g];
+    }
+    __device__ __forceinline__ cx<T> z(const NdJob<T>& J, size_t g, int s) const {
+        if constexpr (EAGER) return z_[NZ > 1 ? s : 0];
+        else return J.psi0[(size_t)s * J.N + g];
+    }
+};
+// which parts of NdAux a sweep needs
+struct NdNeed {
+    bool R, w, U, V, z0;
+};
+
+template <typename T, int S, bool EAGER>
+__device__ __forceinline__ void nd_aux_load(const NdJob<T>& J, size_t g, const NdNeed& nd, NdAux<T, S, EAGER>& a) {
+    if (nd.R) a.R.load(J, g);
+    if constexpr (EAGER) {
+        if (nd.w) a.w_ = J.capw[g];
+        if constexpr (S > 1)
+            if (nd.U)
+#pragma unroll
+                for (int e = 0; e < S * S; ++e) a.U_[e] = J.U[(size_t)e * J.N + g];
+        if (nd.V) {
+            int c = 0;
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int k = i; k < S; ++k) a.V_[c++] = J.V[(size_t)(i * S + k) * J.N + g];
+        }
+        if (nd.z0)
+#pragma unroll
+            for (int s = 0; s < S; ++s) a.z_[s] = J.psi0[(size_t)s * J.N + g];
+    }
+}
+
+// accumAbsorbed at one grid point into slots [SLOT, SLOT + S) (quantum_dynamics.zig:470-500)
+template <typename T, int S, int SLOT, int NV, typename A>
+__device__ __forceinline__ void nd_absorbed(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, const A& a,
+                                            double (&acc)[NV]) {
+    const double w = a.w(J, g);
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        double are = 0, aim = 0;
+        if (J.adiabatic && S > 1) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const double u = a.u(J, g, k, i);
+                are += (double)x[k].x * u;
+                aim += (double)x[k].y * u;
+            }
+        } else {
+            are = (double)x[i].x;
+            aim = (double)x[i].y;
+        }
+        acc[SLOT + i] += w * (are * are + aim * aim);
+    }
+}
+
 // position-space observables at one point (Observables.init, quantum_dynamics.zig:300-360;
 // Wavefunction.norm/pos/pop/epot, wavepacket.zig:206-300)
-template <typename T, int D, int S, int NV>
-__device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, uint32_t obs, double (&acc)[NV]) {
+template <typename T, int D, int S, int NV, typename A>
+__device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S], size_t g, uint32_t obs, const A& a,
+                                           double (&acc)[NV]) {
     using SL = Slots<D, S>;
     double m2 = 0;
     const bool adia = J.adiabatic && S > 1;
@@ -561,13 +619,13 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
     }
     if (obs & (WM_EPOT | WM_ETOT)) { // V is symmetric: diagonal plus twice the upper triangle
         double e = 0;
+        int c = 0;
 #pragma unroll
         for (int i = 0; i < S; ++i) {
-            e += ((double)x[i].x * (double)x[i].x + (double)x[i].y * (double)x[i].y) * J.V[(size_t)(i * S + i) * J.N + g];
+            e += ((double)x[i].x * (double)x[i].x + (double)x[i].y * (double)x[i].y) * a.v(J, g, c++, i, i);
 #pragma unroll
             for (int k = i + 1; k < S; ++k)
-                e += 2.0 * ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) *
-                     J.V[(size_t)(i * S + k) * J.N + g];
+                e += 2.0 * ((double)x[i].x * (double)x[k].x + (double)x[i].y * (double)x[k].y) * a.v(J, g, c++, i, k);
         }
         acc[SL::epot] += e;
     }
@@ -575,7 +633,7 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
         double re = 0, im = 0;
 #pragma unroll
         for (int s = 0; s < S; ++s) {
-            const cx<T> z0 = J.psi0[(size_t)s * J.N + g];
+            const cx<T> z0 = a.z(J, g, s);
             re += (double)z0.x * (double)x[s].x + (double)z0.y * (double)x[s].y;
             im += (double)z0.x * (double)x[s].y - (double)z0.y * (double)x[s].x;
         }
@@ -588,7 +646,7 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
             double are = 0, aim = 0;
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-                const double u = J.U[(size_t)(k * S + i) * J.N + g];
+                const double u = a.u(J, g, k, i);
                 are += (double)x[k].x * u;
                 aim += (double)x[k].y * u;
             }
@@ -601,56 +659,74 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
 // end of step i     1/N (after the inverse transform), accumAbsorbed + R, observables;
 //                   the values are copied to `phi_src` when given (momentum observables)
 // start of step i+1 accumAbsorbed + R
-// R is loaded once per point for both applications.  Returns after a barrier.
+// R is loaded once per point for both applications.  With one state a thread takes its
+// points in batches of four and loads the global inputs of the whole batch first (its
+// loads would otherwise wait one after the other); several states keep one point at a
+// time within the registers.  Returns after a barrier.
 template <typename T, int D, int S, int NV>
 __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T>* phi_src, int ldp, int L, size_t row0,
                                              uint32_t mode, uint32_t obs, double (&acc)[NV]) {
     using SL = Slots<D, S>;
-    const int logn = J.logn, pts = L << logn;
+    constexpr int SB = S == 1 ? 4 : 1;
+    using Aux = NdAux<T, S, (SB > 1)>;
+    const int logn = J.logn, pts = L << logn, nt = blockDim.x;
     const T inv_n = (T)(1.0 / (double)J.N);
-    const bool useR = mode & (RM_REND | RM_RSTART);
-    for (int it = threadIdx.x; it < pts; it += blockDim.x) {
-        const int l = it >> logn, x = it & ((1 << logn) - 1);
-        const size_t g = row0 + it;
-        RPoint<T, S> R;
-        if (useR) R.load(J, g);
-        cx<T> v[S];
+    const bool obsv = mode & RM_OBS, adia = J.adiabatic && S > 1;
+    NdNeed nd;
+    nd.R = mode & (RM_REND | RM_RSTART);
+    nd.w = J.track && nd.R;
+    nd.U = adia && (nd.w || (obsv && (obs & WM_POP)) || J.wfn_out);
+    nd.V = obsv && (obs & (WM_EPOT | WM_ETOT));
+    nd.z0 = obsv && (obs & WM_ACF);
+    for (int it0 = threadIdx.x; it0 < pts; it0 += SB * nt) {
+        Aux a[SB];
 #pragma unroll
-        for (int s = 0; s < S; ++s) v[s] = buf[(s * L + l) * ldp + padx<T>(x)];
-        if (mode & RM_INV)
+        for (int b = 0; b < SB; ++b)
+            if (it0 + b * nt < pts) nd_aux_load<T, S>(J, row0 + it0 + b * nt, nd, a[b]);
 #pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = scale<T>(v[s], inv_n);
-        if (mode & RM_REND) {
-            if (J.track) nd_absorbed<T, S, SL::abs>(J, v, g, acc);
-            R.apply(v);
-        }
-        if (mode & RM_OBS) nd_observe<T, D, S>(J, v, g, obs, acc);
-        if (J.wfn_out) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
+        for (int b = 0; b < SB; ++b) {
+            const int it = it0 + b * nt;
+            if (it >= pts) break;
+            const int l = it >> logn, x = it & ((1 << logn) - 1);
+            const size_t g = row0 + it;
+            cx<T> v[S];
 #pragma unroll
-            for (int i = 0; i < S; ++i) {
-                cx<T> y = v[i];
-                if (J.adiabatic && S > 1) {
-                    double re = 0, im = 0;
+            for (int s = 0; s < S; ++s) v[s] = buf[(s * L + l) * ldp + padx<T>(x)];
+            if (mode & RM_INV)
 #pragma unroll
-                    for (int k = 0; k < S; ++k) {
-                        const double u = J.U[(size_t)(k * S + i) * J.N + g];
-                        re += (double)v[k].x * u;
-                        im += (double)v[k].y * u;
-                    }
-                    y = mk<T>((T)re, (T)im);
-                }
-                J.wfn_out[(size_t)i * J.N + g] = y;
+                for (int s = 0; s < S; ++s) v[s] = scale<T>(v[s], inv_n);
+            if (mode & RM_REND) {
+                if (J.track) nd_absorbed<T, S, SL::abs>(J, v, g, a[b], acc);
+                a[b].R.apply(v);
             }
-        }
-        if (phi_src)
+            if (obsv) nd_observe<T, D, S>(J, v, g, obs, a[b], acc);
+            if (J.wfn_out) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
 #pragma unroll
-            for (int s = 0; s < S; ++s) phi_src[(s * L + l) * ldp + padx<T>(x)] = v[s];
-        if (mode & RM_RSTART) {
-            if (J.track) nd_absorbed<T, S, SL::absn>(J, v, g, acc);
-            R.apply(v);
-        }
+                for (int i = 0; i < S; ++i) {
+                    cx<T> y = v[i];
+                    if (adia) {
+                        double re = 0, im = 0;
 #pragma unroll
-        for (int s = 0; s < S; ++s) buf[(s * L + l) * ldp + padx<T>(x)] = v[s];
+                        for (int k = 0; k < S; ++k) {
+                            const double u = a[b].u(J, g, k, i);
+                            re += (double)v[k].x * u;
+                            im += (double)v[k].y * u;
+                        }
+                        y = mk<T>((T)re, (T)im);
+                    }
+                    J.wfn_out[(size_t)i * J.N + g] = y;
+                }
+            }
+            if (phi_src)
+#pragma unroll
+                for (int s = 0; s < S; ++s) phi_src[(s * L + l) * ldp + padx<T>(x)] = v[s];
+            if (mode & RM_RSTART) {
+                if (J.track) nd_absorbed<T, S, SL::absn>(J, v, g, a[b], acc);
+                a[b].R.apply(v);
+            }
+#pragma unroll
+            for (int s = 0; s < S; ++s) buf[(s * L + l) * ldp + padx<T>(x)] = v[s];
+        }
     }
     __syncthreads();
 }
