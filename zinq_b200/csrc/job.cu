@@ -253,27 +253,41 @@ template <typename T> static int create_line(zqd_job* J) {
     const size_t c = sizeof(cx<T>);
     int rc;
     const size_t tb = sizeof(Tab<T>);
-    if ((rc = J->R.alloc(nsym * n * tb))) return rc;
-    if ((rc = J->expk.alloc(n * tb))) return rc;
-    if ((rc = J->V.alloc(S * S * n * sizeof(double)))) return rc;
-    if (S > 1 && (rc = J->U.alloc(S * S * n * sizeof(double)))) return rc;
-    if (J->o.has_cap && (rc = J->capw.alloc(n * sizeof(double)))) return rc;
-    if ((rc = J->tw.alloc(n * tb))) return rc;
-    if ((rc = J->psi_save.alloc(S * n * c))) return rc;
-    bool acf = J->o.has_spectrum || (J->o.write_mask & ZQD_WRITE_ACF);
-    if (acf && (rc = J->psi0.alloc(S * n * c))) return rc;
-    if (J->o.imag_nstate > 1 && (rc = J->orth.alloc((size_t)(J->o.imag_nstate - 1) * S * n * c))) return rc;
-    size_t rows = (size_t)J->o.iterations + 1;
-    if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double)))) return rc;
-    if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double)))) return rc;
-    if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
-    if ((rc = J->jobs.alloc((size_t)J->nsolve * sizeof(LineJob<T>)))) return rc;
-    if ((rc = J->scratch.alloc(n + 16))) return rc;
-    if ((J->o.write_mask & ZQD_WRITE_WAVEFUNCTION) &&
-        (rc = J->wfn_hist.alloc((size_t)J->nsolve * ((size_t)J->o.iterations + 1) * S * n * c)))
-        return rc;
+    // every buffer of the job in one pool block: one allocation (and one synchronisation)
+    // instead of one per buffer
+    const bool acf = J->o.has_spectrum || (J->o.write_mask & ZQD_WRITE_ACF);
+    const size_t rows = (size_t)J->o.iterations + 1;
+    const struct {
+        DevBuf* b;
+        size_t bytes;
+    } parts[] = {
+        {&J->R, nsym * n * tb},
+        {&J->expk, n * tb},
+        {&J->V, S * S * n * sizeof(double)},
+        {&J->U, S > 1 ? S * S * n * sizeof(double) : 0},
+        {&J->capw, J->o.has_cap ? n * sizeof(double) : 0},
+        {&J->tw, n * tb},
+        {&J->psi_save, S * n * c},
+        {&J->psi0, acf ? S * n * c : 0},
+        {&J->orth, J->o.imag_nstate > 1 ? (size_t)(J->o.imag_nstate - 1) * S * n * c : 0},
+        {&J->hist, (size_t)J->nsolve * rows * J->hc * sizeof(double)},
+        {&J->fin, (size_t)J->nsolve * J->hc * sizeof(double)},
+        {&J->rows, (size_t)J->nsolve * sizeof(int)},
+        {&J->jobs, (size_t)J->nsolve * sizeof(LineJob<T>)},
+        {&J->scratch, n + 16},
+        {&J->wfn_hist, (J->o.write_mask & ZQD_WRITE_WAVEFUNCTION) ? (size_t)J->nsolve * rows * S * n * c : 0},
+        {&J->psi_init, J->o.ic_wfn.empty() ? 0 : S * n * c},
+    };
+    auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t total = 0;
+    for (const auto& pt : parts) total += align(pt.bytes);
+    if ((rc = J->arena.alloc(total))) return rc;
+    size_t off = 0;
+    for (const auto& pt : parts) {
+        pt.b->view(J->arena.as<char>() + off, pt.bytes);
+        off += align(pt.bytes);
+    }
     if (!J->o.ic_wfn.empty()) { // initial wavefunction in the cluster-permuted layout
-        if ((rc = J->psi_init.alloc(S * n * c))) return rc;
         std::vector<cx<T>> h(S * n);
         for (size_t st = 0; st < S; ++st)
             for (size_t p = 0; p < n; ++p) {
@@ -290,8 +304,8 @@ template <typename T> static int create_line(zqd_job* J) {
     std::vector<double> tw = twiddles_f64(J->n);
     std::vector<Tab<T>> twt(n);
     for (size_t t = 0; t < n; ++t) twt[t] = mktab<T>(tw[2 * t], tw[2 * t + 1]);
+    // (a copy from pageable memory has read the host buffer when the call returns)
     ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twt.data(), n * tb, cudaMemcpyHostToDevice, J->stream));
-    ZQD_CUDA(cudaStreamSynchronize(J->stream));
     J->h2d += n * tb + J->pot.bytes;
     if ((rc = run_tables_s<T>(J))) return rc;
     ZQD_CUDA(cudaStreamSynchronize(J->stream));

@@ -14,8 +14,21 @@ namespace zqd {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    ~DevBuf() { dev_free(p); }
+    bool owned = true; // false: a view into another buffer (not freed here)
+    ~DevBuf() {
+        if (owned) dev_free(p);
+    }
+    // a view of b bytes at base (null when b is 0), owned by another DevBuf
+    void view(void* base, size_t b) {
+        if (owned) dev_free(p);
+        p = b ? base : nullptr;
+        bytes = b;
+        owned = false;
+    }
     int alloc(size_t b) {
+        if (owned) dev_free(p);
+        p = nullptr;
+        owned = true;
         bytes = b;
         if (b == 0) return ZQD_OK;
         cudaError_t e = dev_alloc(&p, b);
@@ -53,6 +66,7 @@ struct zqd_job {
     zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
     zqd::DevBuf psi_init;               // initial wavefunction replacing the Gaussian (1-D: permuted layout)
     zqd::DevBuf wfn_hist;               // write.wavefunction: [solve][step][S][N] (1-D: permuted layout)
+    zqd::DevBuf arena;                  // 1-D jobs: one pool block holding the buffers above (views)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)

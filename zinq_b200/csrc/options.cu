@@ -2,7 +2,9 @@
 // src/quantum_dynamics.zig:606-710), potential upload and twiddle tables.
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <unordered_map>
 
 #include "internal.h"
 
@@ -286,7 +288,7 @@ int build_potential(const Opts& o, PotStore& ps) {
     return ZQD_OK;
 }
 
-std::vector<double> twiddles_f64(int n) {
+static std::vector<double> compute_twiddles(int n) {
     // exp(-2 pi i t/n) with the angle reduced to the first octant in exact
     // integer arithmetic, evaluated in long double and rounded once.
     std::vector<double> tw(2 * (size_t)n);
@@ -320,6 +322,25 @@ std::vector<double> twiddles_f64(int n) {
         tw[2 * t + 1] = (double)-s;
     }
     return tw;
+}
+
+// The long-double table costs about a millisecond at 8192 points; jobs of a batch or a
+// stream mostly share their lengths, so each length is computed once per process.
+std::vector<double> twiddles_f64(int n) {
+    static std::mutex mu;
+    static std::unordered_map<int, std::shared_ptr<const std::vector<double>>> cache;
+    std::shared_ptr<const std::vector<double>> t;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(n);
+        if (it != cache.end()) t = it->second;
+    }
+    if (!t) {
+        t = std::make_shared<const std::vector<double>>(compute_twiddles(n));
+        std::lock_guard<std::mutex> lk(mu);
+        cache.emplace(n, t);
+    }
+    return *t;
 }
 
 } // namespace zqd
