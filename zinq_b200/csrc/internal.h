@@ -65,11 +65,8 @@ int validate(const Opts& o);
 // Device resident potential description + its storage.
 struct PotStore {
     PotDev dev{};
-    uint32_t* d_code = nullptr;
-    double* d_consts = nullptr;
-    double* d_lvc = nullptr;
-    double* d_file = nullptr;
-    size_t bytes = 0; // uploaded to the device
+    void* d_blob = nullptr; // the potential's device data (program, constants or tables) in one block
+    size_t bytes = 0;       // uploaded to the device
     ~PotStore();
 };
 int build_potential(const Opts& o, PotStore& ps);

@@ -393,21 +393,66 @@ template <typename T> static int run_line(zqd_job* J) {
     return ZQD_OK;
 }
 
+// Per-thread pinned staging buffer for result copies (device-to-host copies into pageable
+// memory go through the driver's bounce buffer at a fraction of the bandwidth); null when
+// pinned memory cannot be had, and the caller copies directly.
+static char* pinned_staging(size_t bytes) {
+    struct Buf {
+        char* p = nullptr;
+        size_t n = 0;
+        ~Buf() {
+            if (p) cudaFreeHost(p);
+        }
+    };
+    thread_local Buf b;
+    if (b.n < bytes) {
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.n = 0;
+        const size_t want = std::max(bytes, (size_t)1 << 20);
+        if (cudaHostAlloc((void**)&b.p, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return nullptr;
+        }
+        b.n = want;
+    }
+    return b.p;
+}
+
 template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     size_t rows = (size_t)J->o.iterations + 1;
     std::vector<double> hist((size_t)J->nsolve * rows * J->hc), fin((size_t)J->nsolve * J->hc);
     std::vector<int> nrows(J->nsolve);
-    ZQD_CUDA(cudaMemcpyAsync(hist.data(), J->hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
-    ZQD_CUDA(cudaMemcpyAsync(fin.data(), J->fin.p, fin.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
-    ZQD_CUDA(cudaMemcpyAsync(nrows.data(), J->rows.p, nrows.size() * sizeof(int), cudaMemcpyDeviceToHost, J->stream));
     const size_t SN = (size_t)J->S * J->N;
-    std::vector<cx<T>> save(SN), orth;
-    ZQD_CUDA(cudaMemcpyAsync(save.data(), J->psi_save.p, SN * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
-    if (J->nsolve > 1) {
-        orth.resize((size_t)(J->nsolve - 1) * SN);
-        ZQD_CUDA(cudaMemcpyAsync(orth.data(), J->orth.p, orth.size() * sizeof(cx<T>), cudaMemcpyDeviceToHost, J->stream));
+    std::vector<cx<T>> save(SN), orth((size_t)(J->nsolve - 1) * SN);
+    const struct {
+        void* host;
+        const void* dev;
+        size_t bytes;
+    } parts[] = {{hist.data(), J->hist.p, hist.size() * sizeof(double)},
+                 {fin.data(), J->fin.p, fin.size() * sizeof(double)},
+                 {nrows.data(), J->rows.p, nrows.size() * sizeof(int)},
+                 {save.data(), J->psi_save.p, SN * sizeof(cx<T>)},
+                 {orth.data(), J->orth.p, orth.size() * sizeof(cx<T>)}};
+    size_t total = 0;
+    for (const auto& pt : parts) total += (pt.bytes + 15) & ~(size_t)15;
+    char* stage = pinned_staging(total);
+    size_t off = 0;
+    for (const auto& pt : parts) {
+        if (!pt.bytes) continue;
+        ZQD_CUDA(cudaMemcpyAsync(stage ? stage + off : pt.host, pt.dev, pt.bytes, cudaMemcpyDeviceToHost, J->stream));
+        off += (pt.bytes + 15) & ~(size_t)15;
     }
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    if (stage) {
+        off = 0;
+        for (const auto& pt : parts) {
+            if (!pt.bytes) continue;
+            std::memcpy(pt.host, stage + off, pt.bytes);
+            off += (pt.bytes + 15) & ~(size_t)15;
+        }
+    }
     J->d2h += (hist.size() + fin.size()) * sizeof(double) + nrows.size() * sizeof(int) +
               (save.size() + orth.size()) * sizeof(cx<T>);
     R->h2d = J->h2d;

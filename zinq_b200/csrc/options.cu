@@ -212,11 +212,16 @@ void dev_free(void* p) {
     if (p) cudaFreeAsync(p, cudaStreamPerThread);
 }
 
-PotStore::~PotStore() {
-    dev_free(d_code);
-    dev_free(d_consts);
-    dev_free(d_lvc);
-    dev_free(d_file);
+PotStore::~PotStore() { dev_free(d_blob); }
+
+// one device block for the potential's data: one allocation and one copy
+static int upload_blob(PotStore& ps, const std::vector<double>& blob) {
+    if (blob.empty()) return ZQD_OK;
+    const size_t b = blob.size() * sizeof(double);
+    ZQD_CUDA(dev_alloc(&ps.d_blob, b));
+    ZQD_CUDA(cudaMemcpy(ps.d_blob, blob.data(), b, cudaMemcpyHostToDevice));
+    ps.bytes += b;
+    return ZQD_OK;
 }
 
 int build_potential(const Opts& o, PotStore& ps) {
@@ -252,13 +257,14 @@ int build_potential(const Opts& o, PotStore& ps) {
             consts.insert(consts.end(), prog.consts.begin(), prog.consts.end());
         }
         if (consts.empty()) consts.push_back(0.0);
-        ZQD_CUDA(dev_alloc((void**)&ps.d_code, code.size() * sizeof(uint32_t)));
-        ZQD_CUDA(cudaMemcpy(ps.d_code, code.data(), code.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-        ZQD_CUDA(dev_alloc((void**)&ps.d_consts, consts.size() * sizeof(double)));
-        ZQD_CUDA(cudaMemcpy(ps.d_consts, consts.data(), consts.size() * sizeof(double), cudaMemcpyHostToDevice));
-        P.code = ps.d_code;
-        P.consts = ps.d_consts;
-        ps.bytes += code.size() * sizeof(uint32_t) + consts.size() * sizeof(double);
+        // constants first, then the program (two 32-bit words per double slot)
+        std::vector<double> blob(consts.size() + (code.size() + 1) / 2, 0.0);
+        std::memcpy(blob.data(), consts.data(), consts.size() * sizeof(double));
+        std::memcpy(blob.data() + consts.size(), code.data(), code.size() * sizeof(uint32_t));
+        int rc;
+        if ((rc = upload_blob(ps, blob))) return rc;
+        P.consts = static_cast<const double*>(ps.d_blob);
+        P.code = reinterpret_cast<const uint32_t*>(static_cast<const double*>(ps.d_blob) + consts.size());
         break;
     }
     case ZQD_POT_LVC: {
@@ -267,18 +273,16 @@ int build_potential(const Opts& o, PotStore& ps) {
         packed.insert(packed.end(), o.lvc_exc.begin(), o.lvc_exc.end());
         packed.insert(packed.end(), o.lvc_kappa.begin(), o.lvc_kappa.end());
         packed.insert(packed.end(), o.lvc_lambda.begin(), o.lvc_lambda.end());
-        ZQD_CUDA(dev_alloc((void**)&ps.d_lvc, packed.size() * sizeof(double)));
-        ZQD_CUDA(cudaMemcpy(ps.d_lvc, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
-        P.lvc = ps.d_lvc;
-        ps.bytes += packed.size() * sizeof(double);
+        int rc;
+        if ((rc = upload_blob(ps, packed))) return rc;
+        P.lvc = static_cast<const double*>(ps.d_blob);
         P.lvc_nm = (int)o.lvc_freq.size();
         break;
     }
     case ZQD_POT_FILE: {
-        ZQD_CUDA(dev_alloc((void**)&ps.d_file, o.file_table.size() * sizeof(double)));
-        ZQD_CUDA(cudaMemcpy(ps.d_file, o.file_table.data(), o.file_table.size() * sizeof(double), cudaMemcpyHostToDevice));
-        P.file = ps.d_file;
-        ps.bytes += o.file_table.size() * sizeof(double);
+        int rc;
+        if ((rc = upload_blob(ps, o.file_table))) return rc;
+        P.file = static_cast<const double*>(ps.d_blob);
         P.file_nrow = (int)o.file_nrow;
         P.file_ncol = (int)o.file_ncol;
         P.file_size = (int)std::llround(std::pow((double)o.file_nrow, 1.0 / (double)o.file_nd));
