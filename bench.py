@@ -331,7 +331,8 @@ def config_table(qd):
 def serving_leg(qd):
     """The serving stream (seeded generator, Poisson arrivals at 200 jobs/s) through the job server:
     p50/p99 submit-to-completion latency and throughput at that rate, throughput with every job
-    submitted at once (capacity), FP32 population error against the FP64 form job by job."""
+    submitted at once (capacity), FP32 population error against the FP64 form job by job; the same
+    for precision "auto" (FP32 unless a job's smallest adiabatic gap is below 1e-3 Hartree)."""
     import numpy as np
 
     opts, arrivals = qd.serving_stream(SERVE_JOBS, seed=7, rate_per_s=SERVE_RATE, max_steps=SERVE_MAX_STEPS)
@@ -343,8 +344,8 @@ def serving_leg(qd):
     out = {"jobs": SERVE_JOBS, "arrival_rate_per_s": SERVE_RATE, "steps": f"100..{SERVE_MAX_STEPS}",
            "workload": "seeded stream: 1-D 256..16384 pts or 2-D 64^2..512^2, 1-3 states, harmonic or tanh-crossing",
            "units": units}
-    pops = {}
-    for prec in ("fp32", "fp64"):
+    pops, forms = {}, {}
+    for prec in ("fp32", "fp64", "auto"):
         res, lat, wall, st = qd.serve_stream(opts, arrivals, prec)
         lat = np.asarray(lat)
         _, lat_b, wall_b, _ = qd.serve_stream(opts, [0.0] * len(opts), prec)
@@ -354,9 +355,14 @@ def serving_leg(qd):
                      "grouped_launches": st["grouped_launches"], "grouped_jobs": st["grouped_jobs"],
                      "peak_device_bytes": st["peak_device_bytes"]}
         pops[prec] = [r.observables[0].history["population"] for r in res]
+        forms[prec] = [r.precision for r in res]
     errs = [float(np.max(np.abs(a - b))) for a, b in zip(pops["fp32"], pops["fp64"])]
     out["pop_err_fp32_vs_fp64"] = max(errs)
     out["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs)
+    errs_auto = [float(np.max(np.abs(a - b))) for a, b in zip(pops["auto"], pops["fp64"])]
+    out["auto"]["pop_err_vs_fp64"] = max(errs_auto)
+    out["auto"]["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs_auto)
+    out["auto"]["jobs_fp64"] = sum(f == "fp64" for f in forms["auto"])
     out["burst_fp32_over_fp64"] = out["fp32"]["burst_throughput"] / out["fp64"]["burst_throughput"]
     return out
 

@@ -104,9 +104,17 @@ enum {
 };
 
 typedef enum {
-    ZQD_FP64 = 0,      /* plain form: complex FP64 throughout */
-    ZQD_FP32_MIXED = 1 /* FP32 state, butterflies and phases; FP64 tables, eigh and reductions */
+    ZQD_FP64 = 0,       /* plain form: complex FP64 throughout */
+    ZQD_FP32_MIXED = 1, /* FP32 state, butterflies and phases; FP64 tables, eigh and reductions */
+    ZQD_PRECISION_AUTO = 2 /* per job at creation: ZQD_FP32_MIXED, or ZQD_FP64 when the smallest gap
+                              between adiabatic surfaces on the grid (at t = 0) is below
+                              ZQD_AUTO_GAP_THRESHOLD, where FP32 rounding of the state accumulates
+                              in the population transfer of a near-degenerate crossing.  Not valid
+                              for zqd_fft_* */
 } zqd_precision;
+
+/* Smallest adiabatic gap (Hartree) that ZQD_PRECISION_AUTO propagates in FP32. */
+#define ZQD_AUTO_GAP_THRESHOLD 1e-3
 
 typedef struct {
     uint32_t struct_size; /* sizeof(zqd_options); set by zqd_options_init */
@@ -203,6 +211,8 @@ int zqd_result_spectrum(const zqd_result* res, uint32_t solve, const double** ac
                         const double** sigma, size_t* nsigma);
 /* GPU time of the propagation kernels of the whole run, milliseconds (CUDA events) */
 double zqd_result_device_ms(const zqd_result* res);
+/* The precision the job ran in (ZQD_FP64 or ZQD_FP32_MIXED; ZQD_PRECISION_AUTO resolved), -1 for NULL. */
+int zqd_result_precision(const zqd_result* res);
 
 /* History.exportWrite (src/quantum_dynamics.zig:218-277): the recorded time series of solve
    `solve` written as the reference's .mat text (writeMatrixLspace, src/read_write.zig:115-136:

@@ -137,3 +137,23 @@ def test_server_config_defaults_and_no_device_status():
     if not torch.cuda.is_available():
         h = C.c_void_p()
         assert lib.zqd_server_create(C.byref(cfg), C.byref(h)) == -12  # ZQD_ERR_NO_DEVICE
+
+
+def test_auto_precision_is_a_valid_job_option_but_not_an_fft_precision():
+    lib = _abi.load()
+    assert _abi.PRECISION["auto"] == 2
+    opt = copy.deepcopy(BASE)
+    opt["grid"]["npoint"] = 300  # fails after validation: the precision itself was accepted
+    with pytest.raises(qd.ZqdError) as e:
+        qd.Job(opt, "auto")
+    assert e.value.status == -7
+    o, keep = qd.to_struct(BASE, "fp64")
+    o.precision = 7
+    h = C.c_void_p()
+    assert lib.zqd_job_create(C.byref(o), C.byref(h)) == -1
+    assert "UNKNOWN PRECISION" in lib.zqd_last_error().decode()
+    shape = (C.c_int * 1)(64)
+    plan = C.c_void_p()
+    assert lib.zqd_fft_plan_create(1, shape, -1, 2, C.byref(plan)) == -1
+    assert "FFT PRECISION" in lib.zqd_last_error().decode()
+    assert lib.zqd_result_precision(None) == -1

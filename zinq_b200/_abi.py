@@ -26,7 +26,7 @@ WRITE = {"acf": 1 << 0, "kinetic_energy": 1 << 1, "momentum": 1 << 2, "norm": 1 
          "position": 1 << 5, "potential_energy": 1 << 6, "total_energy": 1 << 7, "wavefunction": 1 << 8}
 SERIES = {"position": 0, "momentum": 1, "population": 2, "potential_energy": 3, "kinetic_energy": 4,
           "total_energy": 5, "norm": 6, "acf": 7}
-PRECISION = {"fp64": 0, "fp32": 1}
+PRECISION = {"fp64": 0, "fp32": 1, "auto": 2}
 FFT_PLAN = {"estimate": 0, "measure": 1, "patient": 2, "exhaustive": 3}
 
 DP = C.POINTER(C.c_double)
@@ -106,6 +106,7 @@ SIGNATURES = [
     ("zqd_result_spectrum", C.c_int, [VP, C.c_uint32, C.POINTER(DP), C.POINTER(C.c_size_t), C.POINTER(DP),
                                       C.POINTER(C.c_size_t)]),
     ("zqd_result_device_ms", C.c_double, [VP]),
+    ("zqd_result_precision", C.c_int, [VP]),
     ("zqd_result_export", C.c_int, [VP, C.c_uint32, C.POINTER(ZqdWritePaths)]),
     ("zqd_result_wavefunction_series", C.c_int, [VP, C.c_uint32, DP, C.c_size_t, C.POINTER(C.c_size_t),
                                                  C.POINTER(C.c_size_t)]),

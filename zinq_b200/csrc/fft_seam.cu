@@ -50,6 +50,8 @@ extern "C" int zqd_fft_plan_create(uint32_t ndim, const int* shape, int sign, zq
     int n = shape[0];
     if (n < 2 || (n & (n - 1)) || n > 8192) return fail(ZQD_ERR_PLAN_FAILED, "FFT LENGTH MUST BE A POWER OF TWO 2..8192");
     if (sign != -1 && sign != 1) return fail(ZQD_ERR_PLAN_FAILED, "FFT SIGN MUST BE -1 OR +1");
+    if (precision != ZQD_FP64 && precision != ZQD_FP32_MIXED)
+        return fail(ZQD_ERR_INVALID_INPUT, "FFT PRECISION MUST BE ZQD_FP64 OR ZQD_FP32_MIXED");
     std::unique_ptr<zqd_fft> p(new zqd_fft());
     p->ndim = (int)ndim;
     p->n = n;
@@ -160,6 +162,8 @@ extern "C" int zqd_fft_execute_noalloc(uint32_t ndim, const int* shape, int sign
                                          "TABLE OF zqd_fft_execute_noalloc");
     if (n < 2 || (n & (n - 1))) return fail(ZQD_ERR_PLAN_FAILED, "FFT LENGTH MUST BE A POWER OF TWO 2..8192");
     if (sign != -1 && sign != 1) return fail(ZQD_ERR_PLAN_FAILED, "FFT SIGN MUST BE -1 OR +1");
+    if (precision != ZQD_FP64 && precision != ZQD_FP32_MIXED)
+        return fail(ZQD_ERR_INVALID_INPUT, "FFT PRECISION MUST BE ZQD_FP64 OR ZQD_FP32_MIXED");
     // device address of the static table, looked up once per device with that device current
     static std::mutex mu;
     static void* table[64] = {};

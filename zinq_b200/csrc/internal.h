@@ -95,6 +95,7 @@ struct zqd_result {
     std::vector<zqd::SolveOut> solves;
     std::vector<std::vector<double>> series_cache; // per (solve, series)
     double device_ms = 0;
+    zqd_precision precision = ZQD_FP64; // the form the job ran in
     uint32_t write_mask = 0;
     double time_step = 0;
     std::vector<double> grid; // bounds [ndim][2] and npoint, for the wavefunction file's coordinates

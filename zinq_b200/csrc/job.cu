@@ -26,6 +26,82 @@ template <typename T> struct LineTablesArgs {
     Tab<T>* expk;
 };
 
+// Smallest gap between adiabatic surfaces over the grid at t = 0 (ZQD_PRECISION_AUTO): the
+// eigenvalues of V at every point (eigh as in Hamiltonian.init, wavepacket.zig:96-143), the
+// smallest |W_i - W_k| per block, then an integer atomicMin on the bits (non-negative doubles
+// order like their bit patterns).
+struct GapArgs {
+    PotDev pot;
+    int d, n;
+    size_t N;
+    double lo[3], span[3];
+    unsigned long long* out;
+};
+template <int S> __global__ void min_gap_kernel(GapArgs a) {
+    double best = INFINITY;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < a.N; g += (size_t)gridDim.x * blockDim.x) {
+        double r[3];
+        size_t t = g;
+        for (int l = 0; l < a.d; ++l) { // last axis fastest (Grid.init, wavepacket.zig:55-74)
+            const int j = a.d - 1 - l;
+            r[j] = __dadd_rn(a.lo[j], __dmul_rn((double)(t % (size_t)a.n), a.span[j]) / (double)a.n);
+            t /= (size_t)a.n;
+        }
+        double V[S * S], Vu[S * S], W[S], U[S * S];
+        pot_eval(a.pot, r, 0.0, V);
+        for (int i = 0; i < S; ++i)
+            for (int k = 0; k < S; ++k) Vu[i * S + k] = V[(i < k ? i : k) * S + (i < k ? k : i)];
+        eigh_dev<S>(Vu, W, U);
+        for (int i = 0; i < S; ++i)
+            for (int k = i + 1; k < S; ++k) best = fmin(best, fabs(W[i] - W[k]));
+    }
+    for (int off = 16; off > 0; off >>= 1) best = fmin(best, __shfl_down_sync(0xffffffffu, best, off));
+    __shared__ double wmin[32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = fmin(best, wmin[w]);
+        atomicMin(a.out, (unsigned long long)__double_as_longlong(best));
+    }
+}
+
+// ZQD_PRECISION_AUTO -> ZQD_FP32_MIXED, or ZQD_FP64 below the gap threshold (one launch and
+// one synchronisation on the job's stream; one-state potentials have no gap and take FP32)
+static int resolve_auto_precision(zqd_job* J) {
+    if (J->o.precision != ZQD_PRECISION_AUTO) return ZQD_OK;
+    J->o.precision = ZQD_FP32_MIXED;
+    if (J->S == 1) return ZQD_OK;
+    GapArgs a{};
+    a.pot = J->pot.dev;
+    a.d = J->d;
+    a.n = J->n;
+    a.N = J->N;
+    for (int j = 0; j < J->d; ++j) {
+        a.lo[j] = J->o.bounds[2 * j];
+        a.span[j] = J->o.bounds[2 * j + 1] - J->o.bounds[2 * j];
+    }
+    DevBuf out;
+    int rc;
+    if ((rc = out.alloc(sizeof(unsigned long long)))) return rc;
+    a.out = out.as<unsigned long long>();
+    ZQD_CUDA(cudaMemsetAsync(out.p, 0xff, sizeof(unsigned long long), J->stream)); // above every double's bits
+    const unsigned blocks = (unsigned)std::min<size_t>(1024, (J->N + 255) / 256);
+    switch (J->S) {
+    case 2: min_gap_kernel<2><<<blocks, 256, 0, J->stream>>>(a); break;
+    case 3: min_gap_kernel<3><<<blocks, 256, 0, J->stream>>>(a); break;
+    default: min_gap_kernel<4><<<blocks, 256, 0, J->stream>>>(a); break;
+    }
+    ZQD_CUDA(cudaGetLastError());
+    unsigned long long bits = 0;
+    ZQD_CUDA(cudaMemcpyAsync(&bits, out.p, sizeof(bits), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    double gap;
+    std::memcpy(&gap, &bits, sizeof(gap));
+    J->min_gap = gap;
+    if (!(gap >= ZQD_AUTO_GAP_THRESHOLD)) J->o.precision = ZQD_FP64; // NaN (no point evaluated) included
+    return ZQD_OK;
+}
+
 // Hamiltonian.init/update at t = 0 (wavepacket.zig:96-143) and Propagator.init/update
 // (quantum_dynamics.zig:387-468) for every grid point, written in the cluster-permuted layout.
 template <typename T, int S> __global__ void line_tables_kernel(LineTablesArgs<T> a) {
@@ -394,28 +470,27 @@ template <typename T> static int run_line(zqd_job* J) {
 }
 
 // Per-thread pinned staging buffer for result copies (device-to-host copies into pageable
-// memory go through the driver's bounce buffer at a fraction of the bandwidth); null when
-// pinned memory cannot be had, and the caller copies directly.
+// memory go through the driver's bounce buffer at a fraction of the bandwidth).  Fixed size,
+// allocated at a thread's first result and never reallocated: freeing pinned memory
+// synchronises the whole device, which would stall other jobs' kernels.  Null for larger
+// results (and when pinned memory cannot be had): the caller then copies directly.
 static char* pinned_staging(size_t bytes) {
+    constexpr size_t kBytes = (size_t)8 << 20;
     struct Buf {
         char* p = nullptr;
-        size_t n = 0;
+        bool tried = false;
         ~Buf() {
             if (p) cudaFreeHost(p);
         }
     };
     thread_local Buf b;
-    if (b.n < bytes) {
-        if (b.p) cudaFreeHost(b.p);
-        b.p = nullptr;
-        b.n = 0;
-        const size_t want = std::max(bytes, (size_t)1 << 20);
-        if (cudaHostAlloc((void**)&b.p, want, cudaHostAllocDefault) != cudaSuccess) {
+    if (bytes > kBytes) return nullptr;
+    if (!b.tried) {
+        b.tried = true;
+        if (cudaHostAlloc((void**)&b.p, kBytes, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             b.p = nullptr;
-            return nullptr;
         }
-        b.n = want;
     }
     return b.p;
 }
@@ -466,6 +541,7 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     R->grid = J->o.bounds;
     R->grid.push_back((double)J->o.npoint);
     R->device_ms = J->last_ms;
+    R->precision = J->fp32 ? ZQD_FP32_MIXED : ZQD_FP64;
     R->solves.resize(J->nsolve);
     for (int s = 0; s < J->nsolve; ++s) {
         SolveOut& so = R->solves[s];
@@ -560,15 +636,16 @@ int zqd::job_create_opts(Opts&& o, zqd_job** out) {
     J->n = (int)J->o.npoint;
     J->N = 1;
     for (int i = 0; i < J->d; ++i) J->N *= (size_t)J->n;
-    J->fp32 = J->o.precision == ZQD_FP32_MIXED;
     J->nsolve = J->o.imag_nstate ? (int)J->o.imag_nstate : 1;
     J->hc = RowLayout{J->d, J->S}.width();
-    if (J->d == 1 && (rc = choose_line_shape(J.get()))) return rc;
     if (J->d > 1 && J->n < 8) return fail(ZQD_ERR_UNSUPPORTED, "MULTI-DIMENSIONAL GRIDS NEED AT LEAST 8 POINTS PER AXIS");
     ZQD_CUDA(cudaStreamCreateWithFlags(&J->stream, cudaStreamNonBlocking));
     ZQD_CUDA(cudaEventCreate(&J->ev0));
     ZQD_CUDA(cudaEventCreate(&J->ev1));
     if ((rc = build_potential(J->o, J->pot))) return rc;
+    if ((rc = resolve_auto_precision(J.get()))) return rc;
+    J->fp32 = J->o.precision == ZQD_FP32_MIXED;
+    if (J->d == 1 && (rc = choose_line_shape(J.get()))) return rc;
     if (J->d == 1) rc = J->fp32 ? create_line<float>(J.get()) : create_line<double>(J.get());
     else rc = nd_create(J.get());
     if (rc) return rc;

@@ -67,6 +67,7 @@ struct zqd_job {
     zqd::DevBuf psi_init;               // initial wavefunction replacing the Gaussian (1-D: permuted layout)
     zqd::DevBuf wfn_hist;               // write.wavefunction: [solve][step][S][N] (1-D: permuted layout)
     zqd::DevBuf arena;                  // 1-D jobs: one pool block holding the buffers above (views)
+    double min_gap = -1;                // ZQD_PRECISION_AUTO: smallest adiabatic gap on the grid (-1: not computed)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)

@@ -167,7 +167,8 @@ int validate(const Opts& o) {
     if (o.pot_ns > ZQD_MAX_NSTATE) return fail(ZQD_ERR_UNSUPPORTED, "MORE THAN 4 ELECTRONIC STATES ARE NOT SUPPORTED");
     if ((o.npoint & (o.npoint - 1)) != 0 || o.npoint < 4)
         return fail(ZQD_ERR_UNSUPPORTED, "GRID POINT COUNT MUST BE A POWER OF TWO (>= 4)");
-    if (o.precision != ZQD_FP64 && o.precision != ZQD_FP32_MIXED) return bad("UNKNOWN PRECISION");
+    if (o.precision != ZQD_FP64 && o.precision != ZQD_FP32_MIXED && o.precision != ZQD_PRECISION_AUTO)
+        return bad("UNKNOWN PRECISION");
     // custom expressions must compile (Custom.init fails like exprtk_init returning null)
     for (size_t e = 0; e < o.custom.size(); ++e) {
         ExprProgram prog;

@@ -95,6 +95,7 @@ extern "C" int zqd_result_spectrum(const zqd_result* r, uint32_t s, const double
 }
 
 extern "C" double zqd_result_device_ms(const zqd_result* r) { return r ? r->device_ms : 0.0; }
+extern "C" int zqd_result_precision(const zqd_result* r) { return r ? (int)r->precision : -1; }
 
 namespace {
 // writeMatrixLspace (src/read_write.zig:115-136): "rows cols+1", then per row the grid value

@@ -86,21 +86,24 @@ void zqd_server::run(std::vector<std::shared_ptr<Request>>& batch) {
         if (rc[i]) err[i] = zqd::last_error();
         else jobs[i]->nd_use_graph = false;
     }
-    std::vector<zqd_job*> group;
+    // one grouped launch per precision (ZQD_PRECISION_AUTO requests resolve at creation)
+    std::vector<zqd_job*> group[2];
     for (size_t i = 0; i < batch.size(); ++i)
-        if (!rc[i] && batch[i]->group_key) group.push_back(jobs[i]);
-    int grc = ZQD_OK;
-    std::string gerr;
-    if (group.size() > 1) {
-        grc = zqd::run_line_group(group, group[0]->stream, nullptr);
-        if (grc) gerr = zqd::last_error();
-    }
+        if (!rc[i] && batch[i]->group_key) group[jobs[i]->fp32 ? 1 : 0].push_back(jobs[i]);
+    int grc[2] = {ZQD_OK, ZQD_OK};
+    std::string gerr[2];
+    for (int g = 0; g < 2; ++g)
+        if (group[g].size() > 1) {
+            grc[g] = zqd::run_line_group(group[g], group[g][0]->stream, nullptr);
+            if (grc[g]) gerr[g] = zqd::last_error();
+        }
     for (size_t i = 0; i < batch.size(); ++i) {
         if (rc[i]) continue;
-        const bool grouped = group.size() > 1 && batch[i]->group_key;
+        const int g = jobs[i]->fp32 ? 1 : 0;
+        const bool grouped = group[g].size() > 1 && batch[i]->group_key;
         if (grouped) {
-            rc[i] = grc;
-            err[i] = gerr;
+            rc[i] = grc[g];
+            err[i] = gerr[g];
         } else if ((rc[i] = zqd_job_run(jobs[i]))) {
             err[i] = zqd::last_error();
         }
@@ -119,10 +122,11 @@ void zqd_server::run(std::vector<std::shared_ptr<Request>>& batch) {
         ++stats.completed;
         if (rc[i]) ++stats.failed;
     }
-    if (group.size() > 1) {
-        ++stats.grouped_launches;
-        stats.grouped_jobs += group.size();
-    }
+    for (int g = 0; g < 2; ++g)
+        if (group[g].size() > 1) {
+            ++stats.grouped_launches;
+            stats.grouped_jobs += group[g].size();
+        }
     cv_done.notify_all();
     cv_work.notify_all();
 }

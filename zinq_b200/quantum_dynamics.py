@@ -47,9 +47,19 @@ class Observables:
 
 @dataclass
 class Result:
-    """Result(T) (quantum_dynamics.zig:70-83) plus the device time of the propagation."""
+    """Result(T) (quantum_dynamics.zig:70-83) plus the device time of the propagation and the
+    precision the job ran in ("fp64" or "fp32"; a job submitted as "auto" reports its choice)."""
     observables: list
     device_ms: float = 0.0
+    precision: str = ""
+
+
+_PRECISION_NAME = {0: "fp64", 1: "fp32"}
+
+
+def _result(L, res, obs) -> "Result":
+    return Result(observables=obs, device_ms=L.zqd_result_device_ms(res),
+                  precision=_PRECISION_NAME.get(L.zqd_result_precision(res), ""))
 
 
 def read_matrix(path):
@@ -256,7 +266,7 @@ def run(opt: dict, precision: str = "fp64", log: bool = False, want_wavefunction
         if want_wavefunction and obs:
             S = len(obs[0].pop)
             _attach_wavefunctions(res, obs, _shape(opt), S)
-        return Result(observables=obs, device_ms=L.zqd_result_device_ms(res))
+        return _result(L, res, obs)
     finally:
         L.zqd_result_destroy(res)
 
@@ -274,7 +284,7 @@ def run_batch(opts: list, precision: str = "fp64", want_wavefunction: bool = Fal
             obs = _collect(r)
             if want_wavefunction and obs:
                 _attach_wavefunctions(r, obs, _shape(opts[i]), len(obs[0].pop))
-            out.append(Result(observables=obs, device_ms=L.zqd_result_device_ms(r)))
+            out.append(_result(L, r, obs))
     finally:
         for r in res:
             if r:
@@ -310,7 +320,7 @@ class Job:
             obs = _collect(res)
             if want_wavefunction and obs:
                 _attach_wavefunctions(res, obs, _shape(self.opt), len(obs[0].pop))
-            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res))
+            return _result(self._L, res, obs)
         finally:
             self._L.zqd_result_destroy(res)
 
@@ -353,7 +363,7 @@ class Batch:
             obs = _collect(res)
             if want_wavefunction and obs:
                 _attach_wavefunctions(res, obs, _shape(self.opts[i]), len(obs[0].pop))
-            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res))
+            return _result(self._L, res, obs)
         finally:
             self._L.zqd_result_destroy(res)
 
@@ -390,7 +400,7 @@ def run_batch_e2e(opts: list, precision: str = "fp64"):
             h, d = transfer_bytes(r)
             h2d += h
             d2h += d
-            out.append(Result(observables=_collect(r), device_ms=L.zqd_result_device_ms(r)))
+            out.append(_result(L, r, _collect(r)))
     finally:
         for r in res:
             if r:
@@ -440,7 +450,7 @@ class Server:
             obs = _collect(res)
             if want_wavefunction and obs:
                 _attach_wavefunctions(res, obs, npt, len(obs[0].pop))
-            return Result(observables=obs, device_ms=self._L.zqd_result_device_ms(res)), lat.value
+            return _result(self._L, res, obs), lat.value
         finally:
             self._L.zqd_result_destroy(res)
 
