@@ -167,6 +167,13 @@ __device__ __forceinline__ void fft_local(cx<T>* buf, int ldp, int logm, int nli
     }
 }
 
+// Cluster barrier without memory ordering (a relaxed arrive carries no release fence): for
+// write-after-read protection only, where every remote read before it has been consumed.
+__device__ __forceinline__ void cluster_barrier_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+}
+
 // ------------------------------------------------------------ reductions
 struct RedSmem {
     double warp[32][NRED][2];

@@ -466,8 +466,10 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
                 else pass<2, SIGN, KL>(in, out, p, logp, xbuf);
             }
             // the inverse's first pass read other CTAs' exchange buffers: none may be
-            // overwritten before every CTA of the cluster has finished that gather
-            if (C > 1 && SIGN > 0 && first) cg::this_cluster().sync();
+            // overwritten before every CTA of the cluster has finished that gather.  The
+            // gathered values were consumed (butterflies, stored locally) before the arrive,
+            // so the barrier publishes nothing and its arrive can be relaxed (no fence)
+            if (C > 1 && SIGN > 0 && first) cluster_barrier_relaxed();
             cx<T>* t = in;
             in = out;
             out = t;
