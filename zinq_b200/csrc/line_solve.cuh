@@ -157,6 +157,17 @@ __device__ __forceinline__ void observe_k(Acc* acc, const cx<T>* z, int kidx, in
     if (f.ekin) acc[A_EKIN].add(w * (0.5 * kv * kv / mass));
 }
 
+// observe_k for the wavenumber slot of one state: the state's share of the k-space sums
+template <typename T>
+__device__ __forceinline__ void observe_k1(Acc* acc, const cx<T>& z, int kidx, int n, double dkunit, double mass,
+                                           const ObsFlags& f) {
+    const double w = (double)z.x * (double)z.x + (double)z.y * (double)z.y;
+    const double nn = (double)kidx;
+    const double kv = __dmul_rn(kidx < n / 2 ? nn : __dsub_rn(nn, (double)n), dkunit); // wavepacket.zig:68-70
+    if (f.mom) acc[A_MOM].add(w * kv);
+    if (f.ekin) acc[A_EKIN].add(w * (0.5 * kv * kv / mass));
+}
+
 // ------------------------------------------------------------ rare phases
 // (initial state, imaginary time, time-dependent updates): out of line
 template <typename T> struct LineCtx {
@@ -490,35 +501,21 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             cx<T>* xb = other(res);
             cg::cluster_group cl = cg::this_cluster();
             cl.sync();
-            for (int u = threadIdx.x; u < q; u += blockDim.x) {
-                cx<T> w[S][C];
+            // one (column u, state s) pair per thread: S times the threads of one column each
+            for (int t = threadIdx.x; t < S * q; t += blockDim.x) {
+                const int s = t / q, u = t - s * q;
+                cx<T> w[C];
 #pragma unroll
-                for (int cc = 0; cc < C; ++cc) {
-                    const cx<T>* src = remote<T>(res, cc);
-#pragma unroll
-                    for (int s = 0; s < S; ++s) w[s][cc] = src[s * ldp + padx<T>(cta * q + u)];
-                }
-#pragma unroll
-                for (int s = 0; s < S; ++s) dft<C, -1, T>(w[s]);
+                for (int cc = 0; cc < C; ++cc) w[cc] = remote<T>(res, cc)[s * ldp + padx<T>(cta * q + u)];
+                dft<C, -1, T>(w);
 #pragma unroll
                 for (int k2 = 0; k2 < C; ++k2) {
-                    if (prop) {
-                        const Tab<T> ph = eks[k2 * q + u];
-#pragma unroll
-                        for (int s = 0; s < S; ++s) w[s][k2] = tmul<-1>(w[s][k2], ph);
-                    } else {
-                        cx<T> z[S];
-#pragma unroll
-                        for (int s = 0; s < S; ++s) z[s] = w[s][k2];
-                        observe_k<T, S>(acc, z, cta * q + u + m * k2, n, dkunit, mass, f);
-                    }
+                    if (prop) w[k2] = tmul<-1>(w[k2], eks[k2 * q + u]);
+                    else observe_k1<T>(acc, w[k2], cta * q + u + m * k2, n, dkunit, mass, f);
                 }
+                dft<C, 1, T>(w);
 #pragma unroll
-                for (int s = 0; s < S; ++s) dft<C, 1, T>(w[s]);
-#pragma unroll
-                for (int cc = 0; cc < C; ++cc)
-#pragma unroll
-                    for (int s = 0; s < S; ++s) xb[s * ldp + padx<T>(cc * q + u)] = w[s][cc];
+                for (int cc = 0; cc < C; ++cc) xb[s * ldp + padx<T>(cc * q + u)] = w[cc];
             }
             cl.sync();
             return xb;
