@@ -215,9 +215,10 @@ namespace zqd {
 
 template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
 
-// Cluster shape of a 1-D job: C CTAs of m = n/C points each, m/4 threads per CTA (one
-// radix-4 butterfly of every state per thread; radix 8 and m/8 threads where m/4 threads
-// exceed the kernel's limit).  The default is the smallest C whose CTA fits in shared memory
+// Cluster shape of a 1-D job: C CTAs of m = n/C points each, radix-4 local passes (radix 8
+// where m/4 threads exceed the kernel's limit) and S m/4 threads per CTA, capped at the
+// limit: a pass whose hooks mix the states runs one butterfly of every state per thread on
+// the first m/4 threads, the other passes one (butterfly, state) pair per thread.  The default is the smallest C whose CTA fits in shared memory
 // and holds at most `target` points (256; measured per step: 8192 points on 16 CTAs 18 %
 // faster than on 8, 1024 points on 4 CTAs 15 % faster than on 2); ZQD_LINE_CLUSTER forces C
 // (tuning sweeps).  Radix-8 kernels exist for 16-CTA clusters only (lines above 16384 points in
@@ -244,8 +245,10 @@ static int choose_line_shape(zqd_job* J) {
             const int tmax = J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value;
             if (((m >> 2) + 31) / 32 * 32 > tmax) lrmax = 3;
             if (lrmax == 3 && C != 16) continue; // radix 8 is built for 16-CTA clusters only
-            const int threads = std::max(32, ((m >> lrmax) + 31) / 32 * 32);
-            if (threads > tmax) continue;
+            if (std::max(32, ((m >> lrmax) + 31) / 32 * 32) > tmax) continue;
+            // one thread per butterfly of every state (passes without state-mixing hooks split
+            // the states over the threads), within the kernel's thread limit
+            const int threads = std::min(tmax, std::max(32, ((m >> lrmax) * J->S + 31) / 32 * 32));
             if (pass == 0 && !forced && m > target) continue;
             J->C = C;
             J->m = m;

@@ -415,6 +415,51 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
         constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
         const int logmr = logm - LR, mr = 1 << logmr, nt = blockDim.x;
         const int tshift = logm - logp - LR;
+        // passes whose hooks do not mix states take one (butterfly, state) pair per thread;
+        // the forward first pass (R) and the inverse last pass (R, observables) take all
+        // states of a butterfly in one thread
+        constexpr bool SPLIT = S > 1 && !(KIND & FWD_FIRST) && !(KIND & INV_LAST);
+        if constexpr (SPLIT) {
+            for (int t = threadIdx.x; t < (S << logmr); t += nt) {
+                const int s = t >> logmr, i = t & (mr - 1);
+                cx<T> v[R];
+                if constexpr ((KIND & INV_FIRST) && C > 1) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) { // inv_first for one state
+                        const int k1 = i + r * mr, owner = k1 / q, u = k1 - owner * q;
+                        v[r] = remote<T>(xbuf, owner)[s * ldp + padx<T>(cta * q + u)];
+                        if (cta > 0) v[r] = tmul<1>(v[r], twc[k1]);
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[r] = in[s * ldp + padx<T>(i + r * mr)];
+                }
+                const int kk = i & (p - 1);
+                if (p > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) v[r] = tmul<SIGN>(v[r], twm[(r * kk) << tshift]);
+                }
+                dft<R, SIGN, T>(v);
+                const int o0 = ((i - kk) << LR) + kk;
+                if constexpr (KIND & FWD_LAST) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) { // fwd_last for one state
+                        const int k = o0 + r * p;
+                        if constexpr (C > 1) {
+                            if (cta > 0) v[r] = tmul<-1>(v[r], twc[k]);
+                        } else if (prop) {
+                            v[r] = tmul<-1>(v[r], eks[k]);
+                        } else {
+                            observe_k1<T>(acc, v[r], k, n, dkunit, mass, f);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) out[s * ldp + padx<T>(o0 + r * p)] = v[r];
+            }
+            __syncthreads();
+            return;
+        }
         for (int i = threadIdx.x; i < mr; i += nt) {
             cx<T> v[S][R];
             if constexpr ((KIND & INV_FIRST) && C > 1) {
