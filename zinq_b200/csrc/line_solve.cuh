@@ -315,7 +315,8 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     cx<T>* bufA;
     cx<T>* bufB;
     cx<T>* cur; // holds psi between steps
-    const Tab<T>* twm;
+    const Tab<T>* twm; // local-pass twiddles, pass by pass (see the staging in the kernel)
+    const Tab<T>* twp; // the current pass's table: W at [(r - 1) p + kk]
     const Tab<T>* twc;
     const Tab<T>* Rs;
     int rstride; // component stride of Rs: m when staged in shared memory, n when read from global
@@ -414,7 +415,6 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
                                          const cx<T>* xbuf) {
         constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
         const int logmr = logm - LR, mr = 1 << logmr, nt = blockDim.x;
-        const int tshift = logm - logp - LR;
         // passes whose hooks do not mix states take one (butterfly, state) pair per thread;
         // the forward first pass (R) and the inverse last pass (R, observables) take all
         // states of a butterfly in one thread
@@ -437,7 +437,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
                 const int kk = i & (p - 1);
                 if (p > 1) {
 #pragma unroll
-                    for (int r = 1; r < R; ++r) v[r] = tmul<SIGN>(v[r], twm[(r * kk) << tshift]);
+                    for (int r = 1; r < R; ++r) v[r] = tmul<SIGN>(v[r], twp[(r - 1) * p + kk]);
                 }
                 dft<R, SIGN, T>(v);
                 const int o0 = ((i - kk) << LR) + kk;
@@ -475,7 +475,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             if (p > 1) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    const Tab<T> w = twm[(r * kk) << tshift];
+                    const Tab<T> w = twp[(r - 1) * p + kk];
 #pragma unroll
                     for (int s = 0; s < S; ++s) v[s][r] = tmul<SIGN>(v[s][r], w);
                 }
@@ -496,7 +496,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     // local m-point transform ping-ponging between a (input) and b; returns the result buffer
     template <int SIGN> __device__ __forceinline__ cx<T>* local_fft(cx<T>* a, cx<T>* b, const cx<T>* xbuf) {
         constexpr int KF = SIGN < 0 ? FWD_FIRST : INV_FIRST, KL = SIGN < 0 ? FWD_LAST : INV_LAST;
-        int p = 1, logp = 0, rem = logm;
+        int p = 1, logp = 0, rem = logm, tbase = 0;
         bool first = true;
         cx<T>* in = a;
         cx<T>* out = b;
@@ -505,6 +505,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             // which keeps the kernel's instruction footprint small), smaller at the end
             const int LR = rem >= LRM ? LRM : rem;
             const bool last = rem == LR;
+            twp = twm + tbase;
             if (LRM == 3 && LR == 3) {
                 if constexpr (LRM == 3) {
                     if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
@@ -529,6 +530,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             cx<T>* t = in;
             in = out;
             out = t;
+            tbase += ((1 << LR) - 1) * p;
             p <<= LR;
             logp += LR;
             rem -= LR;
@@ -687,9 +689,27 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
     // stage the time-independent tables
     const int m = X.m, n = X.n;
     for (int t = threadIdx.x; t < m; t += blockDim.x) {
-        twm[t] = J.tw[t * C]; // exp(-2 pi i t/m)
         if (C > 1) twc[t] = J.tw[cta * t];
         eks[t] = J.expk[X.base + t];
+    }
+    // Twiddles of the local passes in pass order (the radix schedule of local_fft): the pass
+    // of span p and radix R holds W_m^(r kk m/(p R)) = exp(-2 pi i r kk / (p R)) at
+    // [(r - 1) p + kk], r = 1..R-1, kk < p.  A warp's twiddle reads are then contiguous
+    // (reading W_m^t at stride m/(p R) put up to 16 of them in the same banks); the tables
+    // take sum (R - 1) p = m - 1 entries.
+    {
+        int p = 1, logp = 0, rem = X.logm, tbase = 0;
+        while (rem > 0) {
+            const int LR = rem >= LRM ? LRM : rem, R = 1 << LR, tshift = X.logm - logp - LR;
+            for (int e = threadIdx.x; e < (R - 1) * p; e += blockDim.x) {
+                const int r = e / p + 1, kk = e - (r - 1) * p;
+                twm[tbase + e] = J.tw[((r * kk) << tshift) * C];
+            }
+            tbase += (R - 1) * p;
+            p <<= LR;
+            logp += LR;
+            rem -= LR;
+        }
     }
     if (!J.r_global)
         for (int e = threadIdx.x; e < NSYM * m; e += blockDim.x) {
