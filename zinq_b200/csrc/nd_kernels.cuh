@@ -94,8 +94,14 @@ template <typename T> __host__ __device__ inline int tile_ldp(int n) { return pa
 template <typename T> __host__ __device__ inline size_t nd_tw_offset(int nbuf, int lines, int n) {
     return ((size_t)nbuf * lines * tile_ldp<T>(n) * sizeof(cx<T>) + 15) & ~(size_t)15;
 }
+// entries of one direction's middle-pass twiddle tables: the middle passes take the span p
+// from 8 (after the first radix-8 pass) to n/8 (before a last radix-8 pass, n >= 64) or n
+// (n = 16, 32), and a pass of span p and radix R holds (R - 1) p entries: p_end - 8 in all
+__host__ __device__ inline int nd_mid_tw(int n) { return n < 16 ? 0 : (n >= 64 ? n / 8 : n) - 8; }
+// after the buffers: W_n^t (t < n) for the register-resident last pass, then the forward
+// and the inverse middle-pass tables
 template <typename T> __host__ __device__ inline size_t nd_smem_bytes(int nbuf, int lines, int n) {
-    return nd_tw_offset<T>(nbuf, lines, n) + (size_t)n * sizeof(Tab<T>);
+    return nd_tw_offset<T>(nbuf, lines, n) + (size_t)(n + 2 * nd_mid_tw(n)) * sizeof(Tab<T>);
 }
 
 template <typename T> __device__ __forceinline__ void grid_coords(const NdJob<T>& J, size_t gidx, double* r) {
@@ -120,12 +126,12 @@ template <typename T> __device__ __forceinline__ void grid_wavenumbers(const NdJ
 // Radix-R Stockham pass over `ngroups` groups of G lines of n = 2^logn points
 // (line (g, s) at index s * ngroups + g, stride ldp).  A thread handles butterfly
 // i of all G lines of a group, so the G states of a grid point meet in one thread.
+// twp: this pass's twiddles W_n^(r kk n/(p R)) at [(r - 1) p + kk] (contiguous for a warp).
 template <typename T, int G, int R, int SIGN, bool FIRST, bool LAST, typename H>
 __device__ __forceinline__ void tpass(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int ldp, int logn, int p,
-                                      int logp, const Tab<T>* __restrict__ twm, int ngroups, H& h) {
+                                      const Tab<T>* __restrict__ twp, int ngroups, H& h) {
     constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
     const int logmr = logn - LR, mr = 1 << logmr;
-    const int tshift = logn - logp - LR;
     const int items = ngroups << logmr;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int g = it >> logmr, i = it & (mr - 1);
@@ -139,7 +145,7 @@ __device__ __forceinline__ void tpass(const cx<T>* __restrict__ in, cx<T>* __res
         if (p > 1) {
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                const Tab<T> w = twm[(r * kk) << tshift];
+                const Tab<T> w = twp[(r - 1) * p + kk];
 #pragma unroll
                 for (int s = 0; s < G; ++s) v[s][r] = tmul<SIGN>(v[s][r], w);
             }
@@ -154,40 +160,6 @@ __device__ __forceinline__ void tpass(const cx<T>* __restrict__ in, cx<T>* __res
             for (int r = 0; r < R; ++r) out[(s * ngroups + g) * ldp + padx<T>(o0 + r * p)] = v[s][r];
     }
     __syncthreads();
-}
-
-// Full n-point transform of the staged lines, ping-ponging a -> b -> ...; the
-// hooks run in the first / last pass.  Returns the buffer holding the result.
-template <typename T, int G, int SIGN, bool HF, bool HL, typename H>
-__device__ __forceinline__ cx<T>* tfft(cx<T>* a, cx<T>* b, int ldp, int logn, const Tab<T>* twm, int ngroups, H& h) {
-    int p = 1, logp = 0, rem = logn;
-    bool first = true;
-    cx<T>* in = a;
-    cx<T>* out = b;
-    while (rem > 0) {
-        const int LR = rem >= 3 ? 3 : rem;
-        const bool last = rem == LR;
-        if (LR == 3) {
-            if (first && last) tpass<T, G, 8, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-            else if (first) tpass<T, G, 8, SIGN, HF, false>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-            else if (last) tpass<T, G, 8, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-            else tpass<T, G, 8, SIGN, false, false>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-        } else if (LR == 2) {
-            if (first) tpass<T, G, 4, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-            else tpass<T, G, 4, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-        } else {
-            if (first) tpass<T, G, 2, SIGN, HF, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-            else tpass<T, G, 2, SIGN, false, HL>(in, out, ldp, logn, p, logp, twm, ngroups, h);
-        }
-        cx<T>* t = in;
-        in = out;
-        out = t;
-        p <<= LR;
-        logp += LR;
-        rem -= LR;
-        first = false;
-    }
-    return in;
 }
 
 struct NdNoHook {
@@ -423,6 +395,29 @@ __device__ __forceinline__ NdSched nd_sched(int logn) {
     return s;
 }
 
+// Stages the middle-pass twiddles of both directions at dst (after W_n, t < n): the pass of
+// span p and radix R in that direction's order holds W_n^(r kk n/(p R)) at [(r - 1) p + kk],
+// r = 1..R-1, kk < p, so the pass reads them contiguously (reading W_n at stride n/(p R)
+// put up to 8 of a warp's twiddles in the same banks).
+template <typename T>
+__device__ __forceinline__ void nd_stage_mid_tw(const Tab<T>* __restrict__ tw, Tab<T>* dst, int logn) {
+    const NdSched sc = nd_sched(logn);
+    const int n = 1 << logn;
+    for (int dir = 0; dir < 2; ++dir) {
+        Tab<T>* d = dst + dir * nd_mid_tw(n);
+        int logp = 3, base = 0;
+        for (int j = 0; j < sc.nmid; ++j) {
+            const int lr = sc.lr(j, dir == 1 && sc.last8), R = 1 << lr, p = 1 << logp, tshift = logn - logp - lr;
+            for (int e = threadIdx.x; e < (R - 1) * p; e += blockDim.x) {
+                const int r = e / p + 1, kk = e - (r - 1) * p;
+                d[base + e] = tw[(r * kk) << tshift];
+            }
+            base += (R - 1) * p;
+            logp += lr;
+        }
+    }
+}
+
 // item it of the CTA -> (line g, 8-point group i); GFAST: consecutive items walk the lines
 template <bool GFAST> __device__ __forceinline__ void nd_item(int it, int logl, int logm, int& g, int& i) {
     if (GFAST) {
@@ -462,16 +457,19 @@ __device__ __forceinline__ void nd_fft_regs(cx<T> (&v)[ND_IPT][8], cx<T>* a, cx<
     __syncthreads();
     cx<T>* in = a;
     cx<T>* out = b;
-    int logp = 3;
+    int logp = 3, tbase = 0;
     NdNoHook none;
+    // this direction's dense middle-pass tables (staged by nd_stage_mid_tw after W_n)
+    const Tab<T>* twd = twm + (1 << logn) + (SIGN > 0 ? nd_mid_tw(1 << logn) : 0);
     for (int j = 0; j < sc.nmid; ++j) {
-        const int lr = sc.lr(j, SIGN > 0 && sc.last8);
-        if (lr == 3) tpass<T, 1, 8, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
-        else if (lr == 2) tpass<T, 1, 4, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
-        else tpass<T, 1, 2, SIGN, false, false>(in, out, ldp, logn, 1 << logp, logp, twm, lines, none);
+        const int lr = sc.lr(j, SIGN > 0 && sc.last8), p = 1 << logp;
+        if (lr == 3) tpass<T, 1, 8, SIGN, false, false>(in, out, ldp, logn, p, twd + tbase, lines, none);
+        else if (lr == 2) tpass<T, 1, 4, SIGN, false, false>(in, out, ldp, logn, p, twd + tbase, lines, none);
+        else tpass<T, 1, 2, SIGN, false, false>(in, out, ldp, logn, p, twd + tbase, lines, none);
         cx<T>* t = in;
         in = out;
         out = t;
+        tbase += ((1 << lr) - 1) * p;
         logp += lr;
     }
 #pragma unroll
@@ -748,6 +746,7 @@ __global__ void __launch_bounds__(MAXT)
     cx<T>* buf1 = buf0 + lines * ldp;
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>(2, lines, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    nd_stage_mid_tw<T>(J.tw, twm + n, logn);
     const size_t row0 = (size_t)blockIdx.x * pts;
     // line g = s * L + l starts at psi[s * N + row0 + l * n]
     auto gaddr = [&](int g) -> size_t { const int s = g / L; return (size_t)s * J.N + row0 + ((size_t)(g - s * L) << logn); };
@@ -867,6 +866,7 @@ __global__ void __launch_bounds__(512)
     cx<T>* buf1 = buf0 + Tn * ldp;
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(smem_raw + nd_tw_offset<T>(2, Tn, n));
     for (int t = threadIdx.x; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    nd_stage_mid_tw<T>(J.tw, twm + n, logn);
     const int lstride = logn * (D - 1 - axis);
     const int ltpo = lstride - logt; // log2 of the tiles per outer index
     const size_t outer = (size_t)blockIdx.x >> ltpo, inner0 = ((size_t)blockIdx.x & ((1u << ltpo) - 1)) << logt;
