@@ -411,7 +411,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     // handles the butterflies i = t, t + nt, ... of every state, so all S states of
     // a grid point meet in one thread.  KIND selects the hooks of first/last passes.
     template <int R, int SIGN, int KIND>
-    __device__ __forceinline__ void pass(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int p, int logp,
+    __device__ __forceinline__ void pass(const cx<T>* __restrict__ in, cx<T>* __restrict__ out, int p,
                                          const cx<T>* xbuf) {
         constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
         const int logmr = logm - LR, mr = 1 << logmr, nt = blockDim.x;
@@ -496,7 +496,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     // local m-point transform ping-ponging between a (input) and b; returns the result buffer
     template <int SIGN> __device__ __forceinline__ cx<T>* local_fft(cx<T>* a, cx<T>* b, const cx<T>* xbuf) {
         constexpr int KF = SIGN < 0 ? FWD_FIRST : INV_FIRST, KL = SIGN < 0 ? FWD_LAST : INV_LAST;
-        int p = 1, logp = 0, rem = logm, tbase = 0;
+        int p = 1, rem = logm, tbase = 0;
         bool first = true;
         cx<T>* in = a;
         cx<T>* out = b;
@@ -508,19 +508,19 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             twp = twm + tbase;
             if (LRM == 3 && LR == 3) {
                 if constexpr (LRM == 3) {
-                    if (first && last) pass<8, SIGN, KF | KL>(in, out, p, logp, xbuf);
-                    else if (first) pass<8, SIGN, KF>(in, out, p, logp, xbuf);
-                    else if (last) pass<8, SIGN, KL>(in, out, p, logp, xbuf);
-                    else pass<8, SIGN, 0>(in, out, p, logp, xbuf);
+                    if (first && last) pass<8, SIGN, KF | KL>(in, out, p, xbuf);
+                    else if (first) pass<8, SIGN, KF>(in, out, p, xbuf);
+                    else if (last) pass<8, SIGN, KL>(in, out, p, xbuf);
+                    else pass<8, SIGN, 0>(in, out, p, xbuf);
                 }
             } else if (LR == 2) {
-                if (first && last) pass<4, SIGN, KF | KL>(in, out, p, logp, xbuf);
-                else if (first) pass<4, SIGN, KF>(in, out, p, logp, xbuf);
-                else if (last) pass<4, SIGN, KL>(in, out, p, logp, xbuf);
-                else pass<4, SIGN, 0>(in, out, p, logp, xbuf);
+                if (first && last) pass<4, SIGN, KF | KL>(in, out, p, xbuf);
+                else if (first) pass<4, SIGN, KF>(in, out, p, xbuf);
+                else if (last) pass<4, SIGN, KL>(in, out, p, xbuf);
+                else pass<4, SIGN, 0>(in, out, p, xbuf);
             } else {
-                if (first) pass<2, SIGN, KF | KL>(in, out, p, logp, xbuf);
-                else pass<2, SIGN, KL>(in, out, p, logp, xbuf);
+                if (first) pass<2, SIGN, KF | KL>(in, out, p, xbuf);
+                else pass<2, SIGN, KL>(in, out, p, xbuf);
             }
             // the inverse's first pass read other CTAs' exchange buffers: none may be
             // overwritten before every CTA of the cluster has finished that gather.  The
@@ -532,7 +532,6 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             out = t;
             tbase += ((1 << LR) - 1) * p;
             p <<= LR;
-            logp += LR;
             rem -= LR;
             first = false;
         }
