@@ -1,16 +1,19 @@
 // line_solve.cuh -- the fused resident 1-D solve (src/quantum_dynamics.zig:860-950).
 //
 // Shared memory of a CTA holds two wavefunction buffers (the Stockham passes
-// ping-pong between them, one barrier per pass), the twiddles exp(-2 pi i t/m),
-// the cluster twiddles exp(-2 pi i c k1/n), the potential propagator R at the
-// CTA's grid points and the kinetic phase at its wavenumbers.  One time step
-// (Propagator.step, :417-427) is
+// ping-pong between them, one barrier per pass), the local passes' twiddles
+// (pass by pass, so that a warp reads them contiguously), the cluster twiddles
+// exp(-2 pi i c k1/n), the potential propagator R at the CTA's grid points and
+// the kinetic phase at its wavenumbers.  One time step (Propagator.step,
+// :417-427) is
 //   forward FFT   first pass: [accumAbsorbed], psi <- R psi, butterflies
 //                 last pass : butterflies, cluster twiddle (C > 1) or kinetic phase (C = 1)
 //   exchange      C-point DFTs across the cluster with the kinetic phase between them (C > 1)
 //   inverse FFT   first pass: remote gather of the exchanged values (C > 1), butterflies
 //                 last pass : butterflies, 1/N, [accumAbsorbed], psi <- R psi, observables
-// followed by one cluster reduction of every observable of the step.
+// followed by one cluster reduction of the observables the step records.  The two
+// passes that apply R take all states of a butterfly in one thread; the other passes
+// and the exchange take one (butterfly or column, state) pair per thread.
 #pragma once
 
 #include "line_kernel.cuh"
