@@ -52,6 +52,14 @@ def test_2d_three_state_coupled_harmonic_fp64():
     compare(coupled_harmonic_2d(npoint=128, iters=300))
 
 
+@pytest.mark.parametrize("npoint", [256, 512])
+def test_2d_single_radix4_and_radix8_middle_pass(npoint):
+    # 256 and 512 points per axis: one radix-4 / radix-8 Stockham pass between the
+    # register-resident first and last passes (its twiddles from the staged per-pass table);
+    # 512^2 x 3 states is the benchmark's 2-D grid
+    compare(coupled_harmonic_2d(npoint=npoint, iters=12))
+
+
 def test_2d_three_state_coupled_harmonic_fp32_populations():
     compare(coupled_harmonic_2d(iters=400), precision="fp32", pop_tol=FP32_POP_TOL, obs_tol=1e-4)
 
