@@ -149,7 +149,7 @@ def oracle_sample(opts, threads):
 def reference_arm(args, rank):
     if rank != 0:
         return
-    sample_iters = 1000  # bounded sample per step: 5 jobs x 1000 steps, all jobs in parallel threads
+    sample_iters = ITERS  # the whole workload per step: 5 jobs x 4000 steps, all jobs in parallel threads
     opts = workload(sample_iters)
     threads = min(len(opts), os.cpu_count() or 1)
     for _ in range(args.warmup):
@@ -162,7 +162,7 @@ def reference_arm(args, rank):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": config({"sample": f"{len(opts)} jobs x {sample_iters} steps per bench step"}),
+            "config": config({"sample": f"{len(opts)} jobs x {sample_iters} steps per bench step (the whole workload)"}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{len(opts)} jobs x {sample_iters} steps, one thread per job"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -212,15 +212,43 @@ class Clocks:
                 "samples": len(sm)}
 
 
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.txt")
+
+
 def read_traffic(kernel, precision):
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
-    if not os.path.exists(path):
+    """DRAM bytes per launch from profiles/traffic.txt: an ncu capture of the same kernel on the same
+    workload, tabulated by `python bench.py --traffic-table <ncu csv>` (not measured by this run)."""
+    if not os.path.exists(TRAFFIC_FILE):
         return None
-    for line in open(path):
+    for line in open(TRAFFIC_FILE):
         p = line.split()
         if len(p) >= 3 and p[0] == kernel and p[1] == precision:
             return float(p[2])
     return None
+
+
+def traffic_table(csv_path, label):
+    """Rows "kernel label bytes_per_launch" from an ncu --csv log with dram__bytes_read.sum and
+    dram__bytes_write.sum: per kernel the mean over its captured launches of read + write bytes."""
+    import csv
+
+    per = {}
+    with open(csv_path) as f:
+        lines = [ln for ln in f if ln.startswith('"')]
+    for row in csv.DictReader(lines):
+        metric = row.get("Metric Name", "")
+        if metric not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        name = row["Kernel Name"].split("<")[0].split("(")[0].replace("void ", "").replace("zqd::", "").strip()
+        unit = row.get("Metric Unit", "byte").lower()
+        scale = {"byte": 1, "kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9}.get(unit, 1)
+        v = float(row["Metric Value"].replace(",", "")) * scale
+        key = (name, row["ID"])
+        per[key] = per.get(key, 0.0) + v
+    by_kernel = {}
+    for (name, _), v in per.items():
+        by_kernel.setdefault(name, []).append(v)
+    return [f"{k} {label} {statistics.mean(v):.4g}" for k, v in sorted(by_kernel.items())]
 
 
 def measured_peak():
@@ -367,6 +395,105 @@ def serving_leg(qd):
     return out
 
 
+def fp32_error_table(qd):
+    """north_star (3): per configuration, the FP32 form's error against the FP64 form (which the tests
+    hold to the oracle at 1e-10 / 1e-12): relative L2 of the final wavefunction, the largest population
+    error over the run, the largest total-energy difference over the run and the energy drift
+    |E(T) - E(0)| of each form."""
+    import numpy as np
+
+    def with_energy(opt):
+        o = dict(opt)
+        o["write"] = dict(opt.get("write") or {}, total_energy="E", population="P")
+        return o
+
+    cases = [("1_harmonic_1d", with_energy(harmonic_1d()))]
+    cases += [(f"2_tanh_crossing_p{int(o['initial_conditions']['momentum'][0])}", with_energy(o)) for o in workload()]
+    cases += [("3_coupled_2d_512sq", with_energy(coupled_harmonic_2d())),
+              ("4_anharmonic_3d_itp", with_energy(anharmonic_3d(500, True))),
+              ("4_anharmonic_3d_realtime", with_energy(anharmonic_3d(2000, False)))]
+    out = {}
+    for name, opt in cases:
+        r = {p: qd.run(opt, precision=p).observables[0] for p in ("fp64", "fp32")}
+        a, b = r["fp32"], r["fp64"]
+        ea, eb = a.history["total_energy"].ravel(), b.history["total_energy"].ravel()
+        out[name] = {
+            "psi_rel_l2": float(np.linalg.norm(a.wavefunction - b.wavefunction) / np.linalg.norm(b.wavefunction)),
+            "pop_max_err": float(np.max(np.abs(a.history["population"] - b.history["population"]))),
+            "energy_max_diff": float(np.max(np.abs(ea - eb))),
+            "energy_drift_fp32": float(abs(ea[-1] - ea[0])), "energy_drift_fp64": float(abs(eb[-1] - eb[0])),
+        }
+    return out
+
+
+def fft_brackets(qd, torch, reps=20):
+    """Transform-only timings at the workloads' sizes (FP64 complex, forward + inverse):
+    cuFFT (torch.fft) against the library's FFT seam (zqd_fft_execute) on the same device buffer,
+    and on the host pocketfft (scipy.fft, every host thread) against the oracle's own FFT, which
+    brackets how far the CPU port's radix-2/4 FFT is from an FFTW-class FFT."""
+    import ctypes as C
+
+    import numpy as np
+    import scipy.fft
+
+    from oracle import qd_ref
+    from zinq_b200 import _abi
+
+    L = _abi.load()
+    nproc = os.cpu_count() or 1
+    out = {"host_threads": nproc}
+    for name, shape in (("1d_8192", (8192,)), ("2d_512sq", (512, 512)), ("3d_128cube", (128, 128, 128)),
+                        ("2d_2048sq", (2048, 2048))):
+        x = torch.randn(*shape, dtype=torch.complex128, device="cuda")
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dims = tuple(range(len(shape)))
+        for _ in range(3):
+            torch.fft.ifftn(torch.fft.fftn(x, dim=dims), dim=dims)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(reps):
+            y = torch.fft.ifftn(torch.fft.fftn(x, dim=dims), dim=dims)
+        ev1.record()
+        torch.cuda.synchronize()
+        cufft_ms = ev0.elapsed_time(ev1) / reps
+        plans = []
+        for sign in (-1, 1):
+            h = C.c_void_p()
+            arr = (C.c_int * len(shape))(*shape)
+            _abi.check(L.zqd_fft_plan_create(len(shape), arr, sign, 0, C.byref(h)))
+            plans.append(h)
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        buf = C.c_void_p(x.data_ptr())
+        for _ in range(3):
+            for h in plans:
+                _abi.check(L.zqd_fft_execute(h, buf, stream))
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(reps):
+            for h in plans:
+                _abi.check(L.zqd_fft_execute(h, buf, stream))
+        ev1.record()
+        torch.cuda.synchronize()
+        own_ms = ev0.elapsed_time(ev1) / reps
+        for h in plans:
+            L.zqd_fft_destroy(h)
+        del x, y
+        hx = np.random.default_rng(1).standard_normal(shape) + 1j * np.random.default_rng(2).standard_normal(shape)
+        nrep = max(1, int(2e7 // hx.size))
+        t0 = time.perf_counter()
+        for _ in range(nrep):
+            scipy.fft.ifftn(scipy.fft.fftn(hx, workers=nproc), workers=nproc)
+        pocket_ms = 1e3 * (time.perf_counter() - t0) / nrep
+        t0 = time.perf_counter()
+        for _ in range(nrep):
+            qd_ref.fft(qd_ref.fft(hx, -1), 1)
+        port_ms = 1e3 * (time.perf_counter() - t0) / nrep
+        out[name] = {"cufft_ms": cufft_ms, "zqd_fft_seam_ms": own_ms, "seam_over_cufft": own_ms / cufft_ms,
+                     "host_pocketfft_ms": pocket_ms, "host_oracle_fft_ms": port_ms,
+                     "oracle_fft_over_pocketfft": port_ms / pocket_ms}
+    return out
+
+
 def max_over_ranks(x, dist, device):
     """The largest of every rank's x (the timed region of the slowest replica); x itself without a group."""
     if dist is None:
@@ -399,7 +526,16 @@ def main():
                          "for ncu captures")
     ap.add_argument("--table", action="store_true",
                     help="print per-configuration CPU (oracle) and GPU rates as one JSON line and exit")
+    ap.add_argument("--clocks-csv", default=None,
+                    help="where the nvidia-smi samples of the timed region go (default: the system temp dir)")
+    ap.add_argument("--traffic-table", nargs=2, metavar=("NCU_CSV", "LABEL"), default=None,
+                    help="print 'kernel LABEL dram_bytes_per_launch' rows from an ncu --csv capture and exit")
+    ap.add_argument("--no-extra", action="store_true", help="skip the FP32 error table and the FFT brackets")
     args = ap.parse_args()
+
+    if args.traffic_table:
+        print("\n".join(traffic_table(*args.traffic_table)))
+        return
 
     if args.table:
         from zinq_b200 import quantum_dynamics as qd
@@ -475,8 +611,9 @@ def main():
 
     fp64 = qd.Batch(opts, "fp64")
     fp32 = qd.Batch(opts, "fp32")
-    clk = Clocks(local, os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                     f"bench_clocks_rank{rank}.csv"))
+    import tempfile
+
+    clk = Clocks(local, args.clocks_csv or os.path.join(tempfile.gettempdir(), f"zqd_bench_clocks_rank{rank}.csv"))
     t32 = timed(fp32, args.steps, args.warmup)
     t64 = timed(fp64, args.steps, args.warmup)
     clocks = clk.stop()
@@ -491,15 +628,20 @@ def main():
         pop_err = max(pop_err, float(np.max(np.abs(a - b))))
 
     # end to end through the public API, host options -> host results
-    for _ in range(args.warmup):
-        qd.run_batch_e2e(opts, "fp32")
-    barrier()
-    e2e_times, h2d, d2h = [], 0, 0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        _, h2d, d2h = qd.run_batch_e2e(opts, "fp32")
-        e2e_times.append(time.perf_counter() - t0)
-    barrier()
+    def e2e(prec):
+        for _ in range(args.warmup):
+            qd.run_batch_e2e(opts, prec)
+        barrier()
+        ts, hb, db = [], 0, 0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            _, hb, db = qd.run_batch_e2e(opts, prec)
+            ts.append(time.perf_counter() - t0)
+        barrier()
+        return ts, hb, db
+
+    e2e_times, h2d, d2h = e2e("fp32")
+    e2e64_times, h2d64, d2h64 = e2e("fp64")
 
     def maxall(x):
         return max_over_ranks(x, dist, "cuda")
@@ -507,6 +649,7 @@ def main():
     s32 = maxall(sum(t32) / 1e3)
     s64 = maxall(sum(t64) / 1e3)
     se2e = maxall(sum(e2e_times))
+    se2e64 = maxall(sum(e2e64_times))
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -533,15 +676,24 @@ def main():
                        "note": "per job; the 5 jobs of a step complete together in one launch"},
         "e2e": {"value": world * U * args.steps / se2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
+        "e2e_fp64": {"value": world * U * args.steps / se2e64, "unit": UNIT, "h2d_bytes_per_step": int(h2d64),
+                     "d2h_bytes_per_step": int(d2h64)},
         "gpu_launches": launches32,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "note": "algorithmic bytes per grid-pt*state*step (psi r+w once, R read twice); the resident "
-                             "kernel keeps psi in shared memory across steps, so frac > 1 is on-chip residency"},
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of line_solve_kernel on "
+                                       "this workload, tabulated in profiles/traffic.txt by bench.py --traffic-table "
+                                       "(an earlier capture, not this run)",
+                     "note": "algorithmic bytes per grid-pt*state*step (psi r+w once, R read twice).  Not the "
+                             "binding roof: the resident kernel keeps psi in shared memory for the whole solve "
+                             "(DRAM sees the tables once per job); see roofline_onchip"},
         "clocks": clocks,
     }
     if not args.no_nd:
         line["nd"] = nd_legs(qd, torch, flush)
+    if not args.no_extra:
+        line["fp32_errors"] = fp32_error_table(qd)
+        line["fft_brackets"] = fft_brackets(qd, torch)
     if not args.no_serve:
         line["serving"] = serving_leg(qd)
     if not args.no_cpu:

@@ -38,7 +38,8 @@ typedef enum {
     ZQD_ERR_TIMEOUT = -9,       /* a bounded device or host wait ran out */
     ZQD_ERR_CANCELLED = -10,    /* job cancelled through the server */
     ZQD_ERR_NOT_FOUND = -11,    /* unknown job id or result index */
-    ZQD_ERR_NO_DEVICE = -12     /* no CUDA device with sm_100 */
+    ZQD_ERR_NO_DEVICE = -12,    /* no CUDA device with sm_100 */
+    ZQD_ERR_NUMERIC = -13       /* a served job's norm or populations became NaN or Inf */
 } zqd_status;
 
 /* Human-readable text of a status code; the last failing call's detail
@@ -259,9 +260,65 @@ int zqd_job_run(zqd_job* job);                           /* every solve, device-
 int zqd_job_result(zqd_job* job, zqd_result** out);      /* device -> host copy of observables */
 int zqd_job_info(const zqd_job* job, uint32_t* ndim, uint32_t* nstate, uint64_t* npoint_total,
                  uint32_t* cluster_ctas, size_t* device_bytes);
-/* device time (ms, CUDA events on the job's stream) of the last zqd_job_run */
+/* device time (ms, CUDA events on the job's stream) of the last zqd_job_run (or of every
+   zqd_job_step call of the current step-wise run) */
 double zqd_job_device_ms(const zqd_job* job);
 void zqd_job_destroy(zqd_job* job);
+
+/* Step-wise form of zqd_job_run, the solve loop of src/quantum_dynamics.zig:860-950 cut into
+   pieces.  The first call of a run records row 0 (the initial state, after setGaussian and
+   toDia) and then propagates nsteps steps; every later call propagates up to nsteps more.  A call
+   ends at the end of a solve (iterations reached, or stop_norm, :933-944) and runs the solve's
+   final Observables.init (:949); with imaginary.nstate > 1 the next call starts the next solve.
+   The wavefunction stays on the device between calls.  zqd_job_run restarts from the beginning. */
+int zqd_job_step(zqd_job* job, uint32_t nsteps);
+/* the solve in progress (the last one once finished), its rows recorded so far, and whether every
+   solve has ended (zqd_job_result needs that) */
+int zqd_job_progress(const zqd_job* job, uint32_t* solve, uint32_t* rows, int* finished);
+
+/* One observables row per recorded step, as History.append records them
+   (src/quantum_dynamics.zig:174-215): width = 5 + 2 ndim + nstate doubles,
+     [0] norm, [1 .. ndim] position, [1 + ndim .. 2 ndim] momentum,
+     [1 + 2 ndim .. 2 ndim + nstate] population,
+     [1 + 2 ndim + nstate] potential energy, [2 + 2 ndim + nstate] kinetic energy,
+     [3 + 2 ndim + nstate] acf re, [4 + 2 ndim + nstate] acf im,
+   NaN where the option set does not record the value (total energy = potential + kinetic). */
+typedef struct {
+    uint32_t solve;       /* solve (imaginary-time state) of these rows */
+    uint32_t first_row;   /* step index of rows[0] */
+    uint32_t nrows;       /* 0: nothing new */
+    uint32_t width;       /* doubles per row */
+    const double* rows;   /* nrows x width, owned by the job, valid until its next call */
+    int solve_finished;   /* the solve's last row is among these (or was returned earlier) */
+} zqd_obs_rows;
+/* The rows recorded since the previous call (of one solve; call again for the next solve).
+   Works after zqd_job_step and after zqd_job_run. */
+int zqd_job_observables(zqd_job* job, zqd_obs_rows* out);
+
+/* ------------------------------------------------------------ autotuner
+ * (no counterpart in the reference, whose FFTW planner is the nearest thing: fft.plan,
+ * src/fourier_transform.zig:15-23).  Launch shapes per key (dims, points per axis, states,
+ * precision): the 1-D resident kernel's CTAs per cluster and largest local radix, the N-D
+ * passes' rows per row-pass CTA and lines per tile-pass CTA.  zqd_autotune times every shape the
+ * kernels accept for the key on the current device (a synthetic job of that size, CUDA events)
+ * and records the fastest in the process's table, which job creation consults; the file named by
+ * the environment variable ZQD_TUNE_FILE is loaded before the first job.  A tuned shape only
+ * refactors the transforms, so results stay within the parity bars of the default shape.
+ */
+typedef struct {
+    uint32_t ndim, npoint, nstate; /* the key (in) */
+    zqd_precision precision;       /* ZQD_FP64 or ZQD_FP32_MIXED (in) */
+    /* out: the chosen shape (0: the built-in rules' choice was fastest), its time per step and the
+       rules' time per step, and how many candidate shapes the kernels accepted */
+    uint32_t cluster_ctas, radix_log2, rows_per_cta, tile_lines;
+    double us_per_step, default_us_per_step;
+    uint32_t candidates;
+} zqd_tune_entry;
+int zqd_autotune(zqd_tune_entry* entry);
+int zqd_tune_save(const char* path); /* text: one "ndim npoint nstate fp32 C radix_log2 rows tile" line per key */
+int zqd_tune_load(const char* path); /* merges a saved table into the process's table */
+void zqd_tune_clear(void);
+uint32_t zqd_tune_size(void);
 
 /* Several independent jobs advanced together on the device (the batched
    form): one launch per group of jobs with equal kernel shape and precision,
@@ -304,8 +361,11 @@ void zqd_fft_destroy(zqd_fft* plan);
    it until exit), so n is at most 8192; larger n returns ZQD_ERR_UNSUPPORTED.
    The first call on a device looks the array's address up once
    (cudaGetSymbolAddress); make that first call before any stream capture.
-   Every call rewrites the shared table on `cuda_stream`, so calls that
-   overlap on the GPU race with one another.  Allocates nothing. */
+   That address is kept for the life of the process: the entry point assumes
+   the CUDA runtime's primary context of the device and no cudaDeviceReset
+   between calls (after one, the kept address is stale).  Every call rewrites
+   the shared table on `cuda_stream`, so calls that overlap on the GPU race with
+   one another.  Allocates nothing. */
 int zqd_fft_execute_noalloc(uint32_t ndim, const int* shape, int sign, zqd_precision precision, void* device_inout,
                             void* cuda_stream);
 
@@ -339,34 +399,71 @@ int zqd_potential_plot(const zqd_options* opt, double time, double* host_U, size
 
 /* ------------------------------------------------------------------ server
  * A request loop around quantum_dynamics.run for streams of independent jobs
- * (the reference runs one job per process and has no counterpart).  Submission
- * validates and copies the options (errors come back at once, with the
- * reference's messages).  Worker threads admit requests in arrival order while
- * their estimated device memory fits the budget; 1-D single-solve requests of
- * the same precision, state count and grid size that wait together share one
- * launch of the resident line kernel.  zqd_server_wait blocks until a request
- * is done and returns its result (owned by the caller) and its latency from
- * submission to completion.  Results equal those of zqd_run on the same options.
+ * (the reference runs one job per process and has no counterpart).
+ * Submission validates and copies the options (errors come back at once, with
+ * the reference's messages).  Worker threads admit requests in arrival order
+ * while their estimated device memory fits the budget and the device's free
+ * memory (measured with cudaMemGetInfo plus the blocks the library's memory pool
+ * keeps).  A worker advances its jobs in launches of stream_steps steps:
+ * 1-D single-solve requests of the same precision, state count and grid size
+ * share each launch of the resident line kernel, every job at its own step;
+ * between launches finished or cancelled jobs leave and waiting requests of the
+ * same shape join (continuous batching).  After every launch each job's new
+ * observable rows are posted as an event; zqd_server_poll pulls events (nothing
+ * is called back).  Results equal those of zqd_run on the same options.
  */
 typedef struct zqd_server zqd_server;
 typedef struct {
     uint32_t struct_size;         /* sizeof(zqd_server_config); set by zqd_server_config_init */
-    uint32_t workers;             /* host threads, each running one launch at a time (default 4) */
-    uint32_t max_batch;           /* requests per grouped launch (default 16) */
+    uint32_t workers;             /* host threads, each advancing one job or group at a time (default 4) */
+    uint32_t max_batch;           /* jobs per grouped launch (default 16) */
     uint64_t device_budget_bytes; /* 0: 90% of the device memory free at creation */
+    uint32_t stream_steps;        /* steps per launch between event posts (default 256; 0: whole jobs) */
+    int stream_rows;              /* post ZQD_EVENT_ROWS events with the observable rows (default 1) */
+    uint32_t max_events;          /* events kept for zqd_server_poll (default 65536); beyond it the oldest
+                                     row events are dropped and counted, completion events never */
 } zqd_server_config;
 typedef struct {
-    uint64_t submitted, completed, failed, queued;
-    uint64_t grouped_launches, grouped_jobs;
+    uint64_t submitted, completed, failed, cancelled, queued;
+    uint64_t grouped_launches, grouped_jobs, joined_jobs; /* joined: admitted into a group already on the GPU */
     uint64_t device_budget_bytes, device_bytes_in_use, peak_device_bytes;
+    uint64_t pending_events, dropped_events;
 } zqd_server_stats;
+typedef enum {
+    ZQD_EVENT_ROWS = 0,     /* new observable rows of a running job (zqd_obs_rows layout) */
+    ZQD_EVENT_DONE = 1,     /* finished; zqd_server_wait returns the result */
+    ZQD_EVENT_FAILED = 2,   /* status says why; zqd_server_wait returns it */
+    ZQD_EVENT_CANCELLED = 3 /* cancelled before it finished */
+} zqd_event_kind;
+typedef struct {
+    uint64_t ticket;
+    int kind;   /* zqd_event_kind */
+    int status; /* 0, or the failure's status code */
+    uint32_t solve, first_row, nrows, width;
+    int solve_finished;
+    const double* rows; /* nrows x width (ZQD_EVENT_ROWS), valid until the next zqd_server_poll */
+} zqd_event;
 void zqd_server_config_init(zqd_server_config* cfg);
 int zqd_server_create(const zqd_server_config* cfg, zqd_server** out);
 int zqd_server_submit(zqd_server* server, const zqd_options* opt, uint64_t* ticket);
+/* Blocks until the request is done; returns its result (owned by the caller) and its latency
+   from submission to completion.  A ticket is waited for once. */
 int zqd_server_wait(zqd_server* server, uint64_t ticket, zqd_result** out, double* latency_ms);
+/* The same, giving up with ZQD_ERR_TIMEOUT after timeout_ms (the request stays waitable). */
+int zqd_server_wait_timeout(zqd_server* server, uint64_t ticket, uint32_t timeout_ms, zqd_result** out,
+                            double* latency_ms);
+/* A queued request is dropped at once; a running one leaves before its next launch.  Its
+   zqd_server_wait then returns ZQD_ERR_CANCELLED (a request already done keeps its result). */
+int zqd_server_cancel(zqd_server* server, uint64_t ticket);
+/* Moves up to max_events pending events into events[], oldest first; *count receives how many. */
+int zqd_server_poll(zqd_server* server, zqd_event* events, uint32_t max_events, uint32_t* count);
 int zqd_server_stats_get(zqd_server* server, zqd_server_stats* out);
 /* waits for every submitted request, then frees the server */
 void zqd_server_destroy(zqd_server* server);
+
+/* Fault injection for tests of the failure paths (no effect unless called): after `after` more
+   successful device allocations, the next `count` ones fail as if the device were out of memory. */
+void zqd_testing_fail_device_allocations(uint64_t after, uint64_t count);
 
 /* ------------------------------------------------------------------ device */
 int zqd_device_count(void);

@@ -224,3 +224,24 @@ def test_2d_wavefunction_history_adiabatic():
            "mass": [100, 50], "iterations": 40, "time_step": 0.5, "adiabatic": True,
            "write": {"population": "P", "wavefunction": "W", "kinetic_energy": "T"}}
     compare(opt)
+
+
+def test_2d_time_dependent_adiabatic_wavefunction_history_signs():
+    # eigenvector signs flip at t = 2.5 (the diagonal difference changes sign); the global alignment
+    # with the previous update (wavepacket.zig:157-167) keeps the adiabatic history continuous
+    opt = {"grid": {"bounds": [[-6, 6], [-6, 6]], "npoint": 32},
+           "initial_conditions": {"position": [-1, 0.5], "momentum": [0.5, 0], "gamma": [1, 1], "state": 0,
+                                  "adiabatic": True},
+           "potential": {"custom": {"ndim": 2, "time_dependent": True,
+                                    "matrix": [["0.5*(r1^2+r2^2) + (t - 2.5)*0.4", "0.3"],
+                                               ["0.3", "0.5*(r1^2+r2^2) - (t - 2.5)*0.4"]]}},
+           "mass": [1, 1], "iterations": 500, "time_step": 0.01, "adiabatic": True,
+           "write": {"population": "P", "wavefunction": "W"}}
+    compare(opt)
+    job = qd.Job(opt)  # graph replay: the second run starts again from the t = 0 tables
+    job.run()
+    job.run()
+    g = job.result().observables[0]
+    job.close()
+    r = qd_ref.run(opt)[0]
+    assert float(np.max(np.abs(g.history["wavefunction"] - r.history["wfn"]))) <= 1e-10

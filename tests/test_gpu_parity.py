@@ -29,9 +29,12 @@ def psi_rel(g, r):
     return float(np.linalg.norm(g - r) / np.linalg.norm(r))
 
 
-def compare(opt, precision="fp64", pop_tol=POP_TOL, psi_tol=PSI_TOL, obs_tol=1e-10, sign_free=False):
+def compare(opt, precision="fp64", pop_tol=POP_TOL, psi_tol=PSI_TOL, obs_tol=1e-10, sign_free=False, nthreads=1,
+            ref=None):
+    """GPU run of opt against the oracle (or against `ref`, an oracle result already computed)."""
     gpu = qd.run(opt, precision=precision)
-    ref = qd_ref.run(opt)
+    if ref is None:
+        ref = qd_ref.run(opt, nthreads=nthreads)
     assert len(gpu.observables) == len(ref)
     worst = {}
     for g, r in zip(gpu.observables, ref):
@@ -289,3 +292,45 @@ def test_radix8_kernel_for_lines_above_the_radix4_thread_limit():
            "potential": {"harmonic": {"k": [0.01]}}, "mass": [2000], "iterations": 100, "time_step": 1,
            "adiabatic": False, "write": {"position": "X", "momentum": "K", "total_energy": "E"}}
     compare(opt)
+
+
+# ---------------------------------------------------------------- eigenvector signs of time-dependent potentials
+def td_crossing_1d(iters=500):
+    # the diagonal difference changes sign at t = 2.5: LAPACK's eigenvector signs flip there, the
+    # global alignment with the previous update (wavepacket.zig:157-167) flips them back
+    return {"grid": {"bounds": [[-8, 8]], "npoint": 256},
+            "initial_conditions": {"momentum": [0.5], "position": [-1], "state": 0, "gamma": [1], "adiabatic": True},
+            # the diagonal difference 0.8 (t - 2.5) + 0.1 r1 also changes sign along the grid (continuity rule);
+            # the constant coupling keeps the adiabatic gap >= 0.6
+            "potential": {"custom": {"ndim": 1, "time_dependent": True,
+                                     "matrix": [["0.5*r1^2 + (t - 2.5)*0.4 + 0.05*r1", "0.3"],
+                                                ["0.3", "0.5*r1^2 - (t - 2.5)*0.4 - 0.05*r1"]]}},
+            "mass": [1], "iterations": iters, "time_step": 0.01, "adiabatic": True,
+            "write": {"population": "P", "wavefunction": "W"}}
+
+
+@pytest.mark.parametrize("cluster", ["1", "4"])
+def test_time_dependent_adiabatic_wavefunction_history_signs(cluster, monkeypatch):
+    # compared without sign freedom: continuity along the grid and alignment across updates
+    monkeypatch.setenv("ZQD_LINE_CLUSTER", cluster)
+    gpu, _, worst = compare(td_crossing_1d())
+    assert gpu.observables[0].history["wavefunction"].shape == (501, 2, 256)
+
+
+def test_time_dependent_imaginary_time_later_solve_uses_aligned_eigenvectors():
+    # the second solve's toDia uses the eigenvectors left by the first solve's last update
+    opt = td_crossing_1d(iters=300)
+    opt["imaginary"] = {"nstate": 2}
+    opt["write"] = {"total_energy": "E", "norm": "N"}
+    compare(opt)
+
+
+def test_time_dependent_job_run_twice_starts_from_t0_tables():
+    opt = td_crossing_1d(iters=200)
+    job = qd.Job(opt)
+    job.run()
+    job.run()
+    g = job.result().observables[0]
+    job.close()
+    r = qd_ref.run(opt)[0]
+    assert float(np.max(np.abs(g.history["wavefunction"] - r.history["wfn"]))) <= 1e-10

@@ -62,6 +62,18 @@ def test_noalloc_fft_matches_plan_fft_on_two_calls_in_a_row(precision):
         assert np.max(np.abs(got - ref)) <= tol * scale
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_noalloc_fft_3d_matches_numpy(precision):
+    # three strided axis passes and the twiddles made on the device, against numpy directly
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((16, 16, 16)) + 1j * rng.standard_normal((16, 16, 16))
+    tol = 1e-12 if precision == "fp64" else 2e-6
+    fwd = _noalloc_fft(x, -1, precision)
+    assert np.max(np.abs(fwd - np.fft.fftn(x))) <= tol * np.sqrt(x.size) * np.abs(x).max()
+    inv = _noalloc_fft(x, +1, precision)
+    assert np.max(np.abs(inv - np.fft.ifftn(x))) <= tol * np.abs(x).max()
+
+
 def test_noalloc_fft_rejects_sizes_beyond_its_table():
     import torch
 

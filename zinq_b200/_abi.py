@@ -18,7 +18,7 @@ STATUS = {
     0: "ZQD_OK", -1: "ZQD_ERR_INVALID_INPUT", -2: "ZQD_ERR_OUT_OF_MEMORY", -3: "ZQD_ERR_DEVICE_OOM",
     -4: "ZQD_ERR_PLAN_FAILED", -5: "ZQD_ERR_EIGEN_FAILED", -6: "ZQD_ERR_EXPRESSION", -7: "ZQD_ERR_UNSUPPORTED",
     -8: "ZQD_ERR_DEVICE", -9: "ZQD_ERR_TIMEOUT", -10: "ZQD_ERR_CANCELLED", -11: "ZQD_ERR_NOT_FOUND",
-    -12: "ZQD_ERR_NO_DEVICE",
+    -12: "ZQD_ERR_NO_DEVICE", -13: "ZQD_ERR_NUMERIC",
 }
 
 POT = {"harmonic": 0, "time_linear": 1, "tully_1": 2, "tully_2": 3, "tully_3": 4, "custom": 5, "lvc": 6, "file": 7}
@@ -80,15 +80,38 @@ class ZqdWritePaths(C.Structure):
     _fields_ = [(n, C.c_char_p) for n in WRITE_PATH_FIELDS]
 
 
+class ZqdObsRows(C.Structure):
+    _fields_ = [("solve", C.c_uint32), ("first_row", C.c_uint32), ("nrows", C.c_uint32), ("width", C.c_uint32),
+                ("rows", DP), ("solve_finished", C.c_int)]
+
+
 class ZqdServerConfig(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
-                ("device_budget_bytes", C.c_uint64)]
+                ("device_budget_bytes", C.c_uint64), ("stream_steps", C.c_uint32), ("stream_rows", C.c_int),
+                ("max_events", C.c_uint32)]
 
 
 class ZqdServerStats(C.Structure):
-    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "queued", "grouped_launches",
-                                          "grouped_jobs", "device_budget_bytes", "device_bytes_in_use",
-                                          "peak_device_bytes")]
+    _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "cancelled", "queued",
+                                          "grouped_launches", "grouped_jobs", "joined_jobs", "device_budget_bytes",
+                                          "device_bytes_in_use", "peak_device_bytes", "pending_events",
+                                          "dropped_events")]
+
+
+EVENT = {0: "rows", 1: "done", 2: "failed", 3: "cancelled"}
+
+
+class ZqdTuneEntry(C.Structure):
+    _fields_ = [("ndim", C.c_uint32), ("npoint", C.c_uint32), ("nstate", C.c_uint32), ("precision", C.c_int),
+                ("cluster_ctas", C.c_uint32), ("radix_log2", C.c_uint32), ("rows_per_cta", C.c_uint32),
+                ("tile_lines", C.c_uint32), ("us_per_step", C.c_double), ("default_us_per_step", C.c_double),
+                ("candidates", C.c_uint32)]
+
+
+class ZqdEvent(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("kind", C.c_int), ("status", C.c_int), ("solve", C.c_uint32),
+                ("first_row", C.c_uint32), ("nrows", C.c_uint32), ("width", C.c_uint32), ("solve_finished", C.c_int),
+                ("rows", DP)]
 
 
 # (name, restype, argtypes) for every entry point of zinq_qd.h
@@ -119,6 +142,9 @@ SIGNATURES = [
                                C.POINTER(C.c_uint32), C.POINTER(C.c_size_t)]),
     ("zqd_job_device_ms", C.c_double, [VP]),
     ("zqd_job_destroy", None, [VP]),
+    ("zqd_job_step", C.c_int, [VP, C.c_uint32]),
+    ("zqd_job_progress", C.c_int, [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)]),
+    ("zqd_job_observables", C.c_int, [VP, C.POINTER(ZqdObsRows)]),
     ("zqd_run_batch", C.c_int, [C.POINTER(C.POINTER(ZqdOptions)), C.c_uint32, C.POINTER(VP)]),
     ("zqd_batch_create", C.c_int, [C.POINTER(C.POINTER(ZqdOptions)), C.c_uint32, C.POINTER(VP)]),
     ("zqd_batch_run", C.c_int, [VP]),
@@ -140,8 +166,17 @@ SIGNATURES = [
     ("zqd_server_create", C.c_int, [C.POINTER(ZqdServerConfig), C.POINTER(VP)]),
     ("zqd_server_submit", C.c_int, [VP, C.POINTER(ZqdOptions), C.POINTER(C.c_uint64)]),
     ("zqd_server_wait", C.c_int, [VP, C.c_uint64, C.POINTER(VP), C.POINTER(C.c_double)]),
+    ("zqd_server_wait_timeout", C.c_int, [VP, C.c_uint64, C.c_uint32, C.POINTER(VP), C.POINTER(C.c_double)]),
+    ("zqd_server_cancel", C.c_int, [VP, C.c_uint64]),
+    ("zqd_server_poll", C.c_int, [VP, C.POINTER(ZqdEvent), C.c_uint32, C.POINTER(C.c_uint32)]),
     ("zqd_server_stats_get", C.c_int, [VP, C.POINTER(ZqdServerStats)]),
     ("zqd_server_destroy", None, [VP]),
+    ("zqd_testing_fail_device_allocations", None, [C.c_uint64, C.c_uint64]),
+    ("zqd_autotune", C.c_int, [C.POINTER(ZqdTuneEntry)]),
+    ("zqd_tune_save", C.c_int, [C.c_char_p]),
+    ("zqd_tune_load", C.c_int, [C.c_char_p]),
+    ("zqd_tune_clear", None, []),
+    ("zqd_tune_size", C.c_uint32, []),
     ("zqd_device_count", C.c_int, []),
     ("zqd_set_device", C.c_int, [C.c_int]),
 ]

@@ -23,6 +23,8 @@ const char* last_error();
 // time); a pool free waits for nothing.  Freed blocks stay cached in the pool for later jobs.
 cudaError_t dev_alloc(void** p, size_t bytes);
 void dev_free(void* p);
+// device memory this process can still allocate: free HBM plus the blocks the pool keeps for reuse
+size_t device_free_bytes();
 
 #define ZQD_CUDA(call)                                                                                             \
     do {                                                                                                           \

@@ -165,7 +165,7 @@ template <int S> __global__ void sign_scan_kernel(double* U, int n, int m, int C
         for (int x = max(x0, 1); x < x1; ++x) {
             double ov = 0;
             for (int k = 0; k < S; ++k)
-                ov += U[(size_t)(k * S + jcol) * n + pos(x)] * U[(size_t)(k * S + jcol) * n + pos(x - 1)];
+                ov = __dadd_rn(ov, __dmul_rn(U[(size_t)(k * S + jcol) * n + pos(x)], U[(size_t)(k * S + jcol) * n + pos(x - 1)]));
             int cd = ov > 0 ? 0 : (ov < 0 ? 1 : 2);
             code[x] = (signed char)cd;
             if (cd == 1) {
@@ -225,8 +225,13 @@ template <typename T> static size_t cxsize() { return sizeof(cx<T>); }
 // FP64, 32768 in FP32); radix-4-only kernels keep the instruction footprint small.
 static int choose_line_shape(zqd_job* J) {
     const size_t budget = 205 * 1024; // dynamic shared memory per CTA
-    int forced = 0;
-    if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env);
+    int forced = 0, forced_lr = 0;
+    ShapeOverride ov;
+    if (lookup_shape(1, J->n, J->S, J->fp32, ov)) { // autotuned (or being measured by the autotuner)
+        forced = ov.C;
+        forced_lr = ov.lrmax;
+    }
+    if (const char* env = std::getenv("ZQD_LINE_CLUSTER")) forced = std::atoi(env), forced_lr = 0;
     const int target = 256;
     // pass 0: the smallest C with at most `target` points per CTA; 1: the largest C that fits
     // (fewest points per CTA); 2: the same with R read from global memory
@@ -244,6 +249,8 @@ static int choose_line_shape(zqd_job* J) {
             int lrmax = 2;
             const int tmax = J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value;
             if (((m >> 2) + 31) / 32 * 32 > tmax) lrmax = 3;
+            if (forced_lr == 3) lrmax = 3;
+            else if (forced_lr == 2 && lrmax != 2) continue;
             if (lrmax == 3 && C != 16) continue; // radix 8 is built for 16-CTA clusters only
             if (std::max(32, ((m >> lrmax) + 31) / 32 * 32) > tmax) continue;
             // one thread per butterfly of every state (passes without state-mixing hooks split
@@ -356,6 +363,9 @@ template <typename T> static int create_line(zqd_job* J) {
         {&J->scratch, n + 16},
         {&J->wfn_hist, (J->o.write_mask & ZQD_WRITE_WAVEFUNCTION) ? (size_t)J->nsolve * rows * S * n * c : 0},
         {&J->psi_init, J->o.ic_wfn.empty() ? 0 : S * n * c},
+        {&J->sgn, needs_sign_tracking(J->o, J->S, J->nsolve) ? S * n * sizeof(double) : 0},
+        {&J->carry, (size_t)J->nsolve * S * sizeof(double)},
+        {&J->done, (size_t)J->nsolve * sizeof(int)},
     };
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t total = 0;
@@ -433,6 +443,8 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
     L.psi_init = J->psi_init.as<cx<T>>();
     L.r_global = J->r_global ? 1 : 0;
     L.lrmax = J->lrmax;
+    L.sign_track = needs_sign_tracking(o, J->S, J->nsolve) ? 1 : 0;
+    L.sgn = J->sgn.as<double>();
     L.wfn_hist = J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + (size_t)s * ((size_t)o.iterations + 1) * J->S * J->n : nullptr;
     L.expk = J->expk.as<Tab<T>>();
     L.V = J->V.as<double>();
@@ -447,12 +459,45 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
     L.hist = J->hist.as<double>() + (size_t)s * rows * J->hc;
     L.fin = J->fin.as<double>() + (size_t)s * J->hc;
     L.rows = J->rows.as<int>() + s;
+    L.i0 = 0;
+    L.i1 = L.iters;
+    L.carry = J->carry.as<double>() + (size_t)s * J->S;
+    L.done = J->done.as<int>() + s;
     L.pot = J->pot.dev;
     return L;
 }
 
+// A time-dependent potential leaves the tables at the last update's time: a later run of the same
+// job starts again from the t = 0 tables (Hamiltonian.init, Propagator.init).
+template <typename T> static int refresh_line_tables(zqd_job* J) {
+    if (!J->o.pot_td || J->runs++ == 0) return ZQD_OK;
+    return run_tables_s<T>(J);
+}
+
+// the start of a run (whole or step-wise): progress and observable cursors back to zero
+static void reset_progress(zqd_job* J) {
+    J->step_solve = 0;
+    J->solve_rows.assign(J->nsolve, 0);
+    J->solve_ended.assign(J->nsolve, 0);
+    J->obs_solve = J->obs_row = 0;
+    J->stepping = false;
+}
+
+// after a whole run: every solve ended, with the row counts the device recorded
+static int mark_all_ended(zqd_job* J) {
+    std::vector<int> rows(J->nsolve);
+    ZQD_CUDA(cudaMemcpyAsync(rows.data(), J->rows.p, rows.size() * sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->solve_rows = rows;
+    J->solve_ended.assign(J->nsolve, 1);
+    J->step_solve = J->nsolve;
+    return ZQD_OK;
+}
+
 template <typename T> static int run_line(zqd_job* J) {
     const size_t SN = (size_t)J->S * J->n * sizeof(cx<T>);
+    reset_progress(J);
+    if (int rc = refresh_line_tables<T>(J)) return rc;
     std::vector<LineJob<T>> descs;
     for (int s = 0; s < J->nsolve; ++s) descs.push_back(line_job_desc<T>(J, s));
     ZQD_CUDA(cudaMemcpyAsync(J->jobs.p, descs.data(), descs.size() * sizeof(LineJob<T>), cudaMemcpyHostToDevice, J->stream));
@@ -469,6 +514,32 @@ template <typename T> static int run_line(zqd_job* J) {
     ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
+    return mark_all_ended(J);
+}
+
+// One launch of rows i0..i1 of solve s of a 1-D job (zqd_job_step); *rows and *ended come back
+// from the device.
+template <typename T> static int step_line(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
+    LineJob<T> d = line_job_desc<T>(J, s);
+    d.i0 = i0;
+    d.i1 = i1;
+    ZQD_CUDA(cudaMemcpyAsync(J->jobs.as<LineJob<T>>() + s, &d, sizeof(d), cudaMemcpyHostToDevice, J->stream));
+    J->h2d += sizeof(d);
+    LaunchShape sh{J->S, J->C, J->E, J->threads, J->smem, J->stream};
+    sh.lrmax = J->lrmax;
+    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+    if (int rc = launch_line_s<T>(&sh, J->jobs.as<LineJob<T>>() + s, 1)) return rc;
+    ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+    int flags[2] = {0, 0};
+    ZQD_CUDA(cudaMemcpyAsync(&flags[0], J->rows.as<int>() + s, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaMemcpyAsync(&flags[1], J->done.as<int>() + s, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    float ms = 0;
+    ZQD_CUDA(cudaEventElapsedTime(&ms, J->ev0, J->ev1));
+    J->last_ms += ms;
+    J->d2h += sizeof(flags);
+    *rows = flags[0];
+    *ended = flags[1];
     return ZQD_OK;
 }
 
@@ -596,7 +667,10 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
 }
 
 // N-D drivers compiled in nd_inst.cu, one translation unit per (precision, states)
-#define ZQD_ND_DECL(t, s) int nd_create_##t##s(zqd_job*); int nd_run_##t##s(zqd_job*);
+#define ZQD_ND_DECL(t, s)                                                                                           \
+    int nd_create_##t##s(zqd_job*);                                                                                 \
+    int nd_run_##t##s(zqd_job*);                                                                                    \
+    int nd_step_##t##s(zqd_job*, int, int, int, int*, int*);
 ZQD_ND_DECL(d, 1) ZQD_ND_DECL(d, 2) ZQD_ND_DECL(d, 3) ZQD_ND_DECL(d, 4)
 ZQD_ND_DECL(f, 1) ZQD_ND_DECL(f, 2) ZQD_ND_DECL(f, 3) ZQD_ND_DECL(f, 4)
 #undef ZQD_ND_DECL
@@ -609,7 +683,50 @@ static int nd_create(zqd_job* J) {
 static int nd_run(zqd_job* J) {
     static int (*const dt[4])(zqd_job*) = {nd_run_d1, nd_run_d2, nd_run_d3, nd_run_d4};
     static int (*const ft[4])(zqd_job*) = {nd_run_f1, nd_run_f2, nd_run_f3, nd_run_f4};
-    return J->fp32 ? ft[J->S - 1](J) : dt[J->S - 1](J);
+    reset_progress(J);
+    const int rc = J->fp32 ? ft[J->S - 1](J) : dt[J->S - 1](J);
+    return rc ? rc : mark_all_ended(J);
+}
+static int nd_step(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
+    using Fn = int (*)(zqd_job*, int, int, int, int*, int*);
+    static const Fn dt[4] = {nd_step_d1, nd_step_d2, nd_step_d3, nd_step_d4};
+    static const Fn ft[4] = {nd_step_f1, nd_step_f2, nd_step_f3, nd_step_f4};
+    return (J->fp32 ? ft : dt)[J->S - 1](J, s, i0, i1, rows, ended);
+}
+
+// Advances a job by up to nsteps propagation steps (zqd_job_step).  The first call of a run also
+// records row 0 (the initial state); a call never crosses into the next imaginary-time solve.
+static int job_step(zqd_job* J, uint32_t nsteps) {
+    if (!J->stepping) {
+        reset_progress(J);
+        J->stepping = true;
+        if (J->d == 1) {
+            const int rc = J->fp32 ? refresh_line_tables<float>(J) : refresh_line_tables<double>(J);
+            if (rc) return rc;
+        }
+        J->last_ms = 0;
+    }
+    const int s = J->step_solve;
+    if (s >= J->nsolve || nsteps == 0) return ZQD_OK;
+    const int iters = (int)J->o.iterations, i0 = J->solve_rows[s];
+    const long long want = i0 == 0 ? (long long)nsteps : (long long)i0 + nsteps - 1;
+    const int i1 = (int)std::min<long long>(iters, want);
+    int rows = 0, ended = 0, rc;
+    if (J->d > 1) rc = nd_step(J, s, i0, i1, &rows, &ended);
+    else rc = J->fp32 ? step_line<float>(J, s, i0, i1, &rows, &ended) : step_line<double>(J, s, i0, i1, &rows, &ended);
+    if (rc) return rc;
+    J->solve_rows[s] = rows;
+    if (ended) {
+        J->solve_ended[s] = 1;
+        if (J->d == 1 && s + 1 < J->nsolve) { // orthw.append (quantum_dynamics.zig:586-591)
+            const size_t SN = (size_t)J->S * J->n * (J->fp32 ? sizeof(cx<float>) : sizeof(cx<double>));
+            ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice,
+                                     J->stream));
+            ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        }
+        ++J->step_solve;
+    }
+    return ZQD_OK;
 }
 
 } // namespace zqd
@@ -662,8 +779,54 @@ extern "C" int zqd_job_run(zqd_job* J) {
     return J->fp32 ? run_line<float>(J) : run_line<double>(J);
 }
 
+extern "C" int zqd_job_step(zqd_job* J, uint32_t nsteps) {
+    if (!J) return fail(ZQD_ERR_INVALID_INPUT, "NULL JOB");
+    return job_step(J, nsteps);
+}
+
+extern "C" int zqd_job_progress(const zqd_job* J, uint32_t* solve, uint32_t* rows, int* finished) {
+    if (!J) return fail(ZQD_ERR_INVALID_INPUT, "NULL JOB");
+    const int s = std::min(J->step_solve, J->nsolve - 1);
+    if (solve) *solve = (uint32_t)s;
+    if (rows) *rows = J->solve_rows.empty() ? 0u : (uint32_t)J->solve_rows[s];
+    if (finished) *finished = J->step_solve >= J->nsolve ? 1 : 0;
+    return ZQD_OK;
+}
+
+extern "C" int zqd_job_observables(zqd_job* J, zqd_obs_rows* out) {
+    if (!J || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    *out = zqd_obs_rows{};
+    out->width = (uint32_t)J->hc;
+    if (J->solve_rows.empty()) return ZQD_OK; // nothing ran yet
+    // the first solve with rows not yet returned
+    while (J->obs_solve < J->nsolve && J->obs_row >= J->solve_rows[J->obs_solve] && J->solve_ended[J->obs_solve] &&
+           J->obs_solve + 1 < J->nsolve) {
+        ++J->obs_solve;
+        J->obs_row = 0;
+    }
+    const int s = J->obs_solve, r0 = J->obs_row, r1 = J->solve_rows[s];
+    out->solve = (uint32_t)s;
+    out->first_row = (uint32_t)r0;
+    if (r1 <= r0) {
+        out->solve_finished = J->solve_ended[s];
+        return ZQD_OK;
+    }
+    const size_t rows_per_solve = (size_t)J->o.iterations + 1;
+    J->obs_buf.resize((size_t)(r1 - r0) * J->hc);
+    ZQD_CUDA(cudaMemcpyAsync(J->obs_buf.data(), J->hist.as<double>() + ((size_t)s * rows_per_solve + r0) * J->hc,
+                             J->obs_buf.size() * sizeof(double), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->d2h += J->obs_buf.size() * sizeof(double);
+    J->obs_row = r1;
+    out->nrows = (uint32_t)(r1 - r0);
+    out->rows = J->obs_buf.data();
+    out->solve_finished = J->solve_ended[s] && r1 == J->solve_rows[s];
+    return ZQD_OK;
+}
+
 extern "C" int zqd_job_result(zqd_job* J, zqd_result** out) {
     if (!J || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    if (J->step_solve < J->nsolve) return fail(ZQD_ERR_INVALID_INPUT, "JOB HAS NOT FINISHED (zqd_job_run or zqd_job_step until finished)");
     std::unique_ptr<zqd_result> R(new (std::nothrow) zqd_result());
     if (!R) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
     int rc = J->fp32 ? fetch_line<float>(J, R.get()) : fetch_line<double>(J, R.get());
@@ -786,6 +949,12 @@ extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, 
 extern "C" int zqd_batch_run(zqd_batch* B) {
     if (!B) return fail(ZQD_ERR_INVALID_INPUT, "NULL BATCH");
     B->launches = 0;
+    for (auto& g : B->groups)
+        for (zqd_job* J : g->members) {
+            const int rc = g->fp32 ? refresh_line_tables<float>(J) : refresh_line_tables<double>(J);
+            if (rc) return rc;
+            if (J->o.pot_td) ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        }
     ZQD_CUDA(cudaEventRecord(B->ev0, B->stream));
     for (auto& g : B->groups) {
         int rc = g->fp32 ? launch_line_s<float>(&g->shape, g->descs.p, (int)g->members.size())
@@ -805,7 +974,10 @@ extern "C" int zqd_batch_run(zqd_batch* B) {
     for (zqd_job* J : B->solo) ms = std::max(ms, J->last_ms);
     B->last_ms = ms;
     for (auto& g : B->groups)
-        for (zqd_job* J : g->members) J->last_ms = ms;
+        for (zqd_job* J : g->members) {
+            J->last_ms = ms;
+            if (int rc = mark_all_ended(J)) return rc;
+        }
     return ZQD_OK;
 }
 
@@ -849,7 +1021,10 @@ int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, floa
         ZQD_CUDA(cudaStreamSynchronize(st));
         float t = 0;
         ZQD_CUDA(cudaEventElapsedTime(&t, e0, e1));
-        for (zqd_job* J : jobs) J->last_ms = t;
+        for (zqd_job* J : jobs) {
+            J->last_ms = t;
+            if ((rc = mark_all_ended(J))) return rc;
+        }
         if (ms) *ms = t;
         return ZQD_OK;
     };
@@ -857,6 +1032,72 @@ int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, floa
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;
+}
+
+// One launch advancing single-solve 1-D jobs of one kernel shape by up to nsteps each, every job
+// from its own position (continuous batching: members join and leave between launches).  Like
+// zqd_job_step per member; waits for the launch.
+int zqd::step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cudaStream_t st) {
+    if (jobs.empty() || nsteps == 0) return ZQD_OK;
+    const zqd_job* a = jobs[0];
+    for (const zqd_job* J : jobs)
+        if (J->d != 1 || J->nsolve != 1 || J->fp32 != a->fp32 || J->S != a->S || J->C != a->C || J->r_global != a->r_global ||
+            J->lrmax != a->lrmax)
+            return fail(ZQD_ERR_INVALID_INPUT, "JOBS OF ONE GROUP MUST SHARE PRECISION, STATES AND CLUSTER SHAPE");
+    LaunchShape sh{a->S, a->C, a->E, 0, 0, st};
+    sh.lrmax = a->lrmax;
+    std::vector<int> i0(jobs.size()), i1(jobs.size());
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        zqd_job* J = jobs[k];
+        if (!J->stepping) {
+            reset_progress(J);
+            J->stepping = true;
+            J->last_ms = 0;
+            const int rc = J->fp32 ? refresh_line_tables<float>(J) : refresh_line_tables<double>(J);
+            if (rc) return rc;
+            ZQD_CUDA(cudaStreamSynchronize(J->stream));
+        }
+        if (J->step_solve >= J->nsolve) return fail(ZQD_ERR_INVALID_INPUT, "JOB OF THE GROUP HAS ALREADY FINISHED");
+        i0[k] = J->solve_rows[0];
+        const long long want = i0[k] == 0 ? (long long)nsteps : (long long)i0[k] + nsteps - 1;
+        i1[k] = (int)std::min<long long>((long long)J->o.iterations, want);
+        sh.threads = std::max(sh.threads, J->threads);
+        sh.smem = std::max(sh.smem, J->smem);
+    }
+    DevBuf descs;
+    std::vector<int> flags(2 * jobs.size());
+    auto go = [&](auto tag) -> int {
+        using T = decltype(tag);
+        std::vector<LineJob<T>> d;
+        for (size_t k = 0; k < jobs.size(); ++k) {
+            d.push_back(line_job_desc<T>(jobs[k], 0));
+            d.back().i0 = i0[k];
+            d.back().i1 = i1[k];
+            jobs[k]->h2d += sizeof(LineJob<T>);
+        }
+        int rc;
+        if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+        ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
+        if ((rc = launch_line_s<T>(&sh, descs.p, (int)jobs.size()))) return rc;
+        return ZQD_OK;
+    };
+    int rc = a->fp32 ? go(float{}) : go(double{});
+    if (rc) return rc;
+    for (size_t k = 0; k < jobs.size(); ++k) { // rows written and the end flag of every member
+        ZQD_CUDA(cudaMemcpyAsync(&flags[2 * k], jobs[k]->rows.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ZQD_CUDA(cudaMemcpyAsync(&flags[2 * k + 1], jobs[k]->done.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    ZQD_CUDA(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        zqd_job* J = jobs[k];
+        J->d2h += 2 * sizeof(int);
+        J->solve_rows[0] = flags[2 * k];
+        if (flags[2 * k + 1]) {
+            J->solve_ended[0] = 1;
+            J->step_solve = 1;
+        }
+    }
+    return ZQD_OK;
 }
 
 extern "C" int zqd_batch_result(zqd_batch* B, uint32_t i, zqd_result** out) {

@@ -47,6 +47,20 @@ struct zqd_job;
 namespace zqd {
 int job_create_opts(Opts&& o, zqd_job** out);
 int run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, float* ms);
+int step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cudaStream_t st);
+// Launch shape chosen by the autotuner (tune.cu) for a (dims, points, states, precision) key, or
+// forced on this thread while the autotuner measures a candidate; zero fields keep the default.
+struct ShapeOverride {
+    int C = 0, lrmax = 0; // 1-D: CTAs per cluster, log2 of the largest local radix
+    int rows = 0, tile = 0; // N-D: rows of the last axis per row-pass CTA, lines per tile-pass CTA
+};
+bool lookup_shape(int d, int n, int S, bool fp32, ShapeOverride& out);
+// Time-dependent potential whose eigenvector signs some output observes: the wavefunction history in
+// the adiabatic basis, or the toDia of a later imaginary-time solve (wavepacket.zig:145-167 then apply).
+inline bool needs_sign_tracking(const Opts& o, int S, int nsolve) {
+    return o.pot_td && S > 1 &&
+           (((o.write_mask & ZQD_WRITE_WAVEFUNCTION) && o.adiabatic) || (o.ic_adiabatic && nsolve > 1));
+}
 } // namespace zqd
 
 struct zqd_job {
@@ -66,12 +80,23 @@ struct zqd_job {
     zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
     zqd::DevBuf psi_init;               // initial wavefunction replacing the Gaussian (1-D: permuted layout)
     zqd::DevBuf wfn_hist;               // write.wavefunction: [solve][step][S][N] (1-D: permuted layout)
+    zqd::DevBuf sgn;                    // eigenvector overlaps with the previous update (sign tracking)
+    zqd::DevBuf carry, done;            // 1-D: absorbed populations between launches; per-solve end flags
     zqd::DevBuf arena;                  // 1-D jobs: one pool block holding the buffers above (views)
     double min_gap = -1;                // ZQD_PRECISION_AUTO: smallest adiabatic gap on the grid (-1: not computed)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)
     float last_ms = 0;
+    int runs = 0; // runs started (a time-dependent potential's tables are rebuilt for every later run)
+    // step-wise progress (zqd_job_step): the solve in progress, rows recorded per solve, solves ended
+    int step_solve = 0;
+    std::vector<int> solve_rows; // rows of each solve's history written so far
+    std::vector<char> solve_ended;
+    bool stepping = false; // a step-wise run is in progress
+    // zqd_job_observables cursor and its host buffer
+    int obs_solve = 0, obs_row = 0;
+    std::vector<double> obs_buf;
     size_t device_bytes = 0;
     uint64_t h2d = 0, d2h = 0; // bytes copied by this job
     ~zqd_job() {

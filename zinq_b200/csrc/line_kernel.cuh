@@ -77,10 +77,21 @@ template <typename T> struct LineJob {
     int r_global;          // R read from global memory instead of shared memory
     int lrmax;             // log2 of the largest local radix (threads per CTA = m >> lrmax)
     cx<T>* wfn_hist;       // [step][S][n] permuted wavefunction history of this solve, or null
+    // time-dependent potentials whose eigenvector signs are observed (the adiabatic wavefunction
+    // history, or the toDia of a later imaginary-time solve): after every update the 1-D
+    // continuity rule and the global alignment with the previous update (wavepacket.zig:145-167)
+    int sign_track;
+    double* sgn; // [S][n] natural order: overlap of each new eigenvector with the previous one
     int northo;
     double* hist;
     double* fin;
-    int* rows;
+    int* rows; // rows of the history written so far
+    // Step range of this launch: rows i0..i1 of the solve (0..iters for the whole solve).  A launch
+    // with i0 > 0 resumes from psi_save and the carried absorbed populations; a launch that ends
+    // before the last step (and before stop_norm) saves both instead of the final observables.
+    int i0, i1;
+    double* carry; // [S] absorbed populations between launches of one solve
+    int* done;     // 1 once the solve has ended (last step or stop_norm)
     PotDev pot;
 };
 

@@ -232,18 +232,133 @@ template <typename T, int S, int C> __device__ __noinline__ void line_orthogonal
     }
 }
 
+// Sign maps of the 1-D eigenvector continuity scan, two bits: 0 s -> s, 1 s -> -s, 2 s -> +1,
+// 3 s -> -1 (a sign s is the bit 0 for +1, 1 for -1).  map_after(f, g) is f applied after g.
+__device__ __forceinline__ int map_after(int f, int g) { return (f & 2) ? f : (g ^ (f & 1)); }
+
+// Eigenvector signs after a time-dependent update (Hamiltonian.update, wavepacket.zig:145-167).
+// J.U holds this update's raw eigenvectors, J.sgn their overlaps d_x with the previous update's
+// (natural order).  Continuity (:145-155): at x > 0 the vector is flipped when its overlap with
+// the already fixed vector at x - 1 is negative, i.e. s_x = s_{x-1}, -s_{x-1} or +1 for a
+// positive, negative or zero raw overlap, s_0 = +1: a scan of sign maps.  CTA c scans the natural
+// points [c m, (c+1) m) -- per thread a run of points, then warps, the CTA and the cluster.
+// Global alignment (:157-167): g_j = sign of sum_x s_x d_x (the new vectors after continuity
+// against the previous ones), and U <- g_j s_x U.  The overlaps are rounded like the reference's
+// (separate multiply and add, in k order), so the decisions are its decisions.
+template <typename T, int S, int C> __device__ __noinline__ void line_sign_align(const LineCtx<T>& X) {
+    const LineJob<T>& J = *X.J;
+    const int m = X.m, n = X.n, cta = X.cta, nt = blockDim.x, t = threadIdx.x;
+    const int lane = t & 31, warp = t >> 5, nw = (nt + 31) >> 5;
+    double* __restrict__ U = J.U;
+    __shared__ int wmap[32][S];
+    __shared__ int cmap[S]; // this CTA's composed map, read by the later CTAs of the cluster
+    // the spare wavefunction buffer holds the per-point codes; remote CTAs may still gather from
+    // it until every CTA has left the step
+    if constexpr (C > 1) cg::this_cluster().sync();
+    signed char* code = reinterpret_cast<signed char*>(X.spare);
+    auto pos = [&](int x) { return (size_t)(x % C) * m + x / C; };
+    const int chunk = (m + nt - 1) / nt;
+    const int x0 = cta * m + min(m, t * chunk), x1 = cta * m + min(m, (t + 1) * chunk);
+    int tm[S];
+#pragma unroll
+    for (int jc = 0; jc < S; ++jc) {
+        int f = 0;
+        for (int x = x0; x < x1; ++x) {
+            int cd = 2; // s_0 = +1
+            if (x > 0) {
+                double ov = 0;
+                for (int k = 0; k < S; ++k)
+                    ov = __dadd_rn(ov, __dmul_rn(U[(size_t)(k * S + jc) * n + pos(x)], U[(size_t)(k * S + jc) * n + pos(x - 1)]));
+                cd = ov > 0 ? 0 : (ov < 0 ? 1 : 2);
+            }
+            code[(size_t)(x - cta * m) * S + jc] = (signed char)cd;
+            f = map_after(cd, f);
+        }
+        // inclusive scan over the warp's lanes (later lanes apply after earlier ones)
+        int inc = f;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, inc, off);
+            if (lane >= off) inc = map_after(inc, o);
+        }
+        const int exc = __shfl_up_sync(0xffffffffu, inc, 1);
+        tm[jc] = lane ? exc : 0;
+        if (lane == 31) wmap[warp][jc] = inc;
+    }
+    __syncthreads();
+    if (t < S) { // exclusive scan over the warps; the CTA's own composed map
+        int acc = 0;
+        for (int w = 0; w < nw; ++w) {
+            const int wm = wmap[w][t];
+            wmap[w][t] = acc;
+            acc = map_after(wm, acc);
+        }
+        cmap[t] = acc;
+    }
+    if constexpr (C > 1) cg::this_cluster().sync();
+    else __syncthreads();
+    Acc tot[S];
+#pragma unroll
+    for (int jc = 0; jc < S; ++jc) {
+        int entry = 0; // the earlier CTAs' maps, in order
+        if constexpr (C > 1)
+            for (int c = 0; c < cta; ++c) entry = map_after(*cg::this_cluster().map_shared_rank(&cmap[jc], c), entry);
+        int f = map_after(tm[jc], map_after(wmap[warp][jc], entry));
+        for (int x = x0; x < x1; ++x) {
+            f = map_after(code[(size_t)(x - cta * m) * S + jc], f);
+            const double d = J.sgn[(size_t)jc * n + x];
+            tot[jc].add((f & 1) ? -d : d);
+        }
+        tm[jc] = map_after(tm[jc], map_after(wmap[warp][jc], entry)); // the sign map entering this thread's run
+    }
+    double g[S];
+    cluster_sum<S, C>(tot, g, X.rs);
+#pragma unroll
+    for (int jc = 0; jc < S; ++jc) {
+        const int gneg = g[jc] < 0 ? 1 : 0;
+        int f = tm[jc];
+        for (int x = x0; x < x1; ++x) {
+            f = map_after(code[(size_t)(x - cta * m) * S + jc], f);
+            if ((f & 1) ^ gneg)
+                for (int k = 0; k < S; ++k) {
+                    double* u = &U[(size_t)(k * S + jc) * n + pos(x)];
+                    *u = -*u;
+                }
+        }
+    }
+    __threadfence();
+    if constexpr (C > 1) cg::this_cluster().sync(); // every CTA reads U at its own points next
+    else __syncthreads();
+}
+
 // time-dependent Hamiltonian.update (wavepacket.zig:137-143) and, with_R,
 // Propagator.update into the shared-memory R table
 template <typename T, int S, int C>
 __device__ __noinline__ void line_ham_update(const LineCtx<T>& X, double t, bool with_R, Tab<T>* Rs, int rstride,
                                              double lo, double span) {
     const LineJob<T>& J = *X.J;
+    const bool track = S > 1 && J.sign_track;
     for (int j = threadIdx.x; j < X.m; j += blockDim.x) {
         const double r = grid_r<C>(lo, span, X.n, X.cta, j);
+        const size_t idx = X.base + j;
+        double Uold[S * S];
+        if (track)
+            for (int e = 0; e < S * S; ++e) Uold[e] = J.U[(size_t)e * X.n + idx];
         td_point_update<T, S>(J.pot, r, t, with_R, J.dt_re, J.dt_im, with_R ? capdecay(J, r) : 1.0, J.V, J.U,
-                              (size_t)X.n, X.base + j, Rs, (size_t)rstride, (size_t)j);
+                              (size_t)X.n, idx, Rs, (size_t)rstride, (size_t)j);
+        if (track) { // overlap of every new (raw) eigenvector with the previous one at this point
+            const int x = X.cta + C * j;
+            for (int jc = 0; jc < S; ++jc) {
+                double d = 0;
+                for (int k = 0; k < S; ++k)
+                    d = __dadd_rn(d, __dmul_rn(J.U[(size_t)(k * S + jc) * X.n + idx], Uold[k * S + jc]));
+                J.sgn[(size_t)jc * X.n + x] = d;
+            }
+        }
     }
     __syncthreads();
+    if constexpr (S > 1)
+        if (track) line_sign_align<T, S, C>(X);
 }
 
 // setGaussian (wavepacket.zig:355-371), toDia (:398-419), autocorrelation reference
@@ -721,17 +836,32 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
     __syncthreads();
 
     LineCtx<T> ctx{&J, X.cur, nullptr, &rs, m, n, X.logm, X.q, X.ldp, cta, X.base};
-    line_initial_state<T, S, C>(ctx, X.lo, X.span);
+    auto spare_of = [&](cx<T>* c) { return c == X.bufA ? X.bufB : X.bufA; };
+    if (J.i0 == 0) {
+        line_initial_state<T, S, C>(ctx, X.lo, X.span);
+    } else { // resume: the wavefunction and the absorbed populations of the previous launch
+        for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
+            const int s = e / m, j = e - s * m;
+            X.cur[s * X.ldp + padx<T>(j)] = J.psi_save[(size_t)s * n + X.base + j];
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) X.pop_abs[s] = J.carry[s];
+        __syncthreads();
+    }
     constexpr int HC = RowLayout{1, S}.width();
     const int iters = J.iters;
-    int rows = iters + 1;
-    for (int i = 0; i <= iters; ++i) {
+    int rows = J.i1 + 1;
+    bool ended = J.i1 >= iters;
+    for (int i = J.i0; i <= J.i1; ++i) {
         const bool logstep = J.log && ((i % J.log_interval == 0) || (i == iters));
         X.set_flags(J.wmask | (logstep ? (uint32_t)WM_ALL_OBS : 0u));
         X.zero_acc();
         X.fuse_obs = i > 0 && !J.itp && !J.td;
         if (i > 0) { // Propagator.step (quantum_dynamics.zig:417-427)
-            if (J.td) line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.rstride, X.lo, X.span);
+            if (J.td) {
+                ctx.spare = spare_of(X.cur);
+                line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.rstride, X.lo, X.span);
+            }
             X.prop = true;
             X.inverse(X.forward());
             ctx.psi = X.cur;
@@ -740,7 +870,10 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
             line_orthogonalize<T, S, C>(ctx);
             line_normalize<T, S, C>(ctx);
         }
-        if (J.td) line_ham_update<T, S, C>(ctx, (double)i * J.tstep, false, Rs, X.rstride, X.lo, X.span);
+        if (J.td) {
+            ctx.spare = spare_of(X.cur);
+            line_ham_update<T, S, C>(ctx, (double)i * J.tstep, false, Rs, X.rstride, X.lo, X.span);
+        }
         if (!X.fuse_obs) X.observe_x();
         if (X.f.mom || X.f.ekin) {
             X.roundtrip();
@@ -773,16 +906,24 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
         }
         if (J.has_stop && nrm < J.stop_norm) { // stop_norm (quantum_dynamics.zig:933-944)
             rows = i + 1;
+            ended = true;
             break;
         }
     }
-    // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
-    X.set_flags(WM_ALL_OBS);
-    X.zero_acc();
-    X.observe_x();
-    X.roundtrip();
-    X.finish_row(J.fin);
-    if (cta == 0 && threadIdx.x == 0) *J.rows = rows;
+    if (ended) { // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
+        X.set_flags(WM_ALL_OBS);
+        X.zero_acc();
+        X.observe_x();
+        X.roundtrip();
+        X.finish_row(J.fin);
+    } else if (cta == 0 && threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) J.carry[s] = X.pop_abs[s];
+    }
+    if (cta == 0 && threadIdx.x == 0) {
+        *J.rows = rows;
+        if (J.done) *J.done = ended ? 1 : 0;
+    }
     for (int e = threadIdx.x; e < S * m; e += blockDim.x) {
         const int s = e / m, j = e - s * m;
         J.psi_save[(size_t)s * n + X.base + j] = X.cur[s * X.ldp + padx<T>(j)];

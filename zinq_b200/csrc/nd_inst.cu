@@ -1,6 +1,6 @@
 // nd_inst.cu -- the 2-D / 3-D driver for one (precision, state count) pair.
 // Compiled once per pair with -DZQD_T=<double|float> -DZQD_S=<1..4>
-// -DZQD_ND_CREATE=<symbol> -DZQD_ND_RUN=<symbol>.
+// -DZQD_ND_CREATE=<symbol> -DZQD_ND_RUN=<symbol> -DZQD_ND_STEP=<symbol>.
 //
 // A solve (src/quantum_dynamics.zig:860-950) is a stream-ordered sequence of
 // axis passes (nd_kernels.cuh); nothing returns to the host until the end.
@@ -11,8 +11,8 @@
 #include "job.h"
 #include "nd_kernels.cuh"
 
-#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_ND_CREATE) || !defined(ZQD_ND_RUN)
-#error "nd_inst.cu needs -DZQD_T, -DZQD_S, -DZQD_ND_CREATE and -DZQD_ND_RUN"
+#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_ND_CREATE) || !defined(ZQD_ND_RUN) || !defined(ZQD_ND_STEP)
+#error "nd_inst.cu needs -DZQD_T, -DZQD_S, -DZQD_ND_CREATE, -DZQD_ND_RUN and -DZQD_ND_STEP"
 #endif
 
 namespace zqd {
@@ -126,6 +126,23 @@ struct Launch {
         return ZQD_OK;
     }
     double* scal() const { return J->book.as<NdBook>()->scal; }
+    // Hamiltonian.update at time t (with_R: and Propagator.update); with sign tracking, the global
+    // eigenvector alignment with the previous update follows (wavepacket.zig:157-167)
+    int table(double t, int with_R) {
+        if (!needs_sign_tracking(J->o, S, J->nsolve)) {
+            nd_table_kernel<T, S><<<(unsigned)((J->N + 127) / 128), 128, 0, J->stream>>>(D, t, with_R);
+            ZQD_CUDA(cudaGetLastError());
+            return ZQD_OK;
+        }
+        const unsigned nb = (unsigned)std::min<size_t>(ngrid, (J->N + 127) / 128);
+        nd_table_sign_kernel<T, S><<<nb, 128, 0, J->stream>>>(D, t, with_R, G);
+        ZQD_CUDA(cudaGetLastError());
+        int rc = reduce(G, G + nb, S);
+        if (rc) return rc;
+        nd_sign_flip_kernel<S><<<(unsigned)ngrid, 256, 0, J->stream>>>(D.U, J->N, scal(), D.stopped);
+        ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
     // scalar sums of slots [0, nv) over partial blocks [b0, b1) into scal()
     int reduce(size_t b0, size_t b1, int nv) {
         nd_reduce_kernel<<<1, 32 * nv, 0, J->stream>>>(D.part, D.nparts, b0, b1, nv, D.stopped, scal());
@@ -172,6 +189,22 @@ int ZQD_ND_CREATE(zqd_job* J) {
     if (nd_smem_bytes<T>(2, Tn, n) > (size_t)budget || Tn * n / 8 > max_items)
         return fail(ZQD_ERR_UNSUPPORTED, "GRID LINE TOO LONG FOR THE TILE PASS");
     J->nd_tile = Tn;
+    ShapeOverride ov; // autotuned shape (or a candidate the autotuner measures), within the same limits
+    if (lookup_shape(J->d, n, S, J->fp32, ov)) {
+        if (ov.rows) {
+            if ((size_t)ov.rows > N / n || (N / n) % (size_t)ov.rows || S * ov.rows * n / 8 > max_items ||
+                nd_smem_bytes<T>(J->nd_row_bufs, S * ov.rows, n) > (size_t)budget)
+                return fail(ZQD_ERR_UNSUPPORTED, "ROW-PASS SHAPE OUTSIDE THE KERNEL'S LIMITS");
+            J->nd_rows = L = ov.rows;
+            J->nd_row_threads = std::max(32, (S * L * n / 8 + 31) / 32 * 32);
+        }
+        if (ov.tile) {
+            if (ov.tile > n || (N / n) % (size_t)ov.tile || ov.tile * n / 8 > max_items ||
+                nd_smem_bytes<T>(2, ov.tile, n) > (size_t)budget)
+                return fail(ZQD_ERR_UNSUPPORTED, "TILE-PASS SHAPE OUTSIDE THE KERNEL'S LIMITS");
+            J->nd_tile = Tn = ov.tile;
+        }
+    }
     J->nd_tile_threads = std::max(32, (Tn * n / 8 + 31) / 32 * 32);
     const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
     const size_t nparts = 3 * nrow_blocks + S * ntile_blocks + 1024;
@@ -229,118 +262,175 @@ int ZQD_ND_CREATE(zqd_job* J) {
 }
 
 namespace {
-// every launch of a run, in stream order (captured into a graph by ZQD_ND_RUN)
-int enqueue(zqd_job* J) {
-    const Opts& o = J->o;
-    Launch Lc{J, describe(J)};
-    const size_t N = J->N;
-    Lc.nrow_blocks = N / J->n / J->nd_rows;
-    Lc.ntile_blocks = N / J->n / J->nd_tile;
-    Lc.ngrid = std::min<size_t>(1024, (N + 255) / 256);
-    Lc.R0 = 0;
-    Lc.R1 = Lc.nrow_blocks;
-    Lc.R2 = 2 * Lc.nrow_blocks;
-    Lc.K = 3 * Lc.nrow_blocks;
-    Lc.G = Lc.K + S * Lc.ntile_blocks;
-    const bool split = o.imag_nstate > 0 || o.pot_td || (o.has_cap && o.cap_has_stop);
-    const bool acf = o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF);
-    const int iters = (int)o.iterations, HC = J->hc;
-    const size_t SN = (size_t)S * N * sizeof(cx<T>);
-    const unsigned ng = (unsigned)Lc.ngrid;
-    int rc;
-    for (int s = 0; s < J->nsolve; ++s) {
+// The launches of a run, in stream order, in three pieces per solve: the prologue (setGaussian,
+// normalise, toDia), the launches of loop index i (step i, then the observables of row i) and the
+// epilogue (final observables, orthw.append).  A whole run (enqueue) is every piece in order; a
+// step range (ZQD_ND_STEP) is a run of consecutive loop indices.
+struct Seq {
+    zqd_job* J;
+    Launch Lc;
+    bool split, acf;
+    int iters, HC;
+    size_t SN;
+    unsigned ng;
+
+    explicit Seq(zqd_job* j) : J(j), Lc{j, describe(j)} {
+        const Opts& o = J->o;
+        const size_t N = J->N;
+        Lc.nrow_blocks = N / J->n / J->nd_rows;
+        Lc.ntile_blocks = N / J->n / J->nd_tile;
+        Lc.ngrid = std::min<size_t>(1024, (N + 255) / 256);
+        Lc.R0 = 0;
+        Lc.R1 = Lc.nrow_blocks;
+        Lc.R2 = 2 * Lc.nrow_blocks;
+        Lc.K = 3 * Lc.nrow_blocks;
+        Lc.G = Lc.K + S * Lc.ntile_blocks;
+        split = o.imag_nstate > 0 || o.pot_td || (o.has_cap && o.cap_has_stop);
+        acf = o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF);
+        iters = (int)o.iterations;
+        HC = J->hc;
+        SN = (size_t)S * N * sizeof(cx<T>);
+        ng = (unsigned)Lc.ngrid;
         Lc.D.orth = J->orth.as<cx<T>>();
-        double* hist = J->hist.as<double>() + (size_t)s * (iters + 1) * HC;
-        int* rows_out = J->rows.as<int>() + s;
+    }
+    double* hist(int s) const { return J->hist.as<double>() + (size_t)s * (iters + 1) * HC; }
+    int* rows_out(int s) const { return J->rows.as<int>() + s; }
+    // this solve's wavefunction history entry of step i (write.wavefunction), or null
+    cx<T>* whist(int s, int i) const {
+        return J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + ((size_t)s * (iters + 1) + i) * S * J->N : nullptr;
+    }
+    // finalize descriptors, run by the last CTA of the launch that ends a step
+    NdFin fin(int s, int kind, size_t x0, size_t x1, bool k, uint32_t mask, double* row, int i) const {
+        const Opts& o = J->o;
+        NdFin f{};
+        f.row = row;
+        f.rows_out = rows_out(s);
+        f.book = J->book.as<NdBook>();
+        f.x0 = x0;
+        f.x1 = x1;
+        f.k0 = Lc.K;
+        f.k1 = k ? Lc.K + S * Lc.ntile_blocks : Lc.K;
+        f.stop_norm = o.cap_stop_norm;
+        f.mask = mask;
+        f.row_index = i;
+        f.kind = kind;
+        f.has_stop = kind == 0 && o.has_cap && o.cap_has_stop;
+        f.enabled = 1;
+        return f;
+    }
+    int itp_ops(int s) { // quantum_dynamics.zig:898-906
+        int rc;
+        for (int j = 0; j < s; ++j) {
+            nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G);
+            if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 2))) return rc;
+            nd_orth_apply_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.scal());
+        }
+        nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, -1, Lc.G);
+        if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc;
+        nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), 0, 0);
+        ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
+    int prologue(int s) {
+        const Opts& o = J->o;
         ZQD_CUDA(cudaMemsetAsync(J->flags.p, 0, 2 * sizeof(int), J->stream));
         ZQD_CUDA(cudaMemsetAsync(J->book.p, 0, sizeof(NdBook), J->stream));
+        if (s == 0 && o.pot_td) { // a later run starts again from the t = 0 tables (Hamiltonian.init, Propagator.init)
+            nd_table_kernel<T, S><<<(unsigned)((J->N + 127) / 128), 128, 0, J->stream>>>(Lc.D, 0.0, 1);
+            ZQD_CUDA(cudaGetLastError());
+        }
         // setGaussian, normalise, toDia, acf reference (quantum_dynamics.zig:867-882)
         nd_gauss_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.G);
         ZQD_CUDA(cudaGetLastError());
-        if ((rc = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc;
+        if (int rc = Lc.reduce(Lc.G, Lc.G + ng, 1)) return rc;
         nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), o.ic_adiabatic ? 1 : 0, acf ? 1 : 0);
         ZQD_CUDA(cudaGetLastError());
-        // this solve's wavefunction history entry of step i (write.wavefunction), or null
-        auto whist = [&](int i) -> cx<T>* {
-            return J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + ((size_t)s * (iters + 1) + i) * S * N : nullptr;
-        };
-        // finalize descriptors, run by the last CTA of the launch that ends a step
-        auto fin = [&](int kind, size_t x0, size_t x1, bool k, uint32_t mask, double* row, int i) {
-            NdFin f{};
-            f.row = row;
-            f.rows_out = rows_out;
-            f.book = J->book.as<NdBook>();
-            f.x0 = x0;
-            f.x1 = x1;
-            f.k0 = Lc.K;
-            f.k1 = k ? Lc.K + S * Lc.ntile_blocks : Lc.K;
-            f.stop_norm = o.cap_stop_norm;
-            f.mask = mask;
-            f.row_index = i;
-            f.kind = kind;
-            f.has_stop = kind == 0 && o.has_cap && o.cap_has_stop;
-            f.enabled = 1;
-            return f;
-        };
-        auto itp_ops = [&]() -> int { // quantum_dynamics.zig:898-906
-            int rc2;
-            for (int j = 0; j < s; ++j) {
-                nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.G);
-                if ((rc2 = Lc.reduce(Lc.G, Lc.G + ng, 2))) return rc2;
-                nd_orth_apply_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, j, Lc.scal());
-            }
-            nd_dot_kernel<T><<<ng, 256, 0, J->stream>>>(Lc.D, -1, Lc.G);
-            if ((rc2 = Lc.reduce(Lc.G, Lc.G + ng, 1))) return rc2;
-            nd_normalize_kernel<T, S><<<ng, 256, 0, J->stream>>>(Lc.D, Lc.scal(), 0, 0);
-            ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
+    int step(int s, int i) {
+        const Opts& o = J->o;
+        int rc;
+        const bool logstep = o.log && ((i % o.log_interval == 0) || (i == iters));
+        const uint32_t mask = o.write_mask | (logstep ? (uint32_t)WM_ALL_OBS : 0u) | (acf ? (uint32_t)WM_ACF : 0u);
+        const bool needk = mask & (WM_MOM | WM_EKIN | WM_ETOT);
+        const uint32_t obs = mask | ((o.has_cap && o.cap_has_stop) ? (uint32_t)WM_NORM : 0u);
+        double* row = hist(s) + (size_t)i * HC;
+        if (i > 0 && (rc = Lc.step_tiles())) return rc;
+        if (!split) {
+            uint32_t mode = RM_OBS | RM_STORE | (needk ? RM_PHI : 0u);
+            if (i > 0) mode |= RM_INV | RM_REND;
+            if (i < iters) mode |= RM_RSTART | RM_FWD;
+            const NdFin f = fin(s, 0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, row, i);
+            if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
+            if (needk && (rc = Lc.kobs(false, f))) return rc;
             return ZQD_OK;
-        };
-        for (int i = 0; i <= iters; ++i) {
-            const bool logstep = o.log && ((i % o.log_interval == 0) || (i == iters));
-            const uint32_t mask = o.write_mask | (logstep ? (uint32_t)WM_ALL_OBS : 0u) | (acf ? (uint32_t)WM_ACF : 0u);
-            const bool needk = mask & (WM_MOM | WM_EKIN | WM_ETOT);
-            const uint32_t obs = mask | ((o.has_cap && o.cap_has_stop) ? (uint32_t)WM_NORM : 0u);
-            if (i > 0 && (rc = Lc.step_tiles())) return rc;
-            if (!split) {
-                uint32_t mode = RM_OBS | RM_STORE | (needk ? RM_PHI : 0u);
-                if (i > 0) mode |= RM_INV | RM_REND;
-                if (i < iters) mode |= RM_RSTART | RM_FWD;
-                const NdFin f = fin(0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
-                if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f, whist(i)))) return rc;
-                if (needk && (rc = Lc.kobs(false, f))) return rc;
-            } else {
-                if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
-                if (o.imag_nstate && (rc = itp_ops())) return rc; // every i, the initial state included
-                if (o.pot_td) {
-                    nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, (double)i * o.time_step, 0);
-                    ZQD_CUDA(cudaGetLastError());
-                }
-                // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
-                const NdFin f = fin(0, i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, hist + (size_t)i * HC, i);
-                if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f, whist(i)))) return rc;
-                if (needk && (rc = Lc.kobs(false, f))) return rc;
-                if (i < iters) {
-                    if (o.pot_td) {
-                        nd_table_kernel<T, S><<<(unsigned)((N + 127) / 128), 128, 0, J->stream>>>(Lc.D, ((double)i + 0.5) * o.time_step, 1);
-                        ZQD_CUDA(cudaGetLastError());
-                    }
-                    // the absorbed sums of step i+1's first accumAbsorbed
-                    const NdFin fc = fin(2, Lc.R2, Lc.R2 + Lc.nrow_blocks, false, 0, nullptr, 0);
-                    if ((rc = Lc.row(RM_RSTART | RM_FWD | RM_STORE, 0, Lc.R2, false, fc))) return rc;
-                }
-            }
         }
+        if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
+        if (o.imag_nstate && (rc = itp_ops(s))) return rc; // every i, the initial state included
+        if (o.pot_td && (rc = Lc.table((double)i * o.time_step, 0))) return rc;
+        // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
+        const NdFin f = fin(s, 0, i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, row, i);
+        if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
+        if (needk && (rc = Lc.kobs(false, f))) return rc;
+        if (i < iters) {
+            if (o.pot_td && (rc = Lc.table(((double)i + 0.5) * o.time_step, 1))) return rc;
+            // the absorbed sums of step i+1's first accumAbsorbed
+            const NdFin fc = fin(s, 2, Lc.R2, Lc.R2 + Lc.nrow_blocks, false, 0, nullptr, 0);
+            if ((rc = Lc.row(RM_RSTART | RM_FWD | RM_STORE, 0, Lc.R2, false, fc))) return rc;
+        }
+        return ZQD_OK;
+    }
+    int epilogue(int s) {
+        int rc;
         // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
         const uint32_t all = WM_ALL_OBS | (acf ? (uint32_t)WM_ACF : 0u);
         if ((rc = Lc.row(RM_OBS | RM_PHI, all, Lc.R1, true))) return rc;
-        if ((rc = Lc.kobs(true, fin(1, Lc.R1, Lc.R1 + Lc.nrow_blocks, true, all, J->fin.as<double>() + (size_t)s * HC, 0))))
+        if ((rc = Lc.kobs(true, fin(s, 1, Lc.R1, Lc.R1 + Lc.nrow_blocks, true, all, J->fin.as<double>() + (size_t)s * HC, 0))))
             return rc;
         if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)
             ZQD_CUDA(cudaMemcpyAsync(J->orth.as<char>() + (size_t)s * SN, J->psi_save.p, SN, cudaMemcpyDeviceToDevice, J->stream));
+        return ZQD_OK;
+    }
+};
+
+// every launch of a run, in stream order (captured into a graph by ZQD_ND_RUN)
+int enqueue(zqd_job* J) {
+    Seq q(J);
+    int rc;
+    for (int s = 0; s < J->nsolve; ++s) {
+        if ((rc = q.prologue(s))) return rc;
+        for (int i = 0; i <= q.iters; ++i)
+            if ((rc = q.step(s, i))) return rc;
+        if ((rc = q.epilogue(s))) return rc;
     }
     return ZQD_OK;
 }
 } // namespace
+
+// Rows i0..i1 of solve s (zqd_job_step), launched directly; then, if the solve ended (its last
+// step, or stop_norm), its final observables.  *rows: rows of the solve's history written so far.
+int ZQD_ND_STEP(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
+    Seq q(J);
+    int rc;
+    ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
+    if (i0 == 0 && (rc = q.prologue(s))) return rc;
+    for (int i = i0; i <= i1; ++i)
+        if ((rc = q.step(s, i))) return rc;
+    int flags[2] = {0, 0}; // stopped, rows
+    ZQD_CUDA(cudaMemcpyAsync(&flags[0], J->flags.p, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaMemcpyAsync(&flags[1], q.rows_out(s), sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->d2h += sizeof(flags);
+    *rows = flags[1];
+    *ended = flags[0] || i1 >= q.iters;
+    if (*ended && (rc = q.epilogue(s))) return rc;
+    ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    float ms = 0;
+    ZQD_CUDA(cudaEventElapsedTime(&ms, J->ev0, J->ev1));
+    J->last_ms += ms;
+    return ZQD_OK;
+}
 
 // A run is a fixed sequence of launches: it is captured into a CUDA graph on the
 // first call and the graph is replayed by every later call on the job.

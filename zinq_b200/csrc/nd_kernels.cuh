@@ -277,7 +277,7 @@ static __global__ void nd_reduce_kernel(const double* __restrict__ part, size_t 
 struct NdBook {
     double pop_abs[4];
     double carry[4];  // absorbed sums of the next step's first accumAbsorbed
-    double scal[2];   // reduced sums for the imaginary-time kernels
+    double scal[4];   // reduced sums for the imaginary-time kernels and the eigenvector alignment
     unsigned counter; // CTAs of the current launch that have written their partials
 };
 
@@ -981,13 +981,13 @@ template <typename T> __global__ void nd_kphase_kernel(const __grid_constant__ N
 // ------------------------------------------------------------ setup, imaginary time, bookkeeping
 // V(r, t), eigh, R (with_R) and cap weights at every grid point (wavepacket.zig:96-168,
 // quantum_dynamics.zig:387-468); no sign continuity in more than one dimension
-template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double t, int with_R) {
-    if (*J.stopped) return;
-    const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (g >= J.N) return;
+// Hamiltonian.update (wavepacket.zig:137-143) and, with_R, Propagator.update (quantum_dynamics.zig:430-468)
+// at grid point g; the new eigenvectors are left in Ul.
+template <typename T, int S>
+__device__ __forceinline__ void nd_table_point(const NdJob<T>& J, size_t g, double t, int with_R, double (&Ul)[S * S]) {
     double r[3];
     grid_coords(J, g, r);
-    double Vl[S * S], Vu[S * S], Wl[S], Ul[S * S];
+    double Vl[S * S], Vu[S * S], Wl[S];
     pot_eval(J.pot, r, t, Vl);
     for (int a = 0; a < S; ++a)
         for (int b = 0; b < S; ++b) Vu[a * S + b] = Vl[(a < b ? a : b) * S + (a < b ? b : a)];
@@ -1012,6 +1012,51 @@ template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double 
             J.R[(size_t)k * J.N + g] = mktab<T>(re, im);
             ++k;
         }
+}
+
+template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double t, int with_R) {
+    if (*J.stopped) return;
+    const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (g >= J.N) return;
+    double Ul[S * S];
+    nd_table_point<T, S>(J, g, t, with_R, Ul);
+}
+
+// The same update for a time-dependent potential whose eigenvector signs are observed: per
+// eigenvector j the partial sums of sum_k U_new[k][j] U_prev[k][j] over the grid (the global
+// alignment with the previous update, wavepacket.zig:157-167), grid-stride over <= 1024 blocks of
+// at most 16 warps.  nd_sign_flip_kernel applies the decision after the sums are reduced.
+template <typename T, int S> __global__ void nd_table_sign_kernel(NdJob<T> J, double t, int with_R, size_t part_base) {
+    if (*J.stopped) return;
+    double acc[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) acc[j] = 0.0;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
+        double Uold[S * S], Ul[S * S];
+        for (int e = 0; e < S * S; ++e) Uold[e] = J.U[(size_t)e * J.N + g];
+        nd_table_point<T, S>(J, g, t, with_R, Ul);
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            double d = 0;
+            for (int k = 0; k < S; ++k) d = __dadd_rn(d, __dmul_rn(Ul[k * S + j], Uold[k * S + j]));
+            acc[j] += d;
+        }
+    }
+    block_partials<S>(acc, 0, J.part, J.nparts, part_base + blockIdx.x);
+}
+
+// U[:, j] <- -U[:, j] at every point for the eigenvectors whose total overlap with the previous
+// update's is negative (tot[j] < 0)
+template <int S> __global__ void nd_sign_flip_kernel(double* __restrict__ U, size_t N, const double* __restrict__ tot,
+                                                     const int* stopped) {
+    if (*stopped) return;
+    bool any = false;
+    for (int j = 0; j < S; ++j) any |= tot[j] < 0;
+    if (!any) return;
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < N; g += (size_t)gridDim.x * blockDim.x)
+        for (int j = 0; j < S; ++j)
+            if (tot[j] < 0)
+                for (int k = 0; k < S; ++k) U[(size_t)(k * S + j) * N + g] = -U[(size_t)(k * S + j) * N + g];
 }
 
 // setGaussian (wavepacket.zig:355-371) and the partial norms

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <unordered_map>
 
@@ -187,7 +188,25 @@ int validate(const Opts& o) {
     return ZQD_OK;
 }
 
+// Host-side fault injection (zqd_testing_fail_device_allocations): after g_alloc_skip more
+// successful device allocations, the next g_alloc_fail ones report cudaErrorMemoryAllocation.
+static std::atomic<long long> g_alloc_skip{-1}, g_alloc_fail{0};
+
+static bool injected_alloc_failure() {
+    if (g_alloc_skip.load(std::memory_order_relaxed) < 0) return false;
+    if (g_alloc_skip.fetch_sub(1) > 0) return false;
+    g_alloc_skip.store(0);
+    if (g_alloc_fail.fetch_sub(1) > 0) return true;
+    g_alloc_skip.store(-1); // disarmed
+    g_alloc_fail.store(0);
+    return false;
+}
+
 cudaError_t dev_alloc(void** p, size_t bytes) {
+    if (injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
     static std::mutex mu;
     static bool configured[64] = {};
     int dev = 0;
@@ -211,6 +230,22 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
 
 void dev_free(void* p) {
     if (p) cudaFreeAsync(p, cudaStreamPerThread);
+}
+
+size_t device_free_bytes() {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int dev = 0;
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+        free_b += (size_t)(reserved - used); // blocks the pool keeps for reuse
+    return free_b;
 }
 
 PotStore::~PotStore() { dev_free(d_blob); }
@@ -367,6 +402,7 @@ extern "C" const char* zqd_status_string(int status) {
     case ZQD_ERR_CANCELLED: return "cancelled";
     case ZQD_ERR_NOT_FOUND: return "not found";
     case ZQD_ERR_NO_DEVICE: return "no CUDA device";
+    case ZQD_ERR_NUMERIC: return "non-finite observable";
     default: return "unknown status";
     }
 }
@@ -392,4 +428,9 @@ extern "C" void zqd_potential_init(zqd_potential* p, zqd_potential_kind kind) {
     case ZQD_POT_TULLY_3: p->p[0] = 6.0e-4; p->p[1] = 0.10; p->p[2] = 0.90; break;
     default: break;
     }
+}
+
+extern "C" void zqd_testing_fail_device_allocations(uint64_t after, uint64_t count) {
+    zqd::g_alloc_fail.store((long long)count);
+    zqd::g_alloc_skip.store(count ? (long long)after : -1);
 }

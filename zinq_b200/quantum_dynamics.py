@@ -313,6 +313,28 @@ class Job:
         check(self._L.zqd_job_run(self._h))
         return self._L.zqd_job_device_ms(self._h)
 
+    def step(self, nsteps: int) -> None:
+        """zqd_job_step: propagate up to nsteps more steps (the first call also records row 0)."""
+        check(self._L.zqd_job_step(self._h, int(nsteps)))
+
+    def progress(self):
+        """(solve in progress, rows recorded in it, every solve finished)"""
+        s, r, f = C.c_uint32(), C.c_uint32(), C.c_int()
+        check(self._L.zqd_job_progress(self._h, C.byref(s), C.byref(r), C.byref(f)))
+        return s.value, r.value, bool(f.value)
+
+    def observables(self):
+        """Rows recorded since the last call: a list of (solve, first_row, rows[nrows, width]), one
+        entry per solve with new rows (zqd_job_observables until it returns none)."""
+        out = []
+        while True:
+            r = _abi.ZqdObsRows()
+            check(self._L.zqd_job_observables(self._h, C.byref(r)))
+            if r.nrows == 0:
+                return out
+            a = np.ctypeslib.as_array(r.rows, shape=(r.nrows * r.width,)).copy().reshape(r.nrows, r.width)
+            out.append((r.solve, r.first_row, a))
+
     def result(self, want_wavefunction=True) -> Result:
         res = C.c_void_p()
         check(self._L.zqd_job_result(self._h, C.byref(res)))
@@ -426,11 +448,13 @@ class Server:
     """Request loop for streams of independent jobs (zqd_server_*): submit() returns a ticket at once,
     wait() returns (Result, latency in ms from submission to completion)."""
 
-    def __init__(self, workers: int = 4, max_batch: int = 16, device_budget_bytes: int = 0):
+    def __init__(self, workers: int = 4, max_batch: int = 16, device_budget_bytes: int = 0, stream_steps: int = 256,
+                 stream_rows: bool = True, max_events: int = 65536):
         self._L = _abi.load()
         cfg = _abi.ZqdServerConfig()
         self._L.zqd_server_config_init(C.byref(cfg))
         cfg.workers, cfg.max_batch, cfg.device_budget_bytes = workers, max_batch, device_budget_bytes
+        cfg.stream_steps, cfg.stream_rows, cfg.max_events = stream_steps, int(bool(stream_rows)), max_events
         self._h = C.c_void_p()
         check(self._L.zqd_server_create(C.byref(cfg), C.byref(self._h)))
         self._shapes = {}
@@ -442,10 +466,14 @@ class Server:
         self._shapes[t.value] = _shape(opt)
         return t.value
 
-    def wait(self, ticket: int, want_wavefunction: bool = False):
+    def wait(self, ticket: int, want_wavefunction: bool = False, timeout_ms: int | None = None):
+        """(Result, latency ms); with timeout_ms, ZqdError(ZQD_ERR_TIMEOUT) when not done in time."""
         res, lat = C.c_void_p(), C.c_double()
+        if timeout_ms is None:
+            check(self._L.zqd_server_wait(self._h, ticket, C.byref(res), C.byref(lat)))
+        else:
+            check(self._L.zqd_server_wait_timeout(self._h, ticket, int(timeout_ms), C.byref(res), C.byref(lat)))
         npt = self._shapes.pop(ticket, None)
-        check(self._L.zqd_server_wait(self._h, ticket, C.byref(res), C.byref(lat)))
         try:
             obs = _collect(res)
             if want_wavefunction and obs:
@@ -453,6 +481,25 @@ class Server:
             return _result(self._L, res, obs), lat.value
         finally:
             self._L.zqd_result_destroy(res)
+
+    def cancel(self, ticket: int) -> None:
+        check(self._L.zqd_server_cancel(self._h, ticket))
+
+    def poll(self, max_events: int = 1024) -> list:
+        """Pending events, oldest first: dicts with ticket, kind ("rows", "done", "failed",
+        "cancelled"), status, solve, first_row and, for row events, rows (nrows x width)."""
+        buf = (_abi.ZqdEvent * max_events)()
+        n = C.c_uint32()
+        check(self._L.zqd_server_poll(self._h, buf, max_events, C.byref(n)))
+        out = []
+        for e in buf[:n.value]:
+            d = {"ticket": e.ticket, "kind": _abi.EVENT[e.kind], "status": e.status, "solve": e.solve,
+                 "first_row": e.first_row, "solve_finished": bool(e.solve_finished)}
+            if e.kind == 0:
+                d["rows"] = (np.ctypeslib.as_array(e.rows, shape=(e.nrows * e.width,)).copy().reshape(e.nrows, e.width)
+                             if e.rows else np.zeros((e.nrows, e.width)))
+            out.append(d)
+        return out
 
     def stats(self) -> dict:
         s = _abi.ZqdServerStats()
@@ -556,6 +603,27 @@ def serving_stream(njobs: int, seed: int = 7, rate_per_s: float = 200.0, max_ste
                      "write": {"population": "P"}})
         arrivals.append(t)
     return opts, arrivals
+
+
+def autotune(ndim: int, npoint: int, nstate: int, precision: str = "fp64") -> dict:
+    """zqd_autotune: measure the launch shapes for a (dims, points, states, precision) key on this
+    device and record the fastest; returns the entry (0 fields: the built-in rules' shape won)."""
+    L = _abi.load()
+    e = _abi.ZqdTuneEntry(ndim=ndim, npoint=npoint, nstate=nstate, precision=_abi.PRECISION[precision])
+    check(L.zqd_autotune(C.byref(e)))
+    return {name: getattr(e, name) for name, _ in e._fields_}
+
+
+def tune_save(path: str) -> None:
+    check(_abi.load().zqd_tune_save(str(path).encode()))
+
+
+def tune_load(path: str) -> None:
+    check(_abi.load().zqd_tune_load(str(path).encode()))
+
+
+def tune_clear() -> None:
+    _abi.load().zqd_tune_clear()
 
 
 def potential_plot(opt: dict, write: bool = False) -> np.ndarray:
