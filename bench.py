@@ -19,7 +19,13 @@ Legs printed in one JSON line:
   nd         2-D 512^2 x 3 states, 3-D 128^3 (ITP and real time), 2-D 2048^2 x 2
              states (larger than L2): FP32 and FP64 device time, HBM roofline;
   serving    a seeded stream of 600 jobs (Poisson arrivals, 200 jobs/s) through
-             the job server: p50/p99 latency, throughput, FP32 vs FP64 error.
+             the job server: p50/p99 latency, throughput, burst throughput, FP32 vs
+             FP64 error, and the plain FP64 form on the same stream (each job alone
+             through zqd_run, one after another);
+  fp32_errors  per configuration, FP32 against FP64: wavefunction rel. L2,
+             largest population error, energy difference and drift;
+  fft_brackets cuFFT against the library's FFT seam on the device, pocketfft
+             (scipy.fft, every host thread) against the oracle's FFT on the host.
 `--impl reference` times the CPU restatement of the reference path (the
 oracle) with all host threads on the same workload.
 """
@@ -381,7 +387,8 @@ def serving_leg(qd):
                      "throughput": units / wall, "unit": UNIT, "wall_s": wall,
                      "burst_throughput": units / wall_b, "burst_wall_s": wall_b,
                      "grouped_launches": st["grouped_launches"], "grouped_jobs": st["grouped_jobs"],
-                     "peak_device_bytes": st["peak_device_bytes"]}
+                     "joined_jobs": st["joined_jobs"], "service_jobs": st["service_jobs"],
+                     "service_launches": st["service_launches"], "peak_device_bytes": st["peak_device_bytes"]}
         pops[prec] = [r.observables[0].history["population"] for r in res]
         forms[prec] = [r.precision for r in res]
     errs = [float(np.max(np.abs(a - b))) for a, b in zip(pops["fp32"], pops["fp64"])]
@@ -392,6 +399,19 @@ def serving_leg(qd):
     out["auto"]["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs_auto)
     out["auto"]["jobs_fp64"] = sum(f == "fp64" for f in forms["auto"])
     out["burst_fp32_over_fp64"] = out["fp32"]["burst_throughput"] / out["fp64"]["burst_throughput"]
+    # the plain FP64 form on the same stream: every job alone through zqd_run, one after another
+    t0 = time.perf_counter()
+    lat_plain = []
+    for o in opts:
+        t1 = time.perf_counter()
+        qd.run(o, precision="fp64", want_wavefunction=False)
+        lat_plain.append(1e3 * (time.perf_counter() - t1))
+    wall_plain = time.perf_counter() - t0
+    out["plain_fp64_sequential"] = {"throughput": units / wall_plain, "unit": UNIT, "wall_s": wall_plain,
+                                    "p50_job_ms": float(np.percentile(lat_plain, 50)),
+                                    "note": "each job alone through zqd_run (FP64), one after another"}
+    out["served_fp32_burst_over_plain_fp64"] = out["fp32"]["burst_throughput"] / out["plain_fp64_sequential"]["throughput"]
+    out["served_auto_burst_over_plain_fp64"] = out["auto"]["burst_throughput"] / out["plain_fp64_sequential"]["throughput"]
     return out
 
 
@@ -486,12 +506,63 @@ def fft_brackets(qd, torch, reps=20):
         pocket_ms = 1e3 * (time.perf_counter() - t0) / nrep
         t0 = time.perf_counter()
         for _ in range(nrep):
+            scipy.fft.ifftn(scipy.fft.fftn(hx, workers=1), workers=1)
+        pocket1_ms = 1e3 * (time.perf_counter() - t0) / nrep
+        t0 = time.perf_counter()
+        for _ in range(nrep):
             qd_ref.fft(qd_ref.fft(hx, -1), 1)
         port_ms = 1e3 * (time.perf_counter() - t0) / nrep
         out[name] = {"cufft_ms": cufft_ms, "zqd_fft_seam_ms": own_ms, "seam_over_cufft": own_ms / cufft_ms,
-                     "host_pocketfft_ms": pocket_ms, "host_oracle_fft_ms": port_ms,
-                     "oracle_fft_over_pocketfft": port_ms / pocket_ms}
+                     "host_pocketfft_ms": pocket_ms, "host_pocketfft_1thread_ms": pocket1_ms,
+                     "host_oracle_fft_ms": port_ms, "oracle_fft_over_pocketfft_1thread": port_ms / pocket1_ms}
     return out
+
+
+def line_step_model(n, S, C, lrmax, c):
+    """Shared-memory traffic and barriers of one step of the resident 1-D kernel, per CTA: local
+    Stockham passes of m = n/C points (largest radix 2^lrmax) forward and inverse, each reading and
+    writing S*m values; their twiddles (16-byte table entries, R-1 per R-point butterfly, from the
+    second pass on); the propagator R applied twice (upper triangle, 16-byte entries); the cluster
+    twiddles and kinetic phase; the exchange across the cluster (DSMEM reads and local writes).
+    Barriers: one per pass, three more per step in the CTA, three across the cluster."""
+    import math
+
+    m = n // C
+    logm = int(math.log2(m))
+    P = -(-logm // lrmax)
+    R = 2 ** lrmax
+    nsym = S * (S + 1) // 2
+    passes = 2 * P * 2 * S * m * c
+    twiddles = 2 * max(P - 1, 0) * (R - 1) / R * S * m * 16
+    rtab = 2 * nsym * m * 16
+    phases = (3 if C > 1 else 1) * m * 16
+    exchange = 3 * S * m * c if C > 1 else 0
+    return {"smem_bytes_per_cta": passes + twiddles + rtab + phases + exchange,
+            "cta_barriers": 2 * P + 3, "cluster_barriers": 3 if C > 1 else 0, "m": m, "passes_per_transform": P}
+
+
+def onchip_roofline(L, step_us, n, S, C, lrmax, c, ctas):
+    """roofline_onchip: the resident kernel's shared-memory bytes per step against the measured per-SM
+    shared-memory bandwidth, and its barrier-latency floor (barriers x measured latency) against the
+    measured step time.  Neither is a DRAM roof: the wavefunction never leaves shared memory."""
+    import ctypes as C_
+
+    from zinq_b200 import _abi
+
+    o = _abi.ZqdOnchip()
+    _abi.check(L.zqd_measure_onchip(C_.byref(o)))
+    mod = line_step_model(n, S, C, lrmax, c)
+    per_sm = mod["smem_bytes_per_cta"] / (step_us * 1e-6) / 1e9
+    floor_cycles = mod["cta_barriers"] * o.syncthreads_cycles + mod["cluster_barriers"] * o.cluster_barrier_cycles
+    floor_us = floor_cycles / (o.sm_clock_mhz)
+    return {"bound": "latency", "us_per_step": step_us, "ctas": ctas,
+            "smem": {"bytes_per_cta_per_step": mod["smem_bytes_per_cta"], "achieved_gbs_per_sm": per_sm,
+                     "peak_gbs_per_sm": o.smem_gbs_per_sm, "peak_bytes_per_cycle_per_sm": o.smem_bytes_per_cycle_per_sm,
+                     "frac": per_sm / o.smem_gbs_per_sm, "peak_kind": "measured (zqd_measure_onchip)"},
+            "barriers": {"cta_per_step": mod["cta_barriers"], "cluster_per_step": mod["cluster_barriers"],
+                         "syncthreads_cycles": o.syncthreads_cycles, "cluster_barrier_cycles": o.cluster_barrier_cycles,
+                         "floor_us_per_step": floor_us, "frac": floor_us / step_us},
+            "shape": {"npoint": n, "states": S, "cluster_ctas": C, "radix": 2 ** lrmax, "points_per_cta": mod["m"]}}
 
 
 def max_over_ranks(x, dist, device):
@@ -609,6 +680,8 @@ def main():
         barrier()
         return times
 
+    # the launch shapes of the workload's key, measured by the library's autotuner (outside the timed region)
+    tuned = {p: qd.autotune(1, NPOINT, NSTATE, p) for p in ("fp32", "fp64")}
     fp64 = qd.Batch(opts, "fp64")
     fp32 = qd.Batch(opts, "fp32")
     import tempfile
@@ -662,6 +735,14 @@ def main():
     achieved = BYTES_PER_UNIT["fp32"] * U / per_launch / 1e9
     traffic = read_traffic("line_solve_kernel", "fp32")
     lat = sorted(t32)
+
+    def shape_of(p):
+        e = tuned[p]
+        if e["cluster_ctas"]:
+            return e["cluster_ctas"], e["radix_log2"]
+        return 16, 2  # the built-in rules for 8192 points: 16 CTAs of 512 points, radix 4
+    C32, lr32 = shape_of("fp32")
+    onchip = onchip_roofline(_abi.load(), 1e6 * per_launch / ITERS, NPOINT, NSTATE, C32, lr32, 8, C32 * len(opts))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * s32 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -688,6 +769,9 @@ def main():
                              "binding roof: the resident kernel keeps psi in shared memory for the whole solve "
                              "(DRAM sees the tables once per job); see roofline_onchip"},
         "clocks": clocks,
+        "roofline_onchip": onchip,
+        "autotune": {p: {k: tuned[p][k] for k in ("cluster_ctas", "radix_log2", "us_per_step", "default_us_per_step",
+                                                  "candidates")} for p in tuned},
     }
     if not args.no_nd:
         line["nd"] = nd_legs(qd, torch, flush)

@@ -410,7 +410,13 @@ int zqd_potential_plot(const zqd_options* opt, double time, double* host_U, size
  * between launches finished or cancelled jobs leave and waiting requests of the
  * same shape join (continuous batching).  After every launch each job's new
  * observable rows are posted as an event; zqd_server_poll pulls events (nothing
- * is called back).  Results equal those of zqd_run on the same options.
+ * is called back).  1-D single-solve requests whose line fits one CTA run instead
+ * on the persistent line-service kernel: resident CTAs claim requests from a job
+ * table in pinned memory as they are posted, keep each wavefunction in shared
+ * memory for its whole solve and publish every observable row as it is written
+ * (a cancelled request there finishes its solve and is then reported cancelled).
+ * Results equal those of zqd_run on the same options, within the parity bars of
+ * the launch shape (bit for bit where the shapes agree).
  */
 typedef struct zqd_server zqd_server;
 typedef struct {
@@ -422,12 +428,18 @@ typedef struct {
     int stream_rows;              /* post ZQD_EVENT_ROWS events with the observable rows (default 1) */
     uint32_t max_events;          /* events kept for zqd_server_poll (default 65536); beyond it the oldest
                                      row events are dropped and counted, completion events never */
+    int persistent_lines;         /* 1-D single-solve requests whose line fits one CTA (npoint <= 2048 FP32,
+                                     1024 FP64) run on the persistent line-service kernel (default 1) */
+    uint32_t service_ctas;        /* CTAs alive per service table (default 64, 0: one per SM); a table
+                                     per (precision, states, CTA size): small lines share an SM */
+    double service_idle_us;       /* a service CTA without work exits after this wait (default 200) */
 } zqd_server_config;
 typedef struct {
     uint64_t submitted, completed, failed, cancelled, queued;
     uint64_t grouped_launches, grouped_jobs, joined_jobs; /* joined: admitted into a group already on the GPU */
     uint64_t device_budget_bytes, device_bytes_in_use, peak_device_bytes;
     uint64_t pending_events, dropped_events;
+    uint64_t service_jobs, service_launches; /* requests run by the persistent kernel; its launches */
 } zqd_server_stats;
 typedef enum {
     ZQD_EVENT_ROWS = 0,     /* new observable rows of a running job (zqd_obs_rows layout) */
@@ -464,10 +476,27 @@ void zqd_server_destroy(zqd_server* server);
 /* Fault injection for tests of the failure paths (no effect unless called): after `after` more
    successful device allocations, the next `count` ones fail as if the device were out of memory. */
 void zqd_testing_fail_device_allocations(uint64_t after, uint64_t count);
+/* Launches the server's persistent line-service kernel with `ctas` CTAs and posts nothing: every
+   CTA's wait for work runs out of its clock64 budget (idle_us) and it exits.  *idle_exits receives
+   the CTAs that left that way, *wall_ms the host time until the kernel had ended. */
+int zqd_testing_service_idle(zqd_precision precision, uint32_t nstate, uint32_t ctas, double idle_us,
+                             uint32_t* idle_exits, double* wall_ms);
 
 /* ------------------------------------------------------------------ device */
 int zqd_device_count(void);
 int zqd_set_device(int device);
+
+/* On-chip denominators for the roofline of the resident 1-D kernel, whose wavefunction stays in
+   shared memory (no counterpart in the reference): the shared-memory bandwidth of one SM with every
+   SM busy (128-bit loads and stores, no bank conflicts), and the latency of __syncthreads in a
+   256-thread CTA and of a barrier across a 16-CTA cluster, measured on the current device. */
+typedef struct {
+    double smem_bytes_per_cycle_per_sm, smem_gbs_per_sm;
+    double syncthreads_cycles, cluster_barrier_cycles;
+    double sm_clock_mhz; /* the device's maximum SM clock */
+    uint32_t sms;
+} zqd_onchip;
+int zqd_measure_onchip(zqd_onchip* out);
 
 #ifdef __cplusplus
 }

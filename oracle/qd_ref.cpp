@@ -12,12 +12,12 @@
 //     long double and rounded (FFTW 3.3.11 in the reference,
 //     src/fourier_transform.zig:38-47); Bluestein for other lengths.
 //     Forward sign -1 unnormalised, inverse sign +1 followed by a 1/N loop.
-//   * eigh: n == 1 and n == 2 restate LAPACK dsyevd (OpenBLAS 0.3.33,
+//   * eigh: restates LAPACK dsyevd('V', 'U') (OpenBLAS 0.3.33,
 //     src/linear_algebra.zig:67): for n == 2 the tridiagonal reduction is the
-//     identity and dsteqr finishes with dlaev2 + one plane rotation, so the
-//     eigenvector signs are LAPACK's.  n >= 3 uses cyclic Jacobi with the
-//     largest-magnitude component of each eigenvector made positive (sign
-//     convention not pinned against LAPACK).
+//     identity and dsteqr finishes with dlaev2 + one plane rotation; n >= 3
+//     runs dsytd2, dsteqr (implicit QL/QR, dlartg of LAPACK >= 3.10) and
+//     dorm2l.  The eigenvector signs are LAPACK's (pinned against
+//     numpy.linalg.eigh(UPLO='U'), which calls LAPACK dsyevd, in the tests).
 //   * custom potentials: an own recursive-descent evaluator of the ExprTk
 //     subset used by Zinq inputs (src/exprtk.cpp:10-40).
 //
@@ -650,48 +650,236 @@ void eigh2(const double* V, double* W, double* U) {
     U[3] = z22;
 }
 
-// cyclic Jacobi for n >= 3 (sorted ascending, largest-|component| made positive)
-void eigh_jacobi(int n, const double* V, double* W, double* U) {
-    std::vector<double> A(V, V + n * n), Z(n * n, 0.0);
-    for (int i = 0; i < n; ++i) Z[i * n + i] = 1.0;
-    for (int sweep = 0; sweep < 64; ++sweep) {
-        double off = 0, diag = 0;
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j)
-                if (i != j) off += A[i * n + j] * A[i * n + j];
-                else diag += A[i * n + j] * A[i * n + j];
-        if (off <= 1e-36 * diag || off == 0.0) break;
-        for (int p = 0; p < n - 1; ++p)
-            for (int q = p + 1; q < n; ++q) {
-                double apq = A[p * n + q];
-                if (apq == 0.0) continue;
-                double app = A[p * n + p], aqq = A[q * n + q];
-                double theta = (aqq - app) / (2.0 * apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
-                for (int k = 0; k < n; ++k) {
-                    double akp = A[k * n + p], akq = A[k * n + q];
-                    A[k * n + p] = c * akp - s * akq;
-                    A[k * n + q] = s * akp + c * akq;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double apk = A[p * n + k], aqk = A[q * n + k];
-                    A[p * n + k] = c * apk - s * aqk;
-                    A[q * n + k] = s * apk + c * aqk;
-                }
-                for (int k = 0; k < n; ++k) {
-                    double zkp = Z[k * n + p], zkq = Z[k * n + q];
-                    Z[k * n + p] = c * zkp - s * zkq;
-                    Z[k * n + q] = s * zkp + c * zkq;
-                }
-            }
+// LAPACK dsyevd('V', 'U') for small n (the reference's eighBatch, src/linear_algebra.zig:55-70,
+// calls LAPACKE_dsyevd row-major; for symmetric input that is dsyevd on the same matrix), restated
+// from the published netlib algorithm: dsytd2 (Householder reduction of the upper triangle, last
+// column first), dsteqr('I') (implicit QL or QR with Wilkinson-type shifts and plane rotations,
+// 2 x 2 blocks by dlaev2, selection sort of the eigenvalues) and dorm2l (the reflectors applied
+// to the eigenvectors of the tridiagonal matrix).  Arithmetic in the published operation order.
+namespace lapack {
+const double EPS = 1.1102230246251565e-16;    // dlamch('E') = 2^-53
+const double SAFMIN = 2.2250738585072014e-308; // dlamch('S')
+
+double sign(double a, double b) { return b >= 0 ? std::fabs(a) : -std::fabs(a); }
+
+double dlapy2(double x, double y) {
+    const double xa = std::fabs(x), ya = std::fabs(y), w = std::max(xa, ya), z = std::min(xa, ya);
+    if (z == 0.0 || w > 1.7976931348623157e308) return w;
+    const double q = z / w;
+    return w * std::sqrt(1.0 + q * q);
+}
+
+// dlartg (LAPACK >= 3.10): c >= 0, r carries the sign of f
+void dlartg(double f, double g, double& c, double& s, double& r) {
+    const double rtmin = std::sqrt(SAFMIN), rtmax = std::sqrt(1.0 / SAFMIN / 2.0);
+    const double f1 = std::fabs(f), g1 = std::fabs(g);
+    if (g == 0.0) {
+        c = 1.0;
+        s = 0.0;
+        r = f;
+    } else if (f == 0.0) {
+        c = 0.0;
+        s = sign(1.0, g);
+        r = g1;
+    } else if (f1 > rtmin && f1 < rtmax && g1 > rtmin && g1 < rtmax) {
+        const double d = std::sqrt(f * f + g * g);
+        c = f1 / d;
+        r = sign(d, f);
+        s = g / r;
+    } else {
+        const double u = std::min(1.0 / SAFMIN, std::max(SAFMIN, std::max(f1, g1)));
+        const double fs = f / u, gs = g / u, d = std::sqrt(fs * fs + gs * gs);
+        c = std::fabs(fs) / d;
+        r = sign(d, f);
+        s = gs / r;
+        r = r * u;
     }
-    std::vector<double> d(n);
-    for (int i = 0; i < n; ++i) d[i] = A[i * n + i];
-    for (int i = 0; i < n - 1; ++i) {
+}
+
+// dlasr('R', 'V', DIRECT, m rows, cols j0 .. j0+nc-1 of Z (n x n, column j of Z at Z[r*n + j]))
+void dlasr_rv(bool forward, int n, int j0, int nc, const double* c, const double* s, double* Z) {
+    auto rot = [&](int j) {
+        const double ct = c[j], st = s[j];
+        if (ct == 1.0 && st == 0.0) return;
+        for (int i = 0; i < n; ++i) {
+            const double t = Z[i * n + j0 + j + 1];
+            Z[i * n + j0 + j + 1] = ct * t - st * Z[i * n + j0 + j];
+            Z[i * n + j0 + j] = st * t + ct * Z[i * n + j0 + j];
+        }
+    };
+    if (forward)
+        for (int j = 0; j < nc - 1; ++j) rot(j);
+    else
+        for (int j = nc - 2; j >= 0; --j) rot(j);
+}
+
+// dsteqr('I'): eigenvalues d (ascending on return) and eigenvectors Z of the tridiagonal (d, e)
+bool dsteqr(int n, double* d, double* e, double* Z) {
+    const double eps2 = EPS * EPS, safmax = 1.0 / SAFMIN, ssfmax = std::sqrt(safmax) / 3.0,
+                 ssfmin = std::sqrt(SAFMIN) / eps2;
+    for (int i = 0; i < n * n; ++i) Z[i] = 0.0;
+    for (int i = 0; i < n; ++i) Z[i * n + i] = 1.0;
+    double wc[8], ws[8]; // work(1:n-1) and work(n:2n-2)
+    const int nmaxit = n * 30;
+    int jtot = 0, l1 = 0;
+    for (;;) { // 10
+        if (l1 > n - 1) break;
+        if (l1 > 0) e[l1 - 1] = 0.0;
+        int m = n - 1;
+        for (int mm = l1; mm < n - 1; ++mm) {
+            const double tst = std::fabs(e[mm]);
+            if (tst == 0.0) {
+                m = mm;
+                break;
+            }
+            if (tst <= (std::sqrt(std::fabs(d[mm])) * std::sqrt(std::fabs(d[mm + 1]))) * EPS) {
+                e[mm] = 0.0;
+                m = mm;
+                break;
+            }
+        }
+        int l = l1;
+        const int lsv = l;
+        int lend = m;
+        const int lendsv = lend;
+        l1 = m + 1;
+        if (lend == l) continue;
+        // scale the block (only outside [ssfmin, ssfmax])
+        double anorm = 0.0;
+        for (int i = l; i <= lend; ++i) anorm = std::max(anorm, std::fabs(d[i]));
+        for (int i = l; i < lend; ++i) anorm = std::max(anorm, std::fabs(e[i]));
+        if (anorm == 0.0) continue;
+        double to = 0.0; // dlascl: the block scaled by to / anorm (outside [ssfmin, ssfmax] only)
+        if (anorm > ssfmax) to = ssfmax;
+        if (anorm < ssfmin) to = ssfmin;
+        if (to != 0.0) {
+            for (int i = l; i <= lend; ++i) d[i] = d[i] * (to / anorm);
+            for (int i = l; i < lend; ++i) e[i] = e[i] * (to / anorm);
+        }
+        if (std::fabs(d[lend]) < std::fabs(d[l])) {
+            lend = lsv;
+            l = lendsv;
+        }
+        if (lend > l) { // QL iteration
+            for (;;) {   // 40
+                int mq = lend;
+                for (int mm = l; mm < lend; ++mm) {
+                    const double tst = std::fabs(e[mm]) * std::fabs(e[mm]);
+                    if (tst <= (eps2 * std::fabs(d[mm])) * std::fabs(d[mm + 1]) + SAFMIN) {
+                        mq = mm;
+                        break;
+                    }
+                }
+                if (mq < lend) e[mq] = 0.0;
+                double p = d[l];
+                if (mq == l) { // eigenvalue found
+                    d[l] = p;
+                    ++l;
+                    if (l <= lend) continue;
+                    break;
+                }
+                if (mq == l + 1) {
+                    double rt1, rt2, c, s;
+                    dlaev2(d[l], e[l], d[l + 1], rt1, rt2, c, s);
+                    wc[0] = c;
+                    ws[0] = s;
+                    dlasr_rv(false, n, l, 2, wc, ws, Z);
+                    d[l] = rt1;
+                    d[l + 1] = rt2;
+                    e[l] = 0.0;
+                    l += 2;
+                    if (l <= lend) continue;
+                    break;
+                }
+                if (jtot == nmaxit) break;
+                ++jtot;
+                double g = (d[l + 1] - p) / (2.0 * e[l]);
+                double r = dlapy2(g, 1.0);
+                g = d[mq] - p + (e[l] / (g + sign(r, g)));
+                double s = 1.0, c = 1.0;
+                p = 0.0;
+                for (int i = mq - 1; i >= l; --i) {
+                    const double f = s * e[i], b = c * e[i];
+                    dlartg(g, f, c, s, r);
+                    if (i != mq - 1) e[i + 1] = r;
+                    g = d[i + 1] - p;
+                    r = (d[i] - g) * s + 2.0 * c * b;
+                    p = s * r;
+                    d[i + 1] = g + p;
+                    g = c * r - b;
+                    wc[i - l] = c;
+                    ws[i - l] = -s;
+                }
+                dlasr_rv(false, n, l, mq - l + 1, wc, ws, Z);
+                d[l] = d[l] - p;
+                e[l] = g;
+            }
+        } else { // QR iteration
+            for (;;) { // 90
+                int mq = lend;
+                for (int mm = l; mm > lend; --mm) {
+                    const double tst = std::fabs(e[mm - 1]) * std::fabs(e[mm - 1]);
+                    if (tst <= (eps2 * std::fabs(d[mm])) * std::fabs(d[mm - 1]) + SAFMIN) {
+                        mq = mm;
+                        break;
+                    }
+                }
+                if (mq > lend) e[mq - 1] = 0.0;
+                double p = d[l];
+                if (mq == l) {
+                    d[l] = p;
+                    --l;
+                    if (l >= lend) continue;
+                    break;
+                }
+                if (mq == l - 1) {
+                    double rt1, rt2, c, s;
+                    dlaev2(d[l - 1], e[l - 1], d[l], rt1, rt2, c, s);
+                    wc[0] = c;
+                    ws[0] = s;
+                    dlasr_rv(true, n, l - 1, 2, wc, ws, Z);
+                    d[l - 1] = rt1;
+                    d[l] = rt2;
+                    e[l - 1] = 0.0;
+                    l -= 2;
+                    if (l >= lend) continue;
+                    break;
+                }
+                if (jtot == nmaxit) break;
+                ++jtot;
+                double g = (d[l - 1] - p) / (2.0 * e[l - 1]);
+                double r = dlapy2(g, 1.0);
+                g = d[mq] - p + (e[l - 1] / (g + sign(r, g)));
+                double s = 1.0, c = 1.0;
+                p = 0.0;
+                for (int i = mq; i <= l - 1; ++i) {
+                    const double f = s * e[i], b = c * e[i];
+                    dlartg(g, f, c, s, r);
+                    if (i != mq) e[i - 1] = r;
+                    g = d[i] - p;
+                    r = (d[i + 1] - g) * s + 2.0 * c * b;
+                    p = s * r;
+                    d[i] = g + p;
+                    g = c * r - b;
+                    wc[i - mq] = c;
+                    ws[i - mq] = s;
+                }
+                dlasr_rv(true, n, mq, l - mq + 1, wc, ws, Z);
+                d[l] = d[l] - p;
+                e[l - 1] = g;
+            }
+        }
+        if (to != 0.0) { // undo the scaling
+            for (int i = lsv; i <= lendsv; ++i) d[i] = d[i] * (anorm / to);
+            for (int i = lsv; i < lendsv; ++i) e[i] = e[i] * (anorm / to);
+        }
+        if (jtot >= nmaxit) return false;
+    }
+    for (int ii = 1; ii < n; ++ii) { // selection sort, ascending
+        const int i = ii - 1;
         int k = i;
         double p = d[i];
-        for (int j = i + 1; j < n; ++j)
+        for (int j = ii; j < n; ++j)
             if (d[j] < p) {
                 k = j;
                 p = d[j];
@@ -702,16 +890,81 @@ void eigh_jacobi(int n, const double* V, double* W, double* U) {
             for (int r = 0; r < n; ++r) std::swap(Z[r * n + i], Z[r * n + k]);
         }
     }
-    for (int m = 0; m < n; ++m) {
-        int big = 0;
-        for (int k = 1; k < n; ++k)
-            if (std::fabs(Z[k * n + m]) > std::fabs(Z[big * n + m])) big = k;
-        if (Z[big * n + m] < 0)
-            for (int k = 0; k < n; ++k) Z[k * n + m] = -Z[k * n + m];
+    return true;
+}
+
+// dsyevd('V', 'U') of the symmetric n x n V (row-major; the upper triangle is read)
+void dsyevd(int n, const double* V, double* W, double* U) {
+    double A[8][8] = {}, d[8] = {}, e[8] = {}, tau[8] = {}; // A[i][j]: LAPACK's A(i+1, j+1)
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) A[i][j] = V[i * n + j];
+    // dsytd2('U'): reflector H(i) annihilates A(1:i-1, i+1), i = n-1 .. 1
+    for (int i = n - 1; i >= 1; --i) {
+        // dlarfg(i, A(i, i+1), A(1:i-1, i+1))
+        double alpha = A[i - 1][i], taui = 0.0;
+        if (i > 1) {
+            double xnorm = 0.0;
+            for (int k = 0; k < i - 1; ++k) xnorm += A[k][i] * A[k][i];
+            xnorm = std::sqrt(xnorm);
+            if (xnorm != 0.0) {
+                const double beta = -sign(dlapy2(alpha, xnorm), alpha);
+                taui = (beta - alpha) / beta;
+                const double sc = 1.0 / (alpha - beta);
+                for (int k = 0; k < i - 1; ++k) A[k][i] = A[k][i] * sc;
+                alpha = beta;
+            }
+        }
+        A[i - 1][i] = alpha;
+        e[i - 1] = alpha;
+        if (taui != 0.0) {
+            A[i - 1][i] = 1.0;
+            // tau(1:i) = taui * A(1:i, 1:i) v, v = A(1:i, i+1) (dsymv, upper)
+            double y[8] = {0};
+            for (int j = 0; j < i; ++j) {
+                const double t1 = taui * A[j][i];
+                double t2 = 0.0;
+                for (int k = 0; k < j; ++k) {
+                    y[k] += t1 * A[k][j];
+                    t2 += A[k][j] * A[k][i];
+                }
+                y[j] += t1 * A[j][j] + taui * t2;
+            }
+            double dot = 0.0;
+            for (int k = 0; k < i; ++k) dot += y[k] * A[k][i];
+            const double al = -0.5 * taui * dot;
+            for (int k = 0; k < i; ++k) y[k] += al * A[k][i];
+            // A := A - v w' - w v' (dsyr2, upper)
+            for (int j = 0; j < i; ++j) {
+                if (A[j][i] != 0.0 || y[j] != 0.0) {
+                    const double t1 = -1.0 * y[j], t2 = -1.0 * A[j][i];
+                    for (int k = 0; k <= j; ++k) A[k][j] += A[k][i] * t1 + y[k] * t2;
+                }
+            }
+            A[i - 1][i] = e[i - 1];
+        }
+        d[i] = A[i][i];
+        tau[i - 1] = taui;
+    }
+    d[0] = A[0][0];
+    double Z[64];
+    if (!dsteqr(n, d, e, Z)) throw std::runtime_error("dsteqr did not converge");
+    // dorm2l('L', 'N'): Z(1:i, :) <- H(i) Z(1:i, :), i = 1 .. n-1, v = [A(1:i-1, i+1); 1]
+    for (int i = 1; i <= n - 1; ++i) {
+        const double t = tau[i - 1];
+        if (t == 0.0) continue;
+        double v[8];
+        for (int k = 0; k < i - 1; ++k) v[k] = A[k][i];
+        v[i - 1] = 1.0;
+        for (int c = 0; c < n; ++c) {
+            double w = 0.0;
+            for (int k = 0; k < i; ++k) w += Z[k * n + c] * v[k];
+            for (int k = 0; k < i; ++k) Z[k * n + c] -= t * v[k] * w;
+        }
     }
     for (int i = 0; i < n; ++i) W[i] = d[i];
     for (int i = 0; i < n * n; ++i) U[i] = Z[i];
 }
+} // namespace lapack
 
 void eigh_any(int n, const double* V, double* W, double* U) {
     if (n == 1) {
@@ -720,7 +973,7 @@ void eigh_any(int n, const double* V, double* W, double* U) {
     } else if (n == 2) {
         eigh2(V, W, U);
     } else {
-        eigh_jacobi(n, V, W, U);
+        lapack::dsyevd(n, V, W, U);
     }
 }
 

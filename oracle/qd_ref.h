@@ -124,8 +124,8 @@ size_t qr_spectrum_len(const qr_result* r, int s, size_t* acf_padded_len);
 void qr_spectrum(const qr_result* r, int s, double* acf_padded /* complex */, double* sigma);
 
 /* ---- unit-level entry points used by the tests ---- */
-/* eigendecomposition of one symmetric n x n matrix (row-major), LAPACK dsyevd conventions
-   for n <= 2, cyclic Jacobi for n >= 3; W ascending; U[k*n+m] = component k of vector m */
+/* eigendecomposition of one symmetric n x n matrix (row-major), LAPACK dsyevd('V', 'U')
+   restated; W ascending; U[k*n+m] = component k of vector m */
 void qr_eigh(int n, const double* V, double* W, double* U);
 /* in-place N-D complex DFT (sign -1 forward unnormalised, +1 inverse with 1/N) */
 void qr_fft(int ndim, const int* shape, int sign, double* data);

@@ -18,6 +18,8 @@ import pytest
 from zinq_b200 import _abi
 from zinq_b200 import quantum_dynamics as qd
 
+from test_gpu_server import alone_as_served
+
 pytestmark = pytest.mark.gpu
 
 
@@ -172,7 +174,8 @@ def drain(srv, tickets, timeout_s=120):
 
 
 def test_streamed_rows_concatenate_to_the_history():
-    srv = qd.Server(workers=2, stream_steps=50)
+    # launches of 50 steps (the persistent kernel's streaming is tested with it)
+    srv = qd.Server(workers=2, stream_steps=50, persistent_lines=False)
     opts = [line_job(p) for p in (10, 20, 30)] + [coupled_2d(130)]
     tickets = [srv.submit(o, "fp64") for o in opts]
     ev = drain(srv, tickets)
@@ -187,7 +190,7 @@ def test_streamed_rows_concatenate_to_the_history():
 
 
 def test_requests_join_a_group_already_on_the_gpu():
-    srv = qd.Server(workers=1, max_batch=8, stream_steps=64)
+    srv = qd.Server(workers=1, max_batch=8, stream_steps=64, persistent_lines=False)
     first = srv.submit(line_job(15, iters=3000), "fp32")
     time.sleep(0.05)  # the first request is on the GPU now
     later = [srv.submit(line_job(p, iters=400), "fp32") for p in (10, 20, 25, 30)]
@@ -219,7 +222,7 @@ def test_cancel_queued_and_running_requests():
     srv.close()
     assert st["cancelled"] == 2
     np.testing.assert_array_equal(r.observables[0].history["population"],
-                                  qd.run(line_job(20, iters=100), want_wavefunction=False).observables[0].history["population"])
+                                  alone_as_served(line_job(20, iters=100), "fp64").observables[0].history["population"])
 
 
 def test_wait_timeout_then_result():
@@ -264,7 +267,7 @@ def test_consumer_that_stops_polling_loses_only_row_events():
     assert sorted(e["ticket"] for e in events if e["kind"] == "done") == sorted(tickets)
     for o, r in zip(opts, res):
         np.testing.assert_array_equal(r.observables[0].history["population"],
-                                      qd.run(o, want_wavefunction=False).observables[0].history["population"])
+                                      alone_as_served(o, "fp64").observables[0].history["population"])
 
 
 def test_job_whose_norm_turns_nan_fails_alone():

@@ -245,3 +245,13 @@ def test_2d_time_dependent_adiabatic_wavefunction_history_signs():
     job.close()
     r = qd_ref.run(opt)[0]
     assert float(np.max(np.abs(g.history["wavefunction"] - r.history["wfn"]))) <= 1e-10
+
+
+def test_2d_three_states_adiabatic_initial_state():
+    # toDia with the three-state eigenvectors at every point (LAPACK dsyevd restated on both sides),
+    # compared without sign freedom
+    opt = coupled_harmonic_2d(npoint=64, iters=100)
+    opt["initial_conditions"] = dict(opt["initial_conditions"], adiabatic=True, state=1)
+    opt["adiabatic"] = True
+    opt["write"] = {"population": "P", "wavefunction": "W"}
+    compare(opt)

@@ -56,13 +56,16 @@ def test_auto_in_a_batch_and_through_the_server():
     for r, a, e in zip(qd.run_batch(opts, "auto"), alone, expected):
         assert r.precision == e
         _same(r, a)
-    srv = qd.Server(workers=1, max_batch=8)
-    tickets = [srv.submit(o, "auto") for o in opts]
-    out = [srv.wait(t)[0] for t in tickets]
-    srv.close()
-    for r, a, e in zip(out, alone, expected):
-        assert r.precision == e
-        _same(r, a)
+    from test_gpu_server import alone_as_served
+
+    for persistent in (False, True):  # grouped launches, then the persistent line-service kernel
+        srv = qd.Server(workers=1, max_batch=8, persistent_lines=persistent)
+        tickets = [srv.submit(o, "auto") for o in opts]
+        out = [srv.wait(t)[0] for t in tickets]
+        srv.close()
+        for r, o, e in zip(out, opts, expected):
+            assert r.precision == e
+            _same(r, alone_as_served(o, e) if persistent else qd.run(o, precision=e, want_wavefunction=False))
 
 
 def test_auto_on_a_2d_grid():

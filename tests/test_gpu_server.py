@@ -1,5 +1,8 @@
-"""The job server (zqd_server_*): a stream of independent requests with HBM admission and grouped
-launches of compatible 1-D jobs returns, per request, exactly what a job run alone returns."""
+"""The job server (zqd_server_*): a stream of independent requests with HBM admission, grouped
+launches of compatible 1-D jobs and the persistent line-service kernel returns, per request, exactly
+what the same job run alone with the same launch shape returns (bit for bit)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -7,6 +10,28 @@ from zinq_b200 import _abi
 from zinq_b200 import quantum_dynamics as qd
 
 pytestmark = pytest.mark.gpu
+
+
+def served_by_service(opt, precision):
+    """The server sends 1-D single-solve requests whose line fits one CTA to the persistent kernel."""
+    return (len(opt["grid"]["bounds"]) == 1 and (opt.get("imaginary") or {}).get("nstate", 1) <= 1
+            and opt["grid"]["npoint"] <= (1024 if precision == "fp64" else 2048))
+
+
+def alone_as_served(opt, precision, want_wavefunction=False):
+    """The job run alone (zqd_run) with the launch shape the server gives it: one CTA per line on the
+    persistent kernel, the built-in rules otherwise."""
+    if not served_by_service(opt, precision):
+        return qd.run(opt, precision=precision, want_wavefunction=want_wavefunction)
+    old = os.environ.get("ZQD_LINE_CLUSTER")
+    os.environ["ZQD_LINE_CLUSTER"] = "1"
+    try:
+        return qd.run(opt, precision=precision, want_wavefunction=want_wavefunction)
+    finally:
+        if old is None:
+            del os.environ["ZQD_LINE_CLUSTER"]
+        else:
+            os.environ["ZQD_LINE_CLUSTER"] = old
 
 
 def _same(a, b):
@@ -24,8 +49,9 @@ def test_scaled_stream_equals_jobs_run_alone(precision):
     res, lat, wall, st = qd.serve_stream(opts, arrivals, precision, workers=4, max_batch=8)
     assert st["completed"] == len(opts) and st["failed"] == 0
     assert all(x > 0 for x in lat)
+    assert st["service_jobs"] >= 1
     for o, r in zip(opts, res):
-        _same(r, qd.run(o, precision=precision, want_wavefunction=False))
+        _same(r, alone_as_served(o, precision))
 
 
 def test_compatible_1d_requests_share_launches():
@@ -39,7 +65,7 @@ def test_compatible_1d_requests_share_launches():
         o = {**base, "initial_conditions": {**base["initial_conditions"], "momentum": [float(p0)],
                                             "gamma": [float(p0 * p0 / 400.0)]}}
         opts.append(o)
-    srv = qd.Server(workers=1, max_batch=16)
+    srv = qd.Server(workers=1, max_batch=16, persistent_lines=False)
     # one worker: while it runs the first request the others queue up and are taken together
     tickets = [srv.submit(o, "fp32") for o in opts]
     out = [srv.wait(t)[0] for t in tickets]

@@ -71,17 +71,20 @@ def test_eigh_matches_oracle(n):
         np.testing.assert_allclose(U[i] @ np.diag(W[i]) @ U[i].T, A[i], atol=1e-15)
 
 
-def test_eigh_2x2_signs_match_lapack():
-    # numpy.linalg.eigh calls LAPACK ?syevd, the routine the reference uses (src/linear_algebra.zig:67)
-    rng = np.random.default_rng(7)
-    A = rng.standard_normal((2000, 2, 2))
+@pytest.mark.parametrize("n", [2, 3, 4])
+def test_eigh_signs_match_lapack(n):
+    # numpy.linalg.eigh calls LAPACK ?syevd, the routine the reference uses (src/linear_algebra.zig:67);
+    # eigenvectors compared without any sign freedom, random and nearly diagonal matrices
+    rng = np.random.default_rng(7 + n)
+    A = rng.standard_normal((3000, n, n))
     A = A + A.transpose(0, 2, 1)
+    A[1000:2000] = 0.01 * A[1000:2000] + np.einsum("ki,ij->kij", rng.standard_normal((1000, n)), np.eye(n))
     L = _abi.load()
-    W, U = np.zeros((2000, 2)), np.zeros((2000, 2, 2))
-    _abi.check(L.zqd_eigh_batch(2, 2000, dptr(np.ascontiguousarray(A)), dptr(W), dptr(U)))
+    W, U = np.zeros((3000, n)), np.zeros((3000, n, n))
+    _abi.check(L.zqd_eigh_batch(n, 3000, dptr(np.ascontiguousarray(A)), dptr(W), dptr(U)))
     w_np, u_np = np.linalg.eigh(A, UPLO="U")
-    np.testing.assert_allclose(W, w_np, atol=1e-14)
-    np.testing.assert_allclose(U, u_np, atol=1e-13)
+    np.testing.assert_allclose(W, w_np, atol=1e-13)
+    np.testing.assert_allclose(U, u_np, atol=1e-12)
 
 
 EXPRS = ["0.5*r1^2", "+sgn(r1) * 0.01 * (1.0 - exp(-1.6 * abs(r1)))", "0.005 * exp(-r1^2)",

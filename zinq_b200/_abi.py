@@ -88,17 +88,24 @@ class ZqdObsRows(C.Structure):
 class ZqdServerConfig(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
                 ("device_budget_bytes", C.c_uint64), ("stream_steps", C.c_uint32), ("stream_rows", C.c_int),
-                ("max_events", C.c_uint32)]
+                ("max_events", C.c_uint32), ("persistent_lines", C.c_int), ("service_ctas", C.c_uint32),
+                ("service_idle_us", C.c_double)]
 
 
 class ZqdServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submitted", "completed", "failed", "cancelled", "queued",
                                           "grouped_launches", "grouped_jobs", "joined_jobs", "device_budget_bytes",
                                           "device_bytes_in_use", "peak_device_bytes", "pending_events",
-                                          "dropped_events")]
+                                          "dropped_events", "service_jobs", "service_launches")]
 
 
 EVENT = {0: "rows", 1: "done", 2: "failed", 3: "cancelled"}
+
+
+class ZqdOnchip(C.Structure):
+    _fields_ = [("smem_bytes_per_cycle_per_sm", C.c_double), ("smem_gbs_per_sm", C.c_double),
+                ("syncthreads_cycles", C.c_double), ("cluster_barrier_cycles", C.c_double),
+                ("sm_clock_mhz", C.c_double), ("sms", C.c_uint32)]
 
 
 class ZqdTuneEntry(C.Structure):
@@ -172,11 +179,14 @@ SIGNATURES = [
     ("zqd_server_stats_get", C.c_int, [VP, C.POINTER(ZqdServerStats)]),
     ("zqd_server_destroy", None, [VP]),
     ("zqd_testing_fail_device_allocations", None, [C.c_uint64, C.c_uint64]),
+    ("zqd_testing_service_idle", C.c_int, [C.c_int, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(C.c_uint32),
+                                           C.POINTER(C.c_double)]),
     ("zqd_autotune", C.c_int, [C.POINTER(ZqdTuneEntry)]),
     ("zqd_tune_save", C.c_int, [C.c_char_p]),
     ("zqd_tune_load", C.c_int, [C.c_char_p]),
     ("zqd_tune_clear", None, []),
     ("zqd_tune_size", C.c_uint32, []),
+    ("zqd_measure_onchip", C.c_int, [C.POINTER(ZqdOnchip)]),
     ("zqd_device_count", C.c_int, []),
     ("zqd_set_device", C.c_int, [C.c_int]),
 ]

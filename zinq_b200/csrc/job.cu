@@ -1100,6 +1100,40 @@ int zqd::step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cud
     return ZQD_OK;
 }
 
+// Descriptor of a created single-solve 1-D job for the persistent service kernel: the whole solve
+// in one claim, rows published through `progress` (a device pointer into pinned host memory).
+size_t zqd::line_desc_bytes(bool fp32) { return fp32 ? sizeof(LineJob<float>) : sizeof(LineJob<double>); }
+
+int zqd::service_desc(zqd_job* J, void* out, int* progress) {
+    if (J->d != 1 || J->nsolve != 1 || J->C != 1) return fail(ZQD_ERR_INVALID_INPUT, "SERVICE JOBS ARE SINGLE-CTA 1-D SOLVES");
+    if (!J->stepping) {
+        reset_progress(J);
+        J->stepping = true;
+        const int rc = J->fp32 ? refresh_line_tables<float>(J) : refresh_line_tables<double>(J);
+        if (rc) return rc;
+        ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    }
+    if (J->fp32) {
+        LineJob<float> d = line_job_desc<float>(J, 0);
+        d.progress = progress;
+        std::memcpy(out, &d, sizeof(d));
+    } else {
+        LineJob<double> d = line_job_desc<double>(J, 0);
+        d.progress = progress;
+        std::memcpy(out, &d, sizeof(d));
+    }
+    J->h2d += line_desc_bytes(J->fp32);
+    return ZQD_OK;
+}
+
+// a service job's solve ended on the device: its progress as after zqd_job_run
+int zqd::service_job_ended(zqd_job* J) { return mark_all_ended(J); }
+
+// rows the service kernel has published for the job (zqd_job_observables reads up to here)
+void zqd::service_job_rows(zqd_job* J, int rows) {
+    if (!J->solve_rows.empty() && rows > J->solve_rows[0]) J->solve_rows[0] = rows;
+}
+
 extern "C" int zqd_batch_result(zqd_batch* B, uint32_t i, zqd_result** out) {
     if (!B || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
     if (i >= B->jobs.size()) return fail(ZQD_ERR_NOT_FOUND, "JOB INDEX OUT OF RANGE");

@@ -48,6 +48,12 @@ namespace zqd {
 int job_create_opts(Opts&& o, zqd_job** out);
 int run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, float* ms);
 int step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cudaStream_t st);
+// the persistent service kernel's side of a job (service.cu)
+size_t line_desc_bytes(bool fp32);
+int service_desc(zqd_job* J, void* out, int* progress);
+int service_job_ended(zqd_job* J);
+void service_job_rows(zqd_job* J, int rows);
+
 // Launch shape chosen by the autotuner (tune.cu) for a (dims, points, states, precision) key, or
 // forced on this thread while the autotuner measures a candidate; zero fields keep the default.
 struct ShapeOverride {
@@ -55,6 +61,8 @@ struct ShapeOverride {
     int rows = 0, tile = 0; // N-D: rows of the last axis per row-pass CTA, lines per tile-pass CTA
 };
 bool lookup_shape(int d, int n, int S, bool fp32, ShapeOverride& out);
+// a job created with a given launch shape (the autotuner's candidates, the service's single CTAs)
+int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out);
 // Time-dependent potential whose eigenvector signs some output observes: the wavefunction history in
 // the adiabatic basis, or the toDia of a later imaginary-time solve (wavepacket.zig:145-167 then apply).
 inline bool needs_sign_tracking(const Opts& o, int S, int nsolve) {

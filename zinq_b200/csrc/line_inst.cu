@@ -1,14 +1,14 @@
 // line_inst.cu -- instantiations of the resident line kernel for one
 // (precision, state count) pair.  The build compiles this file once per pair
-// with -DZQD_T=<double|float> -DZQD_S=<1..4> -DZQD_LAUNCH=<symbol>, so the
+// with -DZQD_T=<double|float> -DZQD_S=<1..4> -DZQD_LAUNCH=<symbol> -DZQD_SERVICE=<symbol>, so the
 // heavy template instantiations spread over parallel nvcc processes.
 #include <mutex>
 
 #include "internal.h"
 #include "line_solve.cuh"
 
-#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_LAUNCH)
-#error "line_inst.cu needs -DZQD_T, -DZQD_S and -DZQD_LAUNCH"
+#if !defined(ZQD_T) || !defined(ZQD_S) || !defined(ZQD_LAUNCH) || !defined(ZQD_SERVICE)
+#error "line_inst.cu needs -DZQD_T, -DZQD_S, -DZQD_LAUNCH and -DZQD_SERVICE"
 #endif
 
 namespace zqd {
@@ -54,6 +54,19 @@ int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
     case 16: return launch_one<16, 2>(J, dj, nj);
     default: return fail(ZQD_ERR_UNSUPPORTED, "CLUSTER SIZE MUST BE 1, 2, 4, 8 OR 16");
     }
+}
+
+// The persistent service kernel (single-CTA jobs, radix-4 local passes): grid CTAs of `threads`
+// threads with `smem` bytes of dynamic shared memory each, on stream st.
+int ZQD_SERVICE(const void* svc, unsigned grid, int threads, size_t smem, cudaStream_t st) {
+    auto kern = line_service_kernel<ZQD_T, ZQD_S, 2>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [&] { attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 215 * 1024); });
+    ZQD_CUDA(attr_err);
+    kern<<<grid, threads, smem, st>>>(*reinterpret_cast<const LineService<ZQD_T>*>(svc));
+    ZQD_CUDA(cudaGetLastError());
+    return ZQD_OK;
 }
 
 } // namespace zqd

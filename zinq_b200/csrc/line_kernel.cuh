@@ -92,6 +92,7 @@ template <typename T> struct LineJob {
     int i0, i1;
     double* carry; // [S] absorbed populations between launches of one solve
     int* done;     // 1 once the solve has ended (last step or stop_norm)
+    int* progress; // or null: rows written so far, published to the host after every row (pinned memory)
     PotDev pot;
 };
 

@@ -750,20 +750,21 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     }
 };
 
+// system-scope release store / acquire load: the host polls and writes these words in pinned memory
+__device__ __forceinline__ void st_release_sys(int* p, int v) {
+    asm volatile("st.release.sys.global.s32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire_sys(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The solve of job J (already in shared memory) on this CTA / cluster.
 template <typename T, int S, int C, int LRM>
-__global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel(const LineJob<T>* __restrict__ jobs) {
+__device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsigned char* smem_raw, int cta) {
     using Solver = LineSolver<T, S, C, LRM>;
     constexpr int NSYM = Solver::NSYM;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ LineJob<T> J;
-    __shared__ RedSmem rs;
-
-    const int cta = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
-    if (threadIdx.x == 0) {
-        J = jobs[blockIdx.x / C];
-        rs.slot_idx = 0;
-    }
-    __syncthreads();
 
     Solver X;
     X.J = &J;
@@ -880,6 +881,10 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
             ctx.psi = X.cur;
         }
         const double nrm = X.finish_row(J.hist + (size_t)i * HC);
+        if (J.progress && cta == 0 && threadIdx.x == 0) { // row i is in memory: publish it to the host
+            __threadfence_system();
+            st_release_sys(J.progress, i + 1);
+        }
         if (J.wfn_hist) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
             cx<T>* __restrict__ dst = J.wfn_hist + (size_t)i * S * n;
             for (int j = threadIdx.x; j < m; j += blockDim.x) {
@@ -929,6 +934,85 @@ __global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel
         J.psi_save[(size_t)s * n + X.base + j] = X.cur[s * X.ldp + padx<T>(j)];
     }
     if constexpr (C > 1) cg::this_cluster().sync(); // keep shared memory alive for remote readers
+}
+
+// One cluster of C CTAs per job of the array: a group of jobs in one launch.
+template <typename T, int S, int C, int LRM>
+__global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_solve_kernel(const LineJob<T>* __restrict__ jobs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ LineJob<T> J;
+    __shared__ RedSmem rs;
+    const int cta = (C > 1) ? (int)cg::this_cluster().block_rank() : 0;
+    if (threadIdx.x == 0) {
+        J = jobs[blockIdx.x / C];
+        rs.slot_idx = 0;
+    }
+    __syncthreads();
+    line_solve_run<T, S, C, LRM>(J, rs, smem_raw, cta);
+}
+
+// ------------------------------------------------------------ the persistent service kernel
+// Words the host writes and the device reads, in pinned host memory.
+struct LineServiceCtl {
+    unsigned tail;   // jobs posted so far (slot k % capacity holds job k)
+    unsigned closed; // exit once every posted job has been claimed
+};
+template <typename T> struct LineService {
+    const LineJob<T>* jobs; // [capacity] descriptors, pinned host memory
+    const LineServiceCtl* ctl;
+    int* done;              // [capacity] pinned host memory: 1 once job k's solve has ended
+    unsigned* counters;     // device memory: [0] jobs claimed so far, [1] CTAs that left idle
+    unsigned capacity;
+    long long idle_cycles;  // clock64 budget of one idle wait for work
+};
+
+// Persistent CTAs working through a job table the host keeps appending to (continuous batching
+// of single-CTA 1-D jobs of uneven sizes): a CTA claims the next posted job, runs its whole solve
+// with the wavefunction resident in shared memory, publishes each history row and the end of the
+// solve to the host, and claims the next.  A CTA that finds no work waits at most idle_cycles
+// (clock64) and then exits; the host relaunches when it posts work to a kernel that has ended.
+template <typename T, int S, int LRM>
+__global__ void __launch_bounds__(LineMaxThreads<T>::value, 1) line_service_kernel(LineService<T> svc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ LineJob<T> J;
+    __shared__ RedSmem rs;
+    __shared__ long long claimed;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            claimed = -1;
+            const long long t0 = clock64();
+            for (;;) {
+                const unsigned tail = ld_acquire_sys(&svc.ctl->tail);
+                const unsigned c = atomicAdd(&svc.counters[0], 0u);
+                if (c < tail) {
+                    if (atomicCAS(&svc.counters[0], c, c + 1) == c) {
+                        claimed = c;
+                        break;
+                    }
+                    continue;
+                }
+                if (ld_acquire_sys(&svc.ctl->closed)) break;
+                if (clock64() - t0 > svc.idle_cycles) { // bounded: nothing posted within the budget
+                    atomicAdd(&svc.counters[1], 1u);
+                    break;
+                }
+                __nanosleep(1000);
+            }
+            if (claimed >= 0) {
+                J = svc.jobs[(unsigned)claimed % svc.capacity];
+                rs.slot_idx = 0;
+            }
+        }
+        __syncthreads();
+        if (claimed < 0) return;
+        line_solve_run<T, S, 1, LRM>(J, rs, smem_raw, 0);
+        __syncthreads(); // every thread's results are written
+        if (threadIdx.x == 0) {
+            __threadfence_system();
+            st_release_sys(&svc.done[(unsigned)claimed % svc.capacity], 1);
+        }
+        __syncthreads(); // J and claimed are rewritten by the next claim
+    }
 }
 
 } // namespace zqd

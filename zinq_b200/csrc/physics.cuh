@@ -356,54 +356,223 @@ __device__ __forceinline__ void eigh2_dev(const double* V, double* W, double* U)
     U[3] = z22;
 }
 
-// cyclic Jacobi for 3 <= n <= MAX_S; ascending, largest-|component| positive
-template <int N> __device__ __noinline__ void eigh_jacobi_dev(const double* V, double* W, double* U) {
-    double A[N * N], Z[N * N];
-    for (int i = 0; i < N * N; ++i) {
-        A[i] = V[i];
-        Z[i] = 0;
+// LAPACK dsyevd('V', 'U') for 3 <= n <= 4, as the reference's eighBatch calls it
+// (src/linear_algebra.zig:55-70, LAPACKE_dsyevd row-major on a symmetric matrix), restated from the
+// published netlib algorithm: dsytd2 (Householder reduction of the upper triangle, last column
+// first), dsteqr('I') (implicit QL or QR, 2 x 2 blocks by dlaev2, selection sort) and dorm2l (the
+// reflectors applied to the tridiagonal eigenvectors); so the eigenvector signs are LAPACK's.
+// Every multiply and add is rounded on its own, in the published order.
+namespace lapack_dev {
+constexpr double EPS = 1.1102230246251565404e-16, SAFMIN = 2.2250738585072014e-308;
+__device__ __forceinline__ double sgn(double a, double b) { return b >= 0 ? fabs(a) : -fabs(a); }
+__device__ __forceinline__ double dlapy2(double x, double y) {
+    const double xa = fabs(x), ya = fabs(y), w = fmax(xa, ya), z = fmin(xa, ya);
+    if (z == 0.0 || w > 1.7976931348623157e308) return w;
+    const double q = z / w;
+    return __dmul_rn(w, sqrt(__dadd_rn(1.0, __dmul_rn(q, q))));
+}
+// dlartg (LAPACK >= 3.10): c >= 0, r carries the sign of f
+__device__ __forceinline__ void dlartg(double f, double g, double& c, double& s, double& r) {
+    const double rtmin = 1.4916681462400413e-154, rtmax = 4.740375954054589e153; // sqrt(safmin), sqrt(safmax/2)
+    const double f1 = fabs(f), g1 = fabs(g);
+    if (g == 0.0) {
+        c = 1.0;
+        s = 0.0;
+        r = f;
+    } else if (f == 0.0) {
+        c = 0.0;
+        s = sgn(1.0, g);
+        r = g1;
+    } else if (f1 > rtmin && f1 < rtmax && g1 > rtmin && g1 < rtmax) {
+        const double d = sqrt(__dadd_rn(__dmul_rn(f, f), __dmul_rn(g, g)));
+        c = f1 / d;
+        r = sgn(d, f);
+        s = g / r;
+    } else {
+        const double u = fmin(1.0 / SAFMIN, fmax(SAFMIN, fmax(f1, g1)));
+        const double fs = f / u, gs = g / u, d = sqrt(__dadd_rn(__dmul_rn(fs, fs), __dmul_rn(gs, gs)));
+        c = fabs(fs) / d;
+        r = sgn(d, f);
+        s = gs / r;
+        r = __dmul_rn(r, u);
     }
-    for (int i = 0; i < N; ++i) Z[i * N + i] = 1;
-    for (int sweep = 0; sweep < 64; ++sweep) {
-        double off = 0, diag = 0;
-        for (int i = 0; i < N; ++i)
-            for (int j = 0; j < N; ++j) {
-                double a2 = __dmul_rn(A[i * N + j], A[i * N + j]);
-                if (i != j) off = __dadd_rn(off, a2);
-                else diag = __dadd_rn(diag, a2);
-            }
-        if (off <= 1e-36 * diag || off == 0.0) break;
-        for (int p = 0; p < N - 1; ++p)
-            for (int q = p + 1; q < N; ++q) {
-                double apq = A[p * N + q];
-                if (apq == 0.0) continue;
-                double app = A[p * N + p], aqq = A[q * N + q];
-                double theta = __dsub_rn(aqq, app) / __dmul_rn(2.0, apq);
-                double t = (theta >= 0 ? 1.0 : -1.0) / __dadd_rn(fabs(theta), sqrt(__dadd_rn(__dmul_rn(theta, theta), 1.0)));
-                double c = 1.0 / sqrt(__dadd_rn(__dmul_rn(t, t), 1.0)), s = __dmul_rn(t, c);
-                for (int k = 0; k < N; ++k) {
-                    double akp = A[k * N + p], akq = A[k * N + q];
-                    A[k * N + p] = __dsub_rn(__dmul_rn(c, akp), __dmul_rn(s, akq));
-                    A[k * N + q] = __dadd_rn(__dmul_rn(s, akp), __dmul_rn(c, akq));
-                }
-                for (int k = 0; k < N; ++k) {
-                    double apk = A[p * N + k], aqk = A[q * N + k];
-                    A[p * N + k] = __dsub_rn(__dmul_rn(c, apk), __dmul_rn(s, aqk));
-                    A[q * N + k] = __dadd_rn(__dmul_rn(s, apk), __dmul_rn(c, aqk));
-                }
-                for (int k = 0; k < N; ++k) {
-                    double zkp = Z[k * N + p], zkq = Z[k * N + q];
-                    Z[k * N + p] = __dsub_rn(__dmul_rn(c, zkp), __dmul_rn(s, zkq));
-                    Z[k * N + q] = __dadd_rn(__dmul_rn(s, zkp), __dmul_rn(c, zkq));
-                }
-            }
+}
+// dlasr('R', 'V', forward or backward) on columns j0 .. j0+nc-1 of Z (N x N, row-major)
+template <int N>
+__device__ __forceinline__ void dlasr_rv(bool forward, int j0, int nc, const double* c, const double* s, double* Z) {
+    for (int jj = 0; jj < nc - 1; ++jj) {
+        const int j = forward ? jj : nc - 2 - jj;
+        const double ct = c[j], st = s[j];
+        if (ct == 1.0 && st == 0.0) continue;
+        for (int i = 0; i < N; ++i) {
+            const double t = Z[i * N + j0 + j + 1], a = Z[i * N + j0 + j];
+            Z[i * N + j0 + j + 1] = __dsub_rn(__dmul_rn(ct, t), __dmul_rn(st, a));
+            Z[i * N + j0 + j] = __dadd_rn(__dmul_rn(st, t), __dmul_rn(ct, a));
+        }
     }
-    double d[N];
-    for (int i = 0; i < N; ++i) d[i] = A[i * N + i];
-    for (int i = 0; i < N - 1; ++i) {
+}
+// dsteqr('I') on the tridiagonal (d, e); false if it did not converge in 30 n sweeps
+template <int N> __device__ __noinline__ bool dsteqr(double* d, double* e, double* Z) {
+    // sqrt(safmax) / 3 and sqrt(safmin) / eps^2, safmax = 1 / safmin
+    const double eps2 = EPS * EPS, ssfmax = 6.703903964971299e153 / 3.0, ssfmin = 1.4916681462400413e-154 / eps2;
+    for (int i = 0; i < N * N; ++i) Z[i] = 0.0;
+    for (int i = 0; i < N; ++i) Z[i * N + i] = 1.0;
+    double wc[N], ws[N];
+    const int nmaxit = N * 30;
+    int jtot = 0, l1 = 0;
+    while (l1 <= N - 1) {
+        if (l1 > 0) e[l1 - 1] = 0.0;
+        int m = N - 1;
+        for (int mm = l1; mm < N - 1; ++mm) {
+            const double tst = fabs(e[mm]);
+            if (tst == 0.0) {
+                m = mm;
+                break;
+            }
+            if (tst <= __dmul_rn(__dmul_rn(sqrt(fabs(d[mm])), sqrt(fabs(d[mm + 1]))), EPS)) {
+                e[mm] = 0.0;
+                m = mm;
+                break;
+            }
+        }
+        int l = l1;
+        const int lsv = l, lendsv = m;
+        int lend = m;
+        l1 = m + 1;
+        if (lend == l) continue;
+        double anorm = 0.0;
+        for (int i = l; i <= lend; ++i) anorm = fmax(anorm, fabs(d[i]));
+        for (int i = l; i < lend; ++i) anorm = fmax(anorm, fabs(e[i]));
+        if (anorm == 0.0) continue;
+        double to = 0.0;
+        if (anorm > ssfmax) to = ssfmax;
+        if (anorm < ssfmin) to = ssfmin;
+        if (to != 0.0) {
+            for (int i = l; i <= lend; ++i) d[i] = __dmul_rn(d[i], to / anorm);
+            for (int i = l; i < lend; ++i) e[i] = __dmul_rn(e[i], to / anorm);
+        }
+        if (fabs(d[lend]) < fabs(d[l])) {
+            lend = lsv;
+            l = lendsv;
+        }
+        if (lend > l) { // QL
+            for (;;) {
+                int mq = lend;
+                for (int mm = l; mm < lend; ++mm) {
+                    const double tst = __dmul_rn(fabs(e[mm]), fabs(e[mm]));
+                    if (tst <= __dadd_rn(__dmul_rn(__dmul_rn(eps2, fabs(d[mm])), fabs(d[mm + 1])), SAFMIN)) {
+                        mq = mm;
+                        break;
+                    }
+                }
+                if (mq < lend) e[mq] = 0.0;
+                double p = d[l];
+                if (mq == l) {
+                    d[l] = p;
+                    if (++l <= lend) continue;
+                    break;
+                }
+                if (mq == l + 1) {
+                    double rt1, rt2, c, s;
+                    dlaev2_dev(d[l], e[l], d[l + 1], rt1, rt2, c, s);
+                    wc[0] = c;
+                    ws[0] = s;
+                    dlasr_rv<N>(false, l, 2, wc, ws, Z);
+                    d[l] = rt1;
+                    d[l + 1] = rt2;
+                    e[l] = 0.0;
+                    l += 2;
+                    if (l <= lend) continue;
+                    break;
+                }
+                if (jtot == nmaxit) break;
+                ++jtot;
+                double g = __dsub_rn(d[l + 1], p) / __dmul_rn(2.0, e[l]);
+                double r = dlapy2(g, 1.0);
+                g = __dadd_rn(__dsub_rn(d[mq], p), e[l] / __dadd_rn(g, sgn(r, g)));
+                double s = 1.0, c = 1.0;
+                p = 0.0;
+                for (int i = mq - 1; i >= l; --i) {
+                    const double f = __dmul_rn(s, e[i]), b = __dmul_rn(c, e[i]);
+                    dlartg(g, f, c, s, r);
+                    if (i != mq - 1) e[i + 1] = r;
+                    g = __dsub_rn(d[i + 1], p);
+                    r = __dadd_rn(__dmul_rn(__dsub_rn(d[i], g), s), __dmul_rn(__dmul_rn(2.0, c), b));
+                    p = __dmul_rn(s, r);
+                    d[i + 1] = __dadd_rn(g, p);
+                    g = __dsub_rn(__dmul_rn(c, r), b);
+                    wc[i - l] = c;
+                    ws[i - l] = -s;
+                }
+                dlasr_rv<N>(false, l, mq - l + 1, wc, ws, Z);
+                d[l] = __dsub_rn(d[l], p);
+                e[l] = g;
+            }
+        } else { // QR
+            for (;;) {
+                int mq = lend;
+                for (int mm = l; mm > lend; --mm) {
+                    const double tst = __dmul_rn(fabs(e[mm - 1]), fabs(e[mm - 1]));
+                    if (tst <= __dadd_rn(__dmul_rn(__dmul_rn(eps2, fabs(d[mm])), fabs(d[mm - 1])), SAFMIN)) {
+                        mq = mm;
+                        break;
+                    }
+                }
+                if (mq > lend) e[mq - 1] = 0.0;
+                double p = d[l];
+                if (mq == l) {
+                    d[l] = p;
+                    if (--l >= lend) continue;
+                    break;
+                }
+                if (mq == l - 1) {
+                    double rt1, rt2, c, s;
+                    dlaev2_dev(d[l - 1], e[l - 1], d[l], rt1, rt2, c, s);
+                    wc[0] = c;
+                    ws[0] = s;
+                    dlasr_rv<N>(true, l - 1, 2, wc, ws, Z);
+                    d[l - 1] = rt1;
+                    d[l] = rt2;
+                    e[l - 1] = 0.0;
+                    l -= 2;
+                    if (l >= lend) continue;
+                    break;
+                }
+                if (jtot == nmaxit) break;
+                ++jtot;
+                double g = __dsub_rn(d[l - 1], p) / __dmul_rn(2.0, e[l - 1]);
+                double r = dlapy2(g, 1.0);
+                g = __dadd_rn(__dsub_rn(d[mq], p), e[l - 1] / __dadd_rn(g, sgn(r, g)));
+                double s = 1.0, c = 1.0;
+                p = 0.0;
+                for (int i = mq; i <= l - 1; ++i) {
+                    const double f = __dmul_rn(s, e[i]), b = __dmul_rn(c, e[i]);
+                    dlartg(g, f, c, s, r);
+                    if (i != mq) e[i - 1] = r;
+                    g = __dsub_rn(d[i], p);
+                    r = __dadd_rn(__dmul_rn(__dsub_rn(d[i + 1], g), s), __dmul_rn(__dmul_rn(2.0, c), b));
+                    p = __dmul_rn(s, r);
+                    d[i] = __dadd_rn(g, p);
+                    g = __dsub_rn(__dmul_rn(c, r), b);
+                    wc[i - mq] = c;
+                    ws[i - mq] = s;
+                }
+                dlasr_rv<N>(true, mq, l - mq + 1, wc, ws, Z);
+                d[l] = __dsub_rn(d[l], p);
+                e[l - 1] = g;
+            }
+        }
+        if (to != 0.0) {
+            for (int i = lsv; i <= lendsv; ++i) d[i] = __dmul_rn(d[i], anorm / to);
+            for (int i = lsv; i < lendsv; ++i) e[i] = __dmul_rn(e[i], anorm / to);
+        }
+        if (jtot >= nmaxit) return false;
+    }
+    for (int ii = 1; ii < N; ++ii) { // selection sort, ascending, swapping eigenvectors
+        const int i = ii - 1;
         int k = i;
         double p = d[i];
-        for (int j = i + 1; j < N; ++j)
+        for (int j = ii; j < N; ++j)
             if (d[j] < p) {
                 k = j;
                 p = d[j];
@@ -412,18 +581,85 @@ template <int N> __device__ __noinline__ void eigh_jacobi_dev(const double* V, d
             d[k] = d[i];
             d[i] = p;
             for (int r = 0; r < N; ++r) {
-                double t = Z[r * N + i];
+                const double t = Z[r * N + i];
                 Z[r * N + i] = Z[r * N + k];
                 Z[r * N + k] = t;
             }
         }
     }
-    for (int m = 0; m < N; ++m) {
-        int big = 0;
-        for (int k = 1; k < N; ++k)
-            if (fabs(Z[k * N + m]) > fabs(Z[big * N + m])) big = k;
-        if (Z[big * N + m] < 0)
-            for (int k = 0; k < N; ++k) Z[k * N + m] = -Z[k * N + m];
+    return true;
+}
+} // namespace lapack_dev
+
+// dsyevd('V', 'U') of the symmetric N x N matrix V (row-major, upper triangle read); W ascending,
+// U[k*N + m] = component k of eigenvector m.  A non-converged case (never seen) leaves NaN.
+template <int N> __device__ __noinline__ void eigh_lapack_dev(const double* V, double* W, double* U) {
+    using namespace lapack_dev;
+    double A[N][N], d[N], e[N], tau[N];
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) A[i][j] = V[i * N + j];
+    for (int i = N - 1; i >= 1; --i) { // dsytd2('U')
+        double alpha = A[i - 1][i], taui = 0.0;
+        if (i > 1) { // dlarfg(i, A(i, i+1), A(1:i-1, i+1))
+            double xn = 0.0;
+            for (int k = 0; k < i - 1; ++k) xn = __dadd_rn(xn, __dmul_rn(A[k][i], A[k][i]));
+            xn = sqrt(xn);
+            if (xn != 0.0) {
+                const double beta = -sgn(dlapy2(alpha, xn), alpha);
+                taui = __dsub_rn(beta, alpha) / beta;
+                const double sc = 1.0 / __dsub_rn(alpha, beta);
+                for (int k = 0; k < i - 1; ++k) A[k][i] = __dmul_rn(A[k][i], sc);
+                alpha = beta;
+            }
+        }
+        A[i - 1][i] = alpha;
+        e[i - 1] = alpha;
+        if (taui != 0.0) {
+            A[i - 1][i] = 1.0;
+            double y[N];
+            for (int k = 0; k < N; ++k) y[k] = 0.0;
+            for (int j = 0; j < i; ++j) { // dsymv('U'): y = taui A v
+                const double t1 = __dmul_rn(taui, A[j][i]);
+                double t2 = 0.0;
+                for (int k = 0; k < j; ++k) {
+                    y[k] = __dadd_rn(y[k], __dmul_rn(t1, A[k][j]));
+                    t2 = __dadd_rn(t2, __dmul_rn(A[k][j], A[k][i]));
+                }
+                y[j] = __dadd_rn(y[j], __dadd_rn(__dmul_rn(t1, A[j][j]), __dmul_rn(taui, t2)));
+            }
+            double dot = 0.0;
+            for (int k = 0; k < i; ++k) dot = __dadd_rn(dot, __dmul_rn(y[k], A[k][i]));
+            const double al = __dmul_rn(__dmul_rn(-0.5, taui), dot);
+            for (int k = 0; k < i; ++k) y[k] = __dadd_rn(y[k], __dmul_rn(al, A[k][i]));
+            for (int j = 0; j < i; ++j) // dsyr2('U'): A -= v w' + w v'
+                if (A[j][i] != 0.0 || y[j] != 0.0) {
+                    const double t1 = -y[j], t2 = -A[j][i];
+                    for (int k = 0; k <= j; ++k)
+                        A[k][j] = __dadd_rn(A[k][j], __dadd_rn(__dmul_rn(A[k][i], t1), __dmul_rn(y[k], t2)));
+                }
+            A[i - 1][i] = e[i - 1];
+        }
+        d[i] = A[i][i];
+        tau[i - 1] = taui;
+    }
+    d[0] = A[0][0];
+    double Z[N * N];
+    if (!dsteqr<N>(d, e, Z)) {
+        for (int i = 0; i < N; ++i) W[i] = nan("");
+        for (int i = 0; i < N * N; ++i) U[i] = nan("");
+        return;
+    }
+    for (int i = 1; i <= N - 1; ++i) { // dorm2l('L', 'N'): Z(1:i, :) <- H(i) Z(1:i, :)
+        const double t = tau[i - 1];
+        if (t == 0.0) continue;
+        double v[N];
+        for (int k = 0; k < i - 1; ++k) v[k] = A[k][i];
+        v[i - 1] = 1.0;
+        for (int c = 0; c < N; ++c) {
+            double w = 0.0;
+            for (int k = 0; k < i; ++k) w = __dadd_rn(w, __dmul_rn(Z[k * N + c], v[k]));
+            for (int k = 0; k < i; ++k) Z[k * N + c] = __dsub_rn(Z[k * N + c], __dmul_rn(__dmul_rn(t, v[k]), w));
+        }
     }
     for (int i = 0; i < N; ++i) W[i] = d[i];
     for (int i = 0; i < N * N; ++i) U[i] = Z[i];
@@ -436,7 +672,7 @@ template <int S> __device__ __forceinline__ void eigh_dev(const double* V, doubl
     } else if constexpr (S == 2) {
         eigh2_dev(V, W, U);
     } else {
-        eigh_jacobi_dev<S>(V, W, U);
+        eigh_lapack_dev<S>(V, W, U);
     }
 }
 

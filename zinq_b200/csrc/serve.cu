@@ -9,6 +9,9 @@
 // of the same shape join (continuous batching).  Other requests run on their own.  After every
 // launch the new observable rows of each job are posted as events (zqd_server_poll); completion,
 // failure and cancellation are events too, and zqd_server_wait hands the result over.
+// 1-D single-solve requests whose line fits one CTA go to the persistent line-service kernel
+// instead (service.h): resident CTAs claim them from a table in pinned memory as they are posted
+// and publish every row; a poller thread streams those rows and completes the requests.
 // The reference has no serving layer: this is the request loop around its quantum_dynamics.run.
 #include <algorithm>
 #include <atomic>
@@ -18,12 +21,15 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <map>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 
 #include "internal.h"
 #include "job.h"
 #include "line_kernel.cuh"
+#include "service.h"
 
 namespace {
 
@@ -76,26 +82,54 @@ uint64_t group_key(const zqd::Opts& o) {
     return 1 + ((uint64_t)o.npoint << 8) + ((uint64_t)o.pot_ns << 2) + ((uint64_t)o.precision << 1);
 }
 
-// every finite entry of the recorded columns (the others are NaN by design) of new rows
-bool rows_finite(const zqd_obs_rows& r, int d, int S, uint32_t wmask) {
+// The first non-finite entry of the recorded columns (the others are NaN by design) of new rows,
+// described for the error message; empty when every entry is finite.
+std::string nonfinite_entry(const zqd_obs_rows& r, int d, int S, uint32_t wmask) {
     const zqd::RowLayout L{d, S};
     for (uint32_t k = 0; k < r.nrows; ++k) {
         const double* row = r.rows + (size_t)k * r.width;
-        if ((wmask & ZQD_WRITE_NORM) && !std::isfinite(row[L.norm()])) return false;
+        int col = -1;
+        if ((wmask & ZQD_WRITE_NORM) && !std::isfinite(row[L.norm()])) col = L.norm();
         if (wmask & ZQD_WRITE_POPULATION)
-            for (int s = 0; s < S; ++s)
-                if (!std::isfinite(row[L.pop() + s])) return false;
+            for (int s = 0; s < S && col < 0; ++s)
+                if (!std::isfinite(row[L.pop() + s])) col = L.pop() + s;
+        if (col >= 0)
+            return "NON-FINITE OBSERVABLE (step " + std::to_string(r.first_row + k) + ", row column " +
+                   std::to_string(col) + ": " + std::to_string(row[col]) + ")";
     }
-    return true;
+    return std::string();
 }
 
 } // namespace
+
+// a request running on the persistent line-service kernel
+struct SvcJob {
+    Req q;
+    zqd::LineServiceHost* host = nullptr;
+    unsigned slot = 0;
+    int streamed = 0; // rows already posted as events
+};
+
+// service tables per (precision, states, threads per CTA, shared memory per CTA)
+using SvcKey = std::tuple<int, int, int, size_t>;
 
 struct zqd_server {
     int device = 0;
     size_t budget = 0, in_use = 0, peak = 0;
     uint32_t max_batch = 16, stream_steps = 256, max_events = 65536;
     bool stream_rows = true;
+    // persistent line service: one table per (precision, states), guarded by svc_mu
+    bool use_service = true;
+    uint32_t service_ctas = 0;
+    double service_idle_us = 200.0;
+    std::mutex svc_mu;
+    std::condition_variable svc_cv;
+    std::map<SvcKey, std::unique_ptr<zqd::LineServiceHost>> svc;
+    std::vector<SvcJob> svc_jobs;
+    bool svc_stop = false;
+    std::thread svc_thread;
+    bool try_service(const Req& q); // true: the service took the request (or it failed there); false: keep it
+    void service_loop();
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Req> queue;
@@ -107,18 +141,25 @@ struct zqd_server {
     zqd_server_stats stats{};
     std::vector<std::thread> workers;
 
+    mutable size_t free_bytes = 0; // device memory free at free_at
+    mutable Clock::time_point free_at{};
     bool fits(const Request& q) const; // under mu
     void work();
     void run_active(std::vector<Req> group);
     void post(Event&& e);                           // under mu
     void finish(const Req& q, int status, const std::string& err, zqd_result* res); // takes mu
-    void stream(const Req& q);
+    int stream(const Req& q, std::string& err); // ZQD_ERR_NUMERIC (err says where) for a non-finite row
 };
 
 bool zqd_server::fits(const Request& q) const {
     if (in_use + q.est > budget) return false;
     if (in_use == 0) return true; // nothing of ours to wait for: the allocation decides
-    return q.est + q.est / 8 <= zqd::device_free_bytes();
+    const Clock::time_point now = Clock::now();
+    if (now - free_at > std::chrono::milliseconds(1)) { // measured at most once a millisecond
+        free_bytes = zqd::device_free_bytes();
+        free_at = now;
+    }
+    return q.est + q.est / 8 <= free_bytes;
 }
 
 void zqd_server::post(Event&& e) {
@@ -157,11 +198,12 @@ void zqd_server::finish(const Req& q, int status, const std::string& err, zqd_re
 }
 
 // the job's observable rows recorded since the last call, as events
-void zqd_server::stream(const Req& q) {
+int zqd_server::stream(const Req& q, std::string& err) {
     for (;;) {
         zqd_obs_rows r{};
-        if (zqd_job_observables(q->job, &r) != ZQD_OK || r.nrows == 0) return;
-        if (!rows_finite(r, (int)q->o.ndim, q->o.pot_ns, q->o.write_mask)) throw ZQD_ERR_NUMERIC;
+        if (zqd_job_observables(q->job, &r) != ZQD_OK || r.nrows == 0) return ZQD_OK;
+        err = nonfinite_entry(r, (int)q->o.ndim, q->o.pot_ns, q->o.write_mask);
+        if (!err.empty()) return ZQD_ERR_NUMERIC;
         Event e;
         e.ticket = q->ticket;
         e.solve = r.solve;
@@ -243,12 +285,7 @@ void zqd_server::run_active(std::vector<Req> group) {
             int rc = q->status;
             int finished = 0;
             if (!rc) {
-                try {
-                    stream(q);
-                } catch (int e) {
-                    rc = e;
-                    q->error = "NON-FINITE OBSERVABLE (the wavefunction norm or a population is NaN or Inf)";
-                }
+                rc = stream(q, q->error);
                 zqd_job_progress(q->job, nullptr, nullptr, &finished);
             }
             if (!rc && !finished) {
@@ -302,6 +339,120 @@ void zqd_server::run_active(std::vector<Req> group) {
     cudaStreamDestroy(st);
 }
 
+// Single-solve 1-D requests whose line fits one CTA: created with the single-CTA shape and posted
+// to the service table of their (precision, states).  False: the request stays with the worker.
+bool zqd_server::try_service(const Req& q) {
+    const zqd::Opts& o = q->o;
+    const bool fp32_req = o.precision != ZQD_FP64;
+    if (!use_service || o.ndim != 1 || o.imag_nstate > 1 || o.npoint > (fp32_req ? 2048u : 1024u)) return false;
+    zqd::ShapeOverride one;
+    one.C = 1;
+    one.lrmax = 2;
+    zqd_job* J = nullptr;
+    zqd::Opts copy = o;
+    if (const int rc = zqd::job_create_shaped(std::move(copy), one, &J)) {
+        if (rc == ZQD_ERR_UNSUPPORTED) return false; // the line does not fit one CTA: the general path
+        finish(q, rc, zqd::last_error(), nullptr);   // e.g. device memory refused: the request fails here
+        return true;
+    }
+    if (J->C != 1 || J->lrmax != 2) {
+        zqd_job_destroy(J);
+        return false;
+    }
+    // the job's shape, rounded up: threads to a power of two (>= 64), shared memory to 16 KiB
+    int threads = 64;
+    while (threads < J->threads) threads <<= 1;
+    const size_t smem = (J->smem + 16383) / 16384 * 16384;
+    std::lock_guard<std::mutex> lk(svc_mu);
+    auto& host = svc[SvcKey{J->fp32 ? 1 : 0, J->S, threads, smem}];
+    if (!host) {
+        host.reset(new zqd::LineServiceHost(J->fp32, J->S, threads, smem));
+        if (host->init(1024, service_ctas, service_idle_us)) {
+            host.reset();
+            zqd_job_destroy(J);
+            return false;
+        }
+    }
+    unsigned slot = 0;
+    if (host->free_slots() == 0 || host->post(J, &slot)) {
+        zqd_job_destroy(J);
+        return false;
+    }
+    q->job = J;
+    svc_jobs.push_back(SvcJob{q, host.get(), slot, 0});
+    svc_cv.notify_one();
+    return true;
+}
+
+// Streams the rows the service kernels publish and completes their requests.  The table's state
+// (post, release, launches) changes under svc_mu; the rows and end flags are read from pinned memory
+// and the copies and result downloads run without the lock, so workers can post meanwhile.
+void zqd_server::service_loop() {
+    cudaSetDevice(device);
+    const int batch_rows = stream_steps ? (int)stream_steps : INT32_MAX;
+    for (;;) {
+        std::vector<SvcJob> snap;
+        {
+            std::unique_lock<std::mutex> lk(svc_mu);
+            if (svc_jobs.empty()) {
+                if (svc_stop) return;
+                svc_cv.wait_for(lk, std::chrono::milliseconds(5));
+                continue;
+            }
+            snap = svc_jobs;
+        }
+        bool progressed = false;
+        std::vector<std::pair<Req, int>> streamed;                                  // new streamed counts
+        std::vector<std::tuple<SvcJob, int, std::string, zqd_result*>> ended_jobs; // to complete
+        for (SvcJob& sj : snap) {
+            const int rows = sj.host->rows(sj.slot);
+            const bool ended = sj.host->ended(sj.slot);
+            int rc = ZQD_OK;
+            std::string err;
+            if (ended) rc = zqd::service_job_ended(sj.q->job);
+            else zqd::service_job_rows(sj.q->job, rows);
+            if (!rc && (ended || rows - sj.streamed >= batch_rows)) { // rows in pieces of stream_steps
+                progressed = true;
+                rc = stream(sj.q, err);
+                streamed.emplace_back(sj.q, rows);
+            }
+            if (!ended) continue; // runs on until its solve ends, even when cancelled
+            zqd_result* res = nullptr;
+            if (!rc && (rc = zqd_job_result(sj.q->job, &res))) err = zqd::last_error();
+            if (!rc) {
+                zqd_observables ob{};
+                zqd_result_final(res, 0, &ob);
+                if (!std::isfinite(ob.norm)) {
+                    rc = ZQD_ERR_NUMERIC;
+                    err = "NON-FINITE OBSERVABLE (the wavefunction norm is NaN or Inf)";
+                }
+            }
+            if (!rc && sj.q->cancel.load()) rc = ZQD_ERR_CANCELLED, err = "CANCELLED";
+            if (rc && res) {
+                zqd_result_destroy(res);
+                res = nullptr;
+            }
+            zqd_job_destroy(sj.q->job);
+            sj.q->job = nullptr;
+            ended_jobs.emplace_back(sj, rc, err, res);
+        }
+        {
+            std::lock_guard<std::mutex> lk(svc_mu);
+            for (auto& p : streamed)
+                for (SvcJob& sj : svc_jobs)
+                    if (sj.q == p.first) sj.streamed = p.second;
+            for (auto& e : ended_jobs) {
+                const SvcJob& sj = std::get<0>(e);
+                sj.host->release(sj.slot);
+                svc_jobs.erase(std::find_if(svc_jobs.begin(), svc_jobs.end(), [&](const SvcJob& x) { return x.q == sj.q; }));
+            }
+            for (auto& kv : svc) kv.second->pump(); // relaunch while posted jobs wait unclaimed
+        }
+        for (auto& e : ended_jobs) finish(std::get<0>(e).q, std::get<1>(e), std::get<2>(e), std::get<3>(e));
+        if (!progressed && ended_jobs.empty()) std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+}
+
 void zqd_server::work() {
     cudaSetDevice(device);
     for (;;) {
@@ -313,8 +464,19 @@ void zqd_server::work() {
             // the head, then waiting requests of its shape while they fit (arrival order)
             Req head = queue.front();
             queue.pop_front();
-            batch.push_back(head);
             in_use += head->est;
+            peak = std::max(peak, in_use);
+            stats.peak_device_bytes = peak;
+            head->state = State::Running;
+            if (!queue.empty()) cv_work.notify_one();
+            lk.unlock();
+            if (try_service(head)) {
+                std::lock_guard<std::mutex> lk2(mu);
+                ++stats.service_jobs;
+                continue;
+            }
+            lk.lock();
+            batch.push_back(head);
             if (head->group_key)
                 for (auto it = queue.begin(); it != queue.end() && batch.size() < max_batch;) {
                     if ((*it)->group_key == head->group_key && fits(**it)) {
@@ -343,6 +505,9 @@ extern "C" void zqd_server_config_init(zqd_server_config* cfg) {
     cfg->stream_steps = 256;
     cfg->stream_rows = 1;
     cfg->max_events = 65536;
+    cfg->persistent_lines = 1;
+    cfg->service_ctas = 64;
+    cfg->service_idle_us = 200.0;
 }
 
 extern "C" int zqd_server_create(const zqd_server_config* cfg, zqd_server** out) {
@@ -362,6 +527,10 @@ extern "C" int zqd_server_create(const zqd_server_config* cfg, zqd_server** out)
     S->stream_rows = cfg->stream_rows != 0;
     S->max_events = std::max(1u, cfg->max_events ? cfg->max_events : 65536u);
     S->stats.device_budget_bytes = S->budget;
+    S->use_service = cfg->persistent_lines != 0;
+    S->service_ctas = cfg->service_ctas;
+    S->service_idle_us = cfg->service_idle_us > 0 ? cfg->service_idle_us : 200.0;
+    S->svc_thread = std::thread([s = S.get()] { s->service_loop(); });
     const uint32_t nw = std::max(1u, cfg->workers ? cfg->workers : 4u);
     for (uint32_t i = 0; i < nw; ++i) S->workers.emplace_back([s = S.get()] { s->work(); });
     *out = S.release();
@@ -466,11 +635,17 @@ extern "C" int zqd_server_poll(zqd_server* S, zqd_event* events, uint32_t max_ev
 
 extern "C" int zqd_server_stats_get(zqd_server* S, zqd_server_stats* out) {
     if (!S || !out) return zqd::fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    uint64_t launches = 0;
+    {
+        std::lock_guard<std::mutex> lk(S->svc_mu);
+        for (auto& kv : S->svc) launches += kv.second->launches();
+    }
     std::lock_guard<std::mutex> lk(S->mu);
     *out = S->stats;
     out->device_bytes_in_use = S->in_use;
     out->queued = S->queue.size();
     out->pending_events = S->events.size();
+    out->service_launches = launches;
     return ZQD_OK;
 }
 
@@ -482,5 +657,11 @@ extern "C" void zqd_server_destroy(zqd_server* S) {
     }
     S->cv_work.notify_all();
     for (std::thread& t : S->workers) t.join();
+    {
+        std::lock_guard<std::mutex> lk(S->svc_mu);
+        S->svc_stop = true;
+    }
+    S->svc_cv.notify_all();
+    if (S->svc_thread.joinable()) S->svc_thread.join(); // every service request has completed
     delete S;
 }

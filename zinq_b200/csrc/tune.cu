@@ -120,6 +120,14 @@ double time_shape(int d, int n, int S, bool fp32, const ShapeOverride& cand) {
 
 } // namespace
 
+int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out) {
+    t_forcing = true;
+    t_forced = shape;
+    const int rc = job_create_opts(std::move(o), out);
+    t_forcing = false;
+    return rc;
+}
+
 bool lookup_shape(int d, int n, int S, bool fp32, ShapeOverride& out) {
     if (t_forcing) {
         out = t_forced;

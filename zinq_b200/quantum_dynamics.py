@@ -449,12 +449,15 @@ class Server:
     wait() returns (Result, latency in ms from submission to completion)."""
 
     def __init__(self, workers: int = 4, max_batch: int = 16, device_budget_bytes: int = 0, stream_steps: int = 256,
-                 stream_rows: bool = True, max_events: int = 65536):
+                 stream_rows: bool = True, max_events: int = 65536, persistent_lines: bool = True,
+                 service_ctas: int = 64, service_idle_us: float = 200.0):
         self._L = _abi.load()
         cfg = _abi.ZqdServerConfig()
         self._L.zqd_server_config_init(C.byref(cfg))
         cfg.workers, cfg.max_batch, cfg.device_budget_bytes = workers, max_batch, device_budget_bytes
         cfg.stream_steps, cfg.stream_rows, cfg.max_events = stream_steps, int(bool(stream_rows)), max_events
+        cfg.persistent_lines, cfg.service_ctas = int(bool(persistent_lines)), service_ctas
+        cfg.service_idle_us = service_idle_us
         self._h = C.c_void_p()
         check(self._L.zqd_server_create(C.byref(cfg), C.byref(self._h)))
         self._shapes = {}
@@ -518,14 +521,15 @@ class Server:
             pass
 
 
-def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers: int = 4, max_batch: int = 16):
+def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers: int = 4, max_batch: int = 16,
+                 **server_kw):
     """Submits opts[i] at arrivals_s[i] seconds after the start (a feeder thread sleeps until each
     arrival), waits for all; returns (results, latencies_ms, wall_s from the first arrival to the
     last completion, server stats)."""
     import threading
     import time
 
-    srv = Server(workers=workers, max_batch=max_batch)
+    srv = Server(workers=workers, max_batch=max_batch, **server_kw)
     tickets = [None] * len(opts)
     errors = []
     t0 = time.perf_counter()
