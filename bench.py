@@ -389,12 +389,22 @@ def serving_leg(qd):
                      "grouped_launches": st["grouped_launches"], "grouped_jobs": st["grouped_jobs"],
                      "joined_jobs": st["joined_jobs"], "service_jobs": st["service_jobs"],
                      "service_launches": st["service_launches"], "peak_device_bytes": st["peak_device_bytes"]}
-        pops[prec] = [r.observables[0].history["population"] for r in res]
-        forms[prec] = [r.precision for r in res]
-    errs = [float(np.max(np.abs(a - b))) for a, b in zip(pops["fp32"], pops["fp64"])]
+        out[prec]["failed_jobs"] = len(st["failures"])
+        pops[prec] = [r.observables[0].history["population"] if r is not None else None for r in res]
+        forms[prec] = [r.precision if r is not None else None for r in res]
+    def errs_of(x, y):  # a failed or non-finite job counts as an infinite error, never silently skipped
+        e = []
+        for a, b in zip(x, y):
+            if a is None or b is None or not (np.all(np.isfinite(a)) and np.all(np.isfinite(b))):
+                e.append(float("inf"))
+            else:
+                e.append(float(np.max(np.abs(a - b))))
+        return e
+
+    errs = errs_of(pops["fp32"], pops["fp64"])
     out["pop_err_fp32_vs_fp64"] = max(errs)
     out["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs)
-    errs_auto = [float(np.max(np.abs(a - b))) for a, b in zip(pops["auto"], pops["fp64"])]
+    errs_auto = errs_of(pops["auto"], pops["fp64"])
     out["auto"]["pop_err_vs_fp64"] = max(errs_auto)
     out["auto"]["jobs_over_1e-5"] = sum(e > 1e-5 for e in errs_auto)
     out["auto"]["jobs_fp64"] = sum(f == "fp64" for f in forms["auto"])

@@ -903,14 +903,43 @@ void dsyevd(int n, const double* V, double* W, double* U) {
         // dlarfg(i, A(i, i+1), A(1:i-1, i+1))
         double alpha = A[i - 1][i], taui = 0.0;
         if (i > 1) {
+            // dnrm2 of A(1:i-1, i+1), scaled by the largest magnitude so that tiny couplings do not
+            // underflow (a naive sum of squares of 1e-162 is denormal and breaks the reflector)
+            double big = 0.0;
+            for (int k = 0; k < i - 1; ++k) big = std::max(big, std::fabs(A[k][i]));
             double xnorm = 0.0;
-            for (int k = 0; k < i - 1; ++k) xnorm += A[k][i] * A[k][i];
-            xnorm = std::sqrt(xnorm);
+            if (big > 0.0) {
+                double ssq = 0.0;
+                for (int k = 0; k < i - 1; ++k) {
+                    const double q = A[k][i] / big;
+                    ssq += q * q;
+                }
+                xnorm = big * std::sqrt(ssq);
+            }
             if (xnorm != 0.0) {
-                const double beta = -sign(dlapy2(alpha, xnorm), alpha);
+                double beta = -sign(dlapy2(alpha, xnorm), alpha);
+                // dlarfg's rescaling: while |beta| < safmin / eps, scale x and alpha by eps / safmin
+                const double sfmin = SAFMIN / EPS, rsafmn = 1.0 / sfmin;
+                int knt = 0;
+                if (std::fabs(beta) < sfmin) {
+                    do {
+                        ++knt;
+                        for (int k = 0; k < i - 1; ++k) A[k][i] = A[k][i] * rsafmn;
+                        beta = beta * rsafmn;
+                        alpha = alpha * rsafmn;
+                    } while (std::fabs(beta) < sfmin && knt < 20);
+                    double big2 = 0.0, ssq = 0.0;
+                    for (int k = 0; k < i - 1; ++k) big2 = std::max(big2, std::fabs(A[k][i]));
+                    for (int k = 0; k < i - 1; ++k) {
+                        const double q = A[k][i] / big2;
+                        ssq += q * q;
+                    }
+                    beta = -sign(dlapy2(alpha, big2 * std::sqrt(ssq)), alpha);
+                }
                 taui = (beta - alpha) / beta;
                 const double sc = 1.0 / (alpha - beta);
                 for (int k = 0; k < i - 1; ++k) A[k][i] = A[k][i] * sc;
+                for (int j = 0; j < knt; ++j) beta = beta * sfmin;
                 alpha = beta;
             }
         }

@@ -105,3 +105,15 @@ def test_submit_rejects_invalid_and_oversized_requests():
     with pytest.raises(_abi.ZqdError, match="BUDGET"):
         srv.submit(big, "fp64")
     srv.close()
+
+
+def test_stream_jobs_with_vanishing_three_state_couplings_stay_finite():
+    # three seeded serving jobs whose equal couplings C exp(-r^2) fall to 1e-196 at the grid edge over
+    # degenerate diagonals; a reflector norm that underflowed once made their propagators non-unitary
+    opts, _ = qd.serving_stream(600, seed=7, rate_per_s=200.0, max_steps=1000)
+    for i in (54, 124, 499):
+        o = dict(opts[i], iterations=600 if i != 124 else opts[i]["iterations"])
+        a = qd.run(o, precision="fp32", want_wavefunction=False).observables[0].history["population"]
+        b = qd.run(o, precision="fp64", want_wavefunction=False).observables[0].history["population"]
+        assert np.all(np.isfinite(a)) and np.all(np.isfinite(b))
+        assert np.max(np.abs(a - b)) <= 1e-5

@@ -71,6 +71,25 @@ def test_eigh_matches_oracle(n):
         np.testing.assert_allclose(U[i] @ np.diag(W[i]) @ U[i].T, A[i], atol=1e-15)
 
 
+@pytest.mark.parametrize("n", [3, 4])
+def test_eigh_orthonormal_at_every_coupling_scale(n):
+    # equal couplings from 1e-1 down to denormals over (partly) degenerate diagonals, as on the far
+    # edges of coupled-surface grids: eigenvectors orthonormal and equal to the oracle's
+    rng = np.random.default_rng(40 + n)
+    count = 3000
+    d = rng.standard_normal((count, n)) * 1e-3
+    d[::5, 1] = d[::5, 0]
+    sc = 10.0 ** rng.uniform(-320, -1, count)
+    A = np.einsum("ki,ij->kij", d, np.eye(n)) + sc[:, None, None] * (np.ones((n, n)) - np.eye(n))
+    L = _abi.load()
+    W, U = np.zeros((count, n)), np.zeros((count, n, n))
+    _abi.check(L.zqd_eigh_batch(n, count, dptr(np.ascontiguousarray(A)), dptr(W), dptr(U)))
+    for i in range(count):
+        assert np.max(np.abs(U[i] @ U[i].T - np.eye(n))) <= 1e-14, A[i]
+        wo, uo = qd_ref.eigh(A[i])
+        np.testing.assert_allclose(U[i], uo, atol=1e-14)
+
+
 @pytest.mark.parametrize("n", [2, 3, 4])
 def test_eigh_signs_match_lapack(n):
     # numpy.linalg.eigh calls LAPACK ?syevd, the routine the reference uses (src/linear_algebra.zig:67);

@@ -48,3 +48,22 @@ def test_eigh_of_the_three_state_workload_potential_matches_lapack():
             wo, Uo = qd_ref.eigh(V)
             assert np.max(np.abs(U - Uo)) <= 1e-11, (x, y)
     assert compared > 1000
+
+
+def test_eigenvectors_stay_orthonormal_at_every_coupling_scale():
+    # couplings from 1e-1 down to denormals, with exactly degenerate diagonals: the reflector norm is
+    # scaled and dlarfg rescales tiny betas (a naive sum of squares underflows and breaks orthogonality)
+    rng = np.random.default_rng(3)
+    for k in range(6000):
+        n = 3 if k % 2 else 4
+        d = rng.standard_normal(n) * 1e-3
+        if k % 5 == 0:
+            d[rng.integers(n)] = d[0]
+        sc = 10.0 ** rng.uniform(-320, -1)
+        A = np.diag(d) + sc * rng.choice([-1, 1]) * (np.ones((n, n)) - np.eye(n))
+        if k % 3 == 0:
+            A = np.diag(d) + sc * rng.standard_normal((n, n))
+            A = (A + A.T) / 2
+        W, U = qd_ref.eigh(A)
+        assert np.max(np.abs(U @ U.T - np.eye(n))) <= 1e-14, A
+        assert np.max(np.abs(U @ np.diag(W) @ U.T - A)) <= 1e-15 + 1e-14 * np.max(np.abs(A))

@@ -601,14 +601,42 @@ template <int N> __device__ __noinline__ void eigh_lapack_dev(const double* V, d
     for (int i = N - 1; i >= 1; --i) { // dsytd2('U')
         double alpha = A[i - 1][i], taui = 0.0;
         if (i > 1) { // dlarfg(i, A(i, i+1), A(1:i-1, i+1))
+            // dnrm2 scaled by the largest magnitude: tiny couplings must not underflow to denormals
+            double big = 0.0;
+            for (int k = 0; k < i - 1; ++k) big = fmax(big, fabs(A[k][i]));
             double xn = 0.0;
-            for (int k = 0; k < i - 1; ++k) xn = __dadd_rn(xn, __dmul_rn(A[k][i], A[k][i]));
-            xn = sqrt(xn);
+            if (big > 0.0) {
+                double ssq = 0.0;
+                for (int k = 0; k < i - 1; ++k) {
+                    const double q = A[k][i] / big;
+                    ssq = __dadd_rn(ssq, __dmul_rn(q, q));
+                }
+                xn = __dmul_rn(big, sqrt(ssq));
+            }
             if (xn != 0.0) {
-                const double beta = -sgn(dlapy2(alpha, xn), alpha);
+                double beta = -sgn(dlapy2(alpha, xn), alpha);
+                // dlarfg's rescaling: while |beta| < safmin / eps, scale x and alpha by eps / safmin
+                const double sfmin = SAFMIN / EPS, rsafmn = 1.0 / sfmin;
+                int knt = 0;
+                if (fabs(beta) < sfmin) {
+                    do {
+                        ++knt;
+                        for (int k = 0; k < i - 1; ++k) A[k][i] = __dmul_rn(A[k][i], rsafmn);
+                        beta = __dmul_rn(beta, rsafmn);
+                        alpha = __dmul_rn(alpha, rsafmn);
+                    } while (fabs(beta) < sfmin && knt < 20);
+                    double big2 = 0.0, ssq = 0.0;
+                    for (int k = 0; k < i - 1; ++k) big2 = fmax(big2, fabs(A[k][i]));
+                    for (int k = 0; k < i - 1; ++k) {
+                        const double q = A[k][i] / big2;
+                        ssq = __dadd_rn(ssq, __dmul_rn(q, q));
+                    }
+                    beta = -sgn(dlapy2(alpha, __dmul_rn(big2, sqrt(ssq))), alpha);
+                }
                 taui = __dsub_rn(beta, alpha) / beta;
                 const double sc = 1.0 / __dsub_rn(alpha, beta);
                 for (int k = 0; k < i - 1; ++k) A[k][i] = __dmul_rn(A[k][i], sc);
+                for (int j = 0; j < knt; ++j) beta = __dmul_rn(beta, sfmin);
                 alpha = beta;
             }
         }

@@ -525,7 +525,8 @@ def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers:
                  **server_kw):
     """Submits opts[i] at arrivals_s[i] seconds after the start (a feeder thread sleeps until each
     arrival), waits for all; returns (results, latencies_ms, wall_s from the first arrival to the
-    last completion, server stats)."""
+    last completion, server stats).  A job that fails leaves None in results and (index, message)
+    in stats["failures"]."""
     import threading
     import time
 
@@ -547,15 +548,20 @@ def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers:
     th = threading.Thread(target=feed)
     th.start()
     results, lats = [None] * len(opts), [0.0] * len(opts)
+    failures = []
     for i in range(len(opts)):
         while tickets[i] is None and th.is_alive():
             time.sleep(0.0005)
         if tickets[i] is None:
             break
-        results[i], lats[i] = srv.wait(tickets[i])
+        try:
+            results[i], lats[i] = srv.wait(tickets[i])
+        except ZqdError as e:  # the job failed alone (e.g. ZQD_ERR_NUMERIC); the others stand
+            failures.append((i, str(e)))
     th.join()
     wall = time.perf_counter() - t0 - (arrivals_s[0] if arrivals_s else 0.0)
     st = srv.stats()
+    st["failures"] = failures
     srv.close()
     if errors:
         raise errors[0]
