@@ -380,9 +380,10 @@ def serving_leg(qd):
            "units": units}
     pops, forms = {}, {}
     for prec in ("fp32", "fp64", "auto"):
-        res, lat, wall, st = qd.serve_stream(opts, arrivals, prec)
+        # the populations are compared; the final wavefunctions are not downloaded
+        res, lat, wall, st = qd.serve_stream(opts, arrivals, prec, fetch_wavefunction=False)
         lat = np.asarray(lat)
-        _, lat_b, wall_b, _ = qd.serve_stream(opts, [0.0] * len(opts), prec)
+        _, lat_b, wall_b, _ = qd.serve_stream(opts, [0.0] * len(opts), prec, fetch_wavefunction=False)
         out[prec] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                      "throughput": units / wall, "unit": UNIT, "wall_s": wall,
                      "burst_throughput": units / wall_b, "burst_wall_s": wall_b,

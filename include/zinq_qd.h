@@ -421,7 +421,7 @@ int zqd_potential_plot(const zqd_options* opt, double time, double* host_U, size
 typedef struct zqd_server zqd_server;
 typedef struct {
     uint32_t struct_size;         /* sizeof(zqd_server_config); set by zqd_server_config_init */
-    uint32_t workers;             /* host threads, each advancing one job or group at a time (default 4) */
+    uint32_t workers;             /* host threads, each advancing one job or group at a time on its own stream (default 8) */
     uint32_t max_batch;           /* jobs per grouped launch (default 16) */
     uint64_t device_budget_bytes; /* 0: 90% of the device memory free at creation */
     uint32_t stream_steps;        /* steps per launch between event posts (default 256; 0: whole jobs) */
@@ -433,6 +433,8 @@ typedef struct {
     uint32_t service_ctas;        /* CTAs alive per service table (default 64, 0: one per SM); a table
                                      per (precision, states, CTA size): small lines share an SM */
     double service_idle_us;       /* a service CTA without work exits after this wait (default 200) */
+    int fetch_wavefunction;       /* results carry the final wavefunction (default 1; 0 saves its download,
+                                     zqd_result_wavefunction then returns ZQD_ERR_NOT_FOUND) */
 } zqd_server_config;
 typedef struct {
     uint64_t submitted, completed, failed, cancelled, queued;

@@ -131,7 +131,7 @@ def test_server_config_defaults_and_no_device_status():
     lib = _abi.load()
     cfg = _abi.ZqdServerConfig()
     lib.zqd_server_config_init(C.byref(cfg))
-    assert cfg.struct_size == C.sizeof(_abi.ZqdServerConfig) and cfg.workers == 4 and cfg.max_batch == 16
+    assert cfg.struct_size == C.sizeof(_abi.ZqdServerConfig) and cfg.workers == 8 and cfg.max_batch == 16
     import torch
 
     if not torch.cuda.is_available():

@@ -89,7 +89,7 @@ class ZqdServerConfig(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("workers", C.c_uint32), ("max_batch", C.c_uint32),
                 ("device_budget_bytes", C.c_uint64), ("stream_steps", C.c_uint32), ("stream_rows", C.c_int),
                 ("max_events", C.c_uint32), ("persistent_lines", C.c_int), ("service_ctas", C.c_uint32),
-                ("service_idle_us", C.c_double)]
+                ("service_idle_us", C.c_double), ("fetch_wavefunction", C.c_int)]
 
 
 class ZqdServerStats(C.Structure):

@@ -21,8 +21,13 @@ const char* last_error();
 // Device buffers of jobs come from the device's stream-ordered memory pool: cudaFree waits for
 // every stream of the device, which would stall concurrent jobs (the server runs several at a
 // time); a pool free waits for nothing.  Freed blocks stay cached in the pool for later jobs.
-cudaError_t dev_alloc(void** p, size_t bytes);
-void dev_free(void* p);
+// With a stream, allocation and free are ordered in that stream (the buffer is usable by work
+// queued there after the call, and by other streams once it has been synchronised); without
+// one, the allocation is complete when the call returns.  A stream that shares a hardware
+// queue with busy streams would make a synchronising call wait for their work too, so jobs
+// allocate in their own stream.
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st = nullptr);
+void dev_free(void* p, cudaStream_t st = nullptr);
 // device memory this process can still allocate: free HBM plus the blocks the pool keeps for reuse
 size_t device_free_bytes();
 
@@ -69,9 +74,12 @@ struct PotStore {
     PotDev dev{};
     void* d_blob = nullptr; // the potential's device data (program, constants or tables) in one block
     size_t bytes = 0;       // uploaded to the device
-    ~PotStore();
+    cudaStream_t st = nullptr; // the stream the block was allocated (and is freed) in
+    void release();
+    ~PotStore() { release(); }
 };
-int build_potential(const Opts& o, PotStore& ps);
+// st: the stream of the job that uses the potential (null: complete on return)
+int build_potential(const Opts& o, PotStore& ps, cudaStream_t st = nullptr);
 
 // Twiddle tables exp(-2 pi i t / n), t < n, generated in long double and rounded.
 std::vector<double> twiddles_f64(int n);

@@ -82,7 +82,7 @@ static int resolve_auto_precision(zqd_job* J) {
     }
     DevBuf out;
     int rc;
-    if ((rc = out.alloc(sizeof(unsigned long long)))) return rc;
+    if ((rc = out.alloc(sizeof(unsigned long long), J->stream))) return rc;
     a.out = out.as<unsigned long long>();
     ZQD_CUDA(cudaMemsetAsync(out.p, 0xff, sizeof(unsigned long long), J->stream)); // above every double's bits
     const unsigned blocks = (unsigned)std::min<size_t>(1024, (J->N + 255) / 256);
@@ -92,6 +92,7 @@ static int resolve_auto_precision(zqd_job* J) {
     default: min_gap_kernel<4><<<blocks, 256, 0, J->stream>>>(a); break;
     }
     ZQD_CUDA(cudaGetLastError());
+    ZQD_CUDA(cudaStreamSynchronize(J->stream)); // the kernel, then the copy into pageable memory
     unsigned long long bits = 0;
     ZQD_CUDA(cudaMemcpyAsync(&bits, out.p, sizeof(bits), cudaMemcpyDeviceToHost, J->stream));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
@@ -370,7 +371,7 @@ template <typename T> static int create_line(zqd_job* J) {
     auto align = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t total = 0;
     for (const auto& pt : parts) total += align(pt.bytes);
-    if ((rc = J->arena.alloc(total))) return rc;
+    if ((rc = J->arena.alloc(total, J->stream))) return rc;
     size_t off = 0;
     for (const auto& pt : parts) {
         pt.b->view(J->arena.as<char>() + off, pt.bytes);
@@ -530,6 +531,9 @@ template <typename T> static int step_line(zqd_job* J, int s, int i0, int i1, in
     ZQD_CUDA(cudaEventRecord(J->ev0, J->stream));
     if (int rc = launch_line_s<T>(&sh, J->jobs.as<LineJob<T>>() + s, 1)) return rc;
     ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
+    // wait first: a copy into pageable memory queued behind the launch would wait inside the driver,
+    // where it can hold up other threads' copies
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
     int flags[2] = {0, 0};
     ZQD_CUDA(cudaMemcpyAsync(&flags[0], J->rows.as<int>() + s, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
     ZQD_CUDA(cudaMemcpyAsync(&flags[1], J->done.as<int>() + s, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
@@ -574,7 +578,9 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     std::vector<double> hist((size_t)J->nsolve * rows * J->hc), fin((size_t)J->nsolve * J->hc);
     std::vector<int> nrows(J->nsolve);
     const size_t SN = (size_t)J->S * J->N;
-    std::vector<cx<T>> save(SN), orth((size_t)(J->nsolve - 1) * SN);
+    // the final wavefunctions are skipped for callers that do not read them (the server's option)
+    const size_t SNw = J->fetch_psi ? SN : 0;
+    std::vector<cx<T>> save(SNw), orth((size_t)(J->nsolve - 1) * SNw);
     const struct {
         void* host;
         const void* dev;
@@ -582,7 +588,7 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
     } parts[] = {{hist.data(), J->hist.p, hist.size() * sizeof(double)},
                  {fin.data(), J->fin.p, fin.size() * sizeof(double)},
                  {nrows.data(), J->rows.p, nrows.size() * sizeof(int)},
-                 {save.data(), J->psi_save.p, SN * sizeof(cx<T>)},
+                 {save.data(), J->psi_save.p, SNw * sizeof(cx<T>)},
                  {orth.data(), J->orth.p, orth.size() * sizeof(cx<T>)}};
     size_t total = 0;
     for (const auto& pt : parts) total += (pt.bytes + 15) & ~(size_t)15;
@@ -630,8 +636,9 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
         }
         if (J->wfn_hist.p && so.rows) { // History.wfn of this solve
             std::vector<cx<T>> w(so.rows * SN);
-            ZQD_CUDA(cudaMemcpy(w.data(), J->wfn_hist.as<cx<T>>() + (size_t)s * rows * SN, w.size() * sizeof(cx<T>),
-                                cudaMemcpyDeviceToHost));
+            ZQD_CUDA(cudaMemcpyAsync(w.data(), J->wfn_hist.as<cx<T>>() + (size_t)s * rows * SN, w.size() * sizeof(cx<T>),
+                                     cudaMemcpyDeviceToHost, J->stream));
+            ZQD_CUDA(cudaStreamSynchronize(J->stream));
             J->d2h += w.size() * sizeof(cx<T>);
             R->d2h = J->d2h;
             so.wfn.resize(2 * w.size());
@@ -646,6 +653,7 @@ template <typename T> static int fetch_line(zqd_job* J, zqd_result* R) {
                     so.wfn[2 * (st * J->N + x) + 1] = (double)w[st * J->N + p].y;
                 }
         }
+        if (!J->fetch_psi) continue;
         const cx<T>* src = (s + 1 < J->nsolve) ? orth.data() + (size_t)s * SN : save.data();
         so.psi.resize(2 * SN);
         if (J->d == 1) {
@@ -743,7 +751,7 @@ extern "C" int zqd_job_create(const zqd_options* opt, zqd_job** out) {
 }
 
 // A job from already copied and validated options (zqd_job_create, the server).
-int zqd::job_create_opts(Opts&& o, zqd_job** out) {
+int zqd::job_create_opts(Opts&& o, zqd_job** out, cudaStream_t stream) {
     *out = nullptr;
     std::unique_ptr<zqd_job> J(new (std::nothrow) zqd_job());
     if (!J) return fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
@@ -759,10 +767,15 @@ int zqd::job_create_opts(Opts&& o, zqd_job** out) {
     J->nsolve = J->o.imag_nstate ? (int)J->o.imag_nstate : 1;
     J->hc = RowLayout{J->d, J->S}.width();
     if (J->d > 1 && J->n < 8) return fail(ZQD_ERR_UNSUPPORTED, "MULTI-DIMENSIONAL GRIDS NEED AT LEAST 8 POINTS PER AXIS");
-    ZQD_CUDA(cudaStreamCreateWithFlags(&J->stream, cudaStreamNonBlocking));
+    if (stream) {
+        J->stream = stream;
+        J->own_stream = false;
+    } else {
+        ZQD_CUDA(cudaStreamCreateWithFlags(&J->stream, cudaStreamNonBlocking));
+    }
     ZQD_CUDA(cudaEventCreate(&J->ev0));
     ZQD_CUDA(cudaEventCreate(&J->ev1));
-    if ((rc = build_potential(J->o, J->pot))) return rc;
+    if ((rc = build_potential(J->o, J->pot, J->stream))) return rc;
     if ((rc = resolve_auto_precision(J.get()))) return rc;
     J->fp32 = J->o.precision == ZQD_FP32_MIXED;
     if (J->d == 1 && (rc = choose_line_shape(J.get()))) return rc;
@@ -1005,14 +1018,14 @@ int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, floa
         if (a->fp32) {
             std::vector<LineJob<float>> d;
             for (zqd_job* J : jobs) d.push_back(line_job_desc<float>(J, 0));
-            if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+            if ((rc = descs.alloc(d.size() * sizeof(d[0]), st))) return rc;
             ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
             ZQD_CUDA(cudaEventRecord(e0, st));
             if ((rc = launch_line_s<float>(&sh, descs.p, (int)jobs.size()))) return rc;
         } else {
             std::vector<LineJob<double>> d;
             for (zqd_job* J : jobs) d.push_back(line_job_desc<double>(J, 0));
-            if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+            if ((rc = descs.alloc(d.size() * sizeof(d[0]), st))) return rc;
             ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
             ZQD_CUDA(cudaEventRecord(e0, st));
             if ((rc = launch_line_s<double>(&sh, descs.p, (int)jobs.size()))) return rc;
@@ -1076,13 +1089,14 @@ int zqd::step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cud
             jobs[k]->h2d += sizeof(LineJob<T>);
         }
         int rc;
-        if ((rc = descs.alloc(d.size() * sizeof(d[0])))) return rc;
+        if ((rc = descs.alloc(d.size() * sizeof(d[0]), st))) return rc;
         ZQD_CUDA(cudaMemcpyAsync(descs.p, d.data(), d.size() * sizeof(d[0]), cudaMemcpyHostToDevice, st));
         if ((rc = launch_line_s<T>(&sh, descs.p, (int)jobs.size()))) return rc;
         return ZQD_OK;
     };
     int rc = a->fp32 ? go(float{}) : go(double{});
     if (rc) return rc;
+    ZQD_CUDA(cudaStreamSynchronize(st)); // the launch first, then the copies into pageable memory
     for (size_t k = 0; k < jobs.size(); ++k) { // rows written and the end flag of every member
         ZQD_CUDA(cudaMemcpyAsync(&flags[2 * k], jobs[k]->rows.p, sizeof(int), cudaMemcpyDeviceToHost, st));
         ZQD_CUDA(cudaMemcpyAsync(&flags[2 * k + 1], jobs[k]->done.p, sizeof(int), cudaMemcpyDeviceToHost, st));

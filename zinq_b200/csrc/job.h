@@ -14,24 +14,28 @@ namespace zqd {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    bool owned = true; // false: a view into another buffer (not freed here)
-    ~DevBuf() {
-        if (owned) dev_free(p);
+    bool owned = true;         // false: a view into another buffer (not freed here)
+    cudaStream_t st = nullptr; // allocated (and freed) in this stream; null: complete on return
+    ~DevBuf() { release(); }
+    void release() {
+        if (owned) dev_free(p, st);
+        p = nullptr;
+        bytes = 0;
     }
     // a view of b bytes at base (null when b is 0), owned by another DevBuf
     void view(void* base, size_t b) {
-        if (owned) dev_free(p);
+        release();
         p = b ? base : nullptr;
         bytes = b;
         owned = false;
     }
-    int alloc(size_t b) {
-        if (owned) dev_free(p);
-        p = nullptr;
+    int alloc(size_t b, cudaStream_t stream = nullptr) {
+        release();
         owned = true;
+        st = stream;
         bytes = b;
         if (b == 0) return ZQD_OK;
-        cudaError_t e = dev_alloc(&p, b);
+        cudaError_t e = dev_alloc(&p, b, stream);
         if (e != cudaSuccess) {
             p = nullptr;
             return fail(ZQD_ERR_DEVICE_OOM, std::string("cudaMalloc(") + std::to_string(b) + "): " + cudaGetErrorString(e));
@@ -45,7 +49,9 @@ struct DevBuf {
 
 struct zqd_job;
 namespace zqd {
-int job_create_opts(Opts&& o, zqd_job** out);
+// stream: the job's work and buffers go to this stream, which the caller owns and keeps until
+// the job is destroyed (null: the job creates its own)
+int job_create_opts(Opts&& o, zqd_job** out, cudaStream_t stream = nullptr);
 int run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, float* ms);
 int step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cudaStream_t st);
 // the persistent service kernel's side of a job (service.cu)
@@ -62,7 +68,7 @@ struct ShapeOverride {
 };
 bool lookup_shape(int d, int n, int S, bool fp32, ShapeOverride& out);
 // a job created with a given launch shape (the autotuner's candidates, the service's single CTAs)
-int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out);
+int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out, cudaStream_t stream = nullptr);
 // Time-dependent potential whose eigenvector signs some output observes: the wavefunction history in
 // the adiabatic basis, or the toDia of a later imaginary-time solve (wavepacket.zig:145-167 then apply).
 inline bool needs_sign_tracking(const Opts& o, int S, int nsolve) {
@@ -83,6 +89,7 @@ struct zqd_job {
     int nsolve = 1, hc = 0;
     zqd::PotStore pot;
     cudaStream_t stream = nullptr;
+    bool own_stream = true; // false: the caller's stream (the server's per-worker streams)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     zqd::DevBuf R, expk, V, U, capw, tw, psi_save, psi0, orth, hist, fin, rows, jobs, scratch;
     zqd::DevBuf phi, part, book, flags; // N-D grids: momentum scratch, partial sums, bookkeeping, stop flags
@@ -102,16 +109,23 @@ struct zqd_job {
     std::vector<int> solve_rows; // rows of each solve's history written so far
     std::vector<char> solve_ended;
     bool stepping = false; // a step-wise run is in progress
+    bool fetch_psi = true; // zqd_job_result downloads the final wavefunctions
     // zqd_job_observables cursor and its host buffer
     int obs_solve = 0, obs_row = 0;
     std::vector<double> obs_buf;
     size_t device_bytes = 0;
     uint64_t h2d = 0, d2h = 0; // bytes copied by this job
+    // The buffers go back to the pool in the job's stream order, without waiting: the job's work in
+    // other streams (group launches, the service kernel) has been waited for by whoever launched it.
     ~zqd_job() {
-        if (stream) cudaStreamSynchronize(stream); // the buffers are released without a device-wide wait
+        zqd::DevBuf* bufs[] = {&R,   &expk, &V,    &U,        &capw,     &tw,  &psi_save, &psi0,  &orth,
+                               &hist, &fin, &rows, &jobs,     &scratch,  &phi, &part,     &book,  &flags,
+                               &psi_init, &wfn_hist, &sgn, &carry, &done, &arena};
+        for (zqd::DevBuf* b : bufs) b->release();
+        pot.release();
         if (nd_graph) cudaGraphExecDestroy(nd_graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (stream) cudaStreamDestroy(stream);
+        if (stream && own_stream) cudaStreamDestroy(stream);
     }
 };

@@ -209,34 +209,34 @@ int ZQD_ND_CREATE(zqd_job* J) {
     const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
     const size_t nparts = 3 * nrow_blocks + S * ntile_blocks + 1024;
     int rc;
-    if ((rc = J->psi_save.alloc((size_t)S * N * c))) return rc;
-    if ((rc = J->phi.alloc((size_t)S * N * c))) return rc;
-    if ((o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF)) && (rc = J->psi0.alloc((size_t)S * N * c))) return rc;
-    if (o.imag_nstate > 1 && (rc = J->orth.alloc((size_t)(o.imag_nstate - 1) * S * N * c))) return rc;
-    if ((rc = J->R.alloc((size_t)NSYM * N * tb))) return rc;
-    if ((rc = J->V.alloc((size_t)S * S * N * sizeof(double)))) return rc;
-    if (S > 1 && (rc = J->U.alloc((size_t)S * S * N * sizeof(double)))) return rc;
-    if (o.has_cap && (rc = J->capw.alloc(N * sizeof(double)))) return rc;
-    if ((rc = J->tw.alloc((size_t)n * tb))) return rc;
-    if ((rc = J->expk.alloc((size_t)J->d * n * (sizeof(double2) + sizeof(double4))))) return rc; // phases, axis table
-    if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double)))) return rc;
+    if ((rc = J->psi_save.alloc((size_t)S * N * c, J->stream))) return rc;
+    if ((rc = J->phi.alloc((size_t)S * N * c, J->stream))) return rc;
+    if ((o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF)) && (rc = J->psi0.alloc((size_t)S * N * c, J->stream))) return rc;
+    if (o.imag_nstate > 1 && (rc = J->orth.alloc((size_t)(o.imag_nstate - 1) * S * N * c, J->stream))) return rc;
+    if ((rc = J->R.alloc((size_t)NSYM * N * tb, J->stream))) return rc;
+    if ((rc = J->V.alloc((size_t)S * S * N * sizeof(double), J->stream))) return rc;
+    if (S > 1 && (rc = J->U.alloc((size_t)S * S * N * sizeof(double), J->stream))) return rc;
+    if (o.has_cap && (rc = J->capw.alloc(N * sizeof(double), J->stream))) return rc;
+    if ((rc = J->tw.alloc((size_t)n * tb, J->stream))) return rc;
+    if ((rc = J->expk.alloc((size_t)J->d * n * (sizeof(double2) + sizeof(double4)), J->stream))) return rc; // phases, axis table
+    if ((rc = J->part.alloc(nparts * NDV * 2 * sizeof(double), J->stream))) return rc;
     if ((o.write_mask & ZQD_WRITE_WAVEFUNCTION) &&
-        (rc = J->wfn_hist.alloc((size_t)J->nsolve * (o.iterations + 1) * S * N * c)))
+        (rc = J->wfn_hist.alloc((size_t)J->nsolve * (o.iterations + 1) * S * N * c, J->stream)))
         return rc;
     if (!o.ic_wfn.empty()) { // initial wavefunction, natural order
-        if ((rc = J->psi_init.alloc((size_t)S * N * c))) return rc;
+        if ((rc = J->psi_init.alloc((size_t)S * N * c, J->stream))) return rc;
         std::vector<cx<T>> h((size_t)S * N);
         for (size_t e = 0; e < (size_t)S * N; ++e) h[e] = mk<T>((T)o.ic_wfn[2 * e], (T)o.ic_wfn[2 * e + 1]);
         ZQD_CUDA(cudaMemcpyAsync(J->psi_init.p, h.data(), (size_t)S * N * c, cudaMemcpyHostToDevice, J->stream));
         ZQD_CUDA(cudaStreamSynchronize(J->stream));
         J->h2d += (size_t)S * N * c;
     }
-    if ((rc = J->book.alloc(sizeof(NdBook)))) return rc;
-    if ((rc = J->flags.alloc(2 * sizeof(int)))) return rc;
+    if ((rc = J->book.alloc(sizeof(NdBook), J->stream))) return rc;
+    if ((rc = J->flags.alloc(2 * sizeof(int), J->stream))) return rc;
     const size_t rows = (size_t)o.iterations + 1;
-    if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double)))) return rc;
-    if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double)))) return rc;
-    if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int)))) return rc;
+    if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double), J->stream))) return rc;
+    if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double), J->stream))) return rc;
+    if ((rc = J->rows.alloc((size_t)J->nsolve * sizeof(int), J->stream))) return rc;
     J->device_bytes = J->psi_save.bytes + J->phi.bytes + J->psi0.bytes + J->orth.bytes + J->R.bytes + J->V.bytes +
                       J->U.bytes + J->capw.bytes + J->part.bytes + J->hist.bytes;
     std::vector<double> tw = twiddles_f64(n);
@@ -416,6 +416,9 @@ int ZQD_ND_STEP(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
     if (i0 == 0 && (rc = q.prologue(s))) return rc;
     for (int i = i0; i <= i1; ++i)
         if ((rc = q.step(s, i))) return rc;
+    // the steps first, then the copies into pageable memory (one queued behind the steps would wait
+    // inside the driver, where it can hold up other threads' copies)
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
     int flags[2] = {0, 0}; // stopped, rows
     ZQD_CUDA(cudaMemcpyAsync(&flags[0], J->flags.p, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
     ZQD_CUDA(cudaMemcpyAsync(&flags[1], q.rows_out(s), sizeof(int), cudaMemcpyDeviceToHost, J->stream));

@@ -202,7 +202,7 @@ static bool injected_alloc_failure() {
     return false;
 }
 
-cudaError_t dev_alloc(void** p, size_t bytes) {
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
     if (injected_alloc_failure()) {
         *p = nullptr;
         return cudaErrorMemoryAllocation;
@@ -223,13 +223,14 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
             configured[dev] = true;
         }
     }
+    if (st) return cudaMallocAsync(p, bytes, st);
     e = cudaMallocAsync(p, bytes, cudaStreamPerThread);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamPerThread); // usable from any stream after this
     return e;
 }
 
-void dev_free(void* p) {
-    if (p) cudaFreeAsync(p, cudaStreamPerThread);
+void dev_free(void* p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st ? st : cudaStreamPerThread);
 }
 
 size_t device_free_bytes() {
@@ -248,19 +249,26 @@ size_t device_free_bytes() {
     return free_b;
 }
 
-PotStore::~PotStore() { dev_free(d_blob); }
+void PotStore::release() {
+    dev_free(d_blob, st);
+    d_blob = nullptr;
+}
 
 // one device block for the potential's data: one allocation and one copy
 static int upload_blob(PotStore& ps, const std::vector<double>& blob) {
     if (blob.empty()) return ZQD_OK;
     const size_t b = blob.size() * sizeof(double);
-    ZQD_CUDA(dev_alloc(&ps.d_blob, b));
-    ZQD_CUDA(cudaMemcpy(ps.d_blob, blob.data(), b, cudaMemcpyHostToDevice));
+    const cudaStream_t st = ps.st ? ps.st : cudaStreamPerThread;
+    ZQD_CUDA(dev_alloc(&ps.d_blob, b, st));
+    ZQD_CUDA(cudaMemcpyAsync(ps.d_blob, blob.data(), b, cudaMemcpyHostToDevice, st));
+    ZQD_CUDA(cudaStreamSynchronize(st));
     ps.bytes += b;
     return ZQD_OK;
 }
 
-int build_potential(const Opts& o, PotStore& ps) {
+int build_potential(const Opts& o, PotStore& ps, cudaStream_t st) {
+    ps.release();
+    ps.st = st;
     PotDev& P = ps.dev;
     std::memset(&P, 0, sizeof(P));
     P.kind = o.pkind;

@@ -76,6 +76,7 @@ extern "C" int zqd_result_wavefunction(const zqd_result* r, uint32_t s, double* 
     if (!r || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
     if (s >= r->solves.size()) return fail(ZQD_ERR_NOT_FOUND, "SOLVE INDEX OUT OF RANGE");
     const std::vector<double>& p = r->solves[s].psi;
+    if (p.empty()) return fail(ZQD_ERR_NOT_FOUND, "THE FINAL WAVEFUNCTION WAS NOT DOWNLOADED (server option)");
     if (capacity < p.size()) return fail(ZQD_ERR_INVALID_INPUT, "OUTPUT BUFFER TOO SMALL");
     std::memcpy(out, p.data(), p.size() * sizeof(double));
     return ZQD_OK;

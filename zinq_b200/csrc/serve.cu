@@ -1,7 +1,7 @@
 // serve.cu -- a job server for streams of independent propagation requests.
 //
-// Requests are validated and copied at submission.  Worker threads (one CUDA stream per job)
-// admit them in arrival order while their estimated device memory fits the budget and the
+// Requests are validated and copied at submission.  Worker threads (one CUDA stream each, which
+// their jobs use for all their work and buffers) admit them in arrival order while their estimated device memory fits the budget and the
 // device's measured free memory.  A worker advances its jobs in launches of `stream_steps`
 // steps (zqd_job_step): 1-D single-solve requests that share a kernel shape (precision, states,
 // grid points) form one group advanced by one launch of the resident line kernel, every member
@@ -118,6 +118,7 @@ struct zqd_server {
     size_t budget = 0, in_use = 0, peak = 0;
     uint32_t max_batch = 16, stream_steps = 256, max_events = 65536;
     bool stream_rows = true;
+    bool fetch_psi = true; // results carry the final wavefunction
     // persistent line service: one table per (precision, states), guarded by svc_mu
     bool use_service = true;
     uint32_t service_ctas = 0;
@@ -141,25 +142,61 @@ struct zqd_server {
     zqd_server_stats stats{};
     std::vector<std::thread> workers;
 
-    mutable size_t free_bytes = 0; // device memory free at free_at
+    // Device memory measured free (cudaMemGetInfo and the pool's spare blocks) at free_at, when this
+    // server's admitted estimates summed to in_use_at.  A measurement takes milliseconds while kernels
+    // run, so admission works from it and the estimates admitted or released since.
+    mutable size_t free_bytes = 0, in_use_at = 0;
     mutable Clock::time_point free_at{};
+    size_t free_estimate() const { // under mu
+        const long long f = (long long)free_bytes + (long long)in_use_at - (long long)in_use;
+        return f > 0 ? (size_t)f : 0;
+    }
     bool fits(const Request& q) const; // under mu
+    void refresh_free();               // measures without mu
+    // Streams live as long as the server: a stream per worker, and one for the service's requests
+    // (creation, row and result copies).  CUDA maps streams onto a few hardware queues; a stream
+    // made per job would soon share one with another worker's busy stream, and every wait on it
+    // (an allocation, a copy) would wait for that worker's kernels as well.
+    cudaStream_t svc_io = nullptr;
     void work();
-    void run_active(std::vector<Req> group);
+    void run_active(std::vector<Req> group, cudaStream_t ws);
     void post(Event&& e);                           // under mu
     void finish(const Req& q, int status, const std::string& err, zqd_result* res); // takes mu
     int stream(const Req& q, std::string& err); // ZQD_ERR_NUMERIC (err says where) for a non-finite row
 };
 
+// A request fits when its estimate stays within the budget and, with an eighth to spare, within the
+// free device memory.  The free memory is measured again here only when the running estimate says
+// no (at most every 20 ms); the service thread refreshes it while requests wait (refresh_free).
 bool zqd_server::fits(const Request& q) const {
     if (in_use + q.est > budget) return false;
     if (in_use == 0) return true; // nothing of ours to wait for: the allocation decides
+    const size_t need = q.est + q.est / 8;
+    if (need <= free_estimate()) return true;
     const Clock::time_point now = Clock::now();
-    if (now - free_at > std::chrono::milliseconds(1)) { // measured at most once a millisecond
-        free_bytes = zqd::device_free_bytes();
-        free_at = now;
+    if (now - free_at < std::chrono::milliseconds(20)) return false;
+    free_bytes = zqd::device_free_bytes();
+    free_at = now;
+    in_use_at = in_use;
+    return need <= free_bytes;
+}
+
+// Measures the free device memory without holding mu (other processes' use shows up here).  The
+// estimates admitted meanwhile count as taken and those released meanwhile as still held: in_use_at
+// is the smaller of the sums before and after the measurement.
+void zqd_server::refresh_free() {
+    size_t before;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (queue.empty() || in_use == 0) return; // nobody waits for admission
+        before = in_use;
     }
-    return q.est + q.est / 8 <= free_bytes;
+    const size_t f = zqd::device_free_bytes();
+    std::lock_guard<std::mutex> lk(mu);
+    free_bytes = f;
+    in_use_at = std::min(before, in_use);
+    free_at = Clock::now();
+    cv_work.notify_all();
 }
 
 void zqd_server::post(Event&& e) {
@@ -197,8 +234,9 @@ void zqd_server::finish(const Req& q, int status, const std::string& err, zqd_re
     cv_work.notify_all();
 }
 
-// the job's observable rows recorded since the last call, as events
+// the job's observable rows recorded since the last call, as events (none without stream_rows)
 int zqd_server::stream(const Req& q, std::string& err) {
+    if (!stream_rows) return ZQD_OK; // no row events: the final observables are checked at the end
     for (;;) {
         zqd_obs_rows r{};
         if (zqd_job_observables(q->job, &r) != ZQD_OK || r.nrows == 0) return ZQD_OK;
@@ -219,23 +257,18 @@ int zqd_server::stream(const Req& q, std::string& err) {
 
 // Advances `group` (one request, or 1-D requests of one shape) launch by launch until every
 // member has left; waiting requests of the same shape join between launches.
-void zqd_server::run_active(std::vector<Req> group) {
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
-        cudaGetLastError();
-        for (const Req& q : group) finish(q, ZQD_ERR_DEVICE, "cudaStreamCreateWithFlags failed", nullptr);
-        return;
-    }
+void zqd_server::run_active(std::vector<Req> group, cudaStream_t st) {
     const uint64_t key = group.front()->group_key;
     auto create = [&](const Req& q) -> bool {
         zqd::Opts o = q->o;
-        const int rc = zqd::job_create_opts(std::move(o), &q->job);
+        const int rc = zqd::job_create_opts(std::move(o), &q->job, st);
         if (rc) {
             finish(q, rc, zqd::last_error(), nullptr);
             q->job = nullptr;
             return false;
         }
         q->job->nd_use_graph = false;
+        q->job->fetch_psi = fetch_psi;
         return true;
     };
     std::vector<Req> active;
@@ -336,7 +369,6 @@ void zqd_server::run_active(std::vector<Req> group) {
                 if (create(q)) active.push_back(q);
         }
     }
-    cudaStreamDestroy(st);
 }
 
 // Single-solve 1-D requests whose line fits one CTA: created with the single-CTA shape and posted
@@ -350,7 +382,7 @@ bool zqd_server::try_service(const Req& q) {
     one.lrmax = 2;
     zqd_job* J = nullptr;
     zqd::Opts copy = o;
-    if (const int rc = zqd::job_create_shaped(std::move(copy), one, &J)) {
+    if (const int rc = zqd::job_create_shaped(std::move(copy), one, &J, svc_io)) {
         if (rc == ZQD_ERR_UNSUPPORTED) return false; // the line does not fit one CTA: the general path
         finish(q, rc, zqd::last_error(), nullptr);   // e.g. device memory refused: the request fails here
         return true;
@@ -359,6 +391,7 @@ bool zqd_server::try_service(const Req& q) {
         zqd_job_destroy(J);
         return false;
     }
+    J->fetch_psi = fetch_psi;
     // the job's shape, rounded up: threads to a power of two (>= 64), shared memory to 16 KiB
     int threads = 64;
     while (threads < J->threads) threads <<= 1;
@@ -390,7 +423,12 @@ bool zqd_server::try_service(const Req& q) {
 void zqd_server::service_loop() {
     cudaSetDevice(device);
     const int batch_rows = stream_steps ? (int)stream_steps : INT32_MAX;
+    Clock::time_point refreshed = Clock::now();
     for (;;) {
+        if (Clock::now() - refreshed > std::chrono::milliseconds(250)) { // free device memory for admission
+            refresh_free();
+            refreshed = Clock::now();
+        }
         std::vector<SvcJob> snap;
         {
             std::unique_lock<std::mutex> lk(svc_mu);
@@ -455,6 +493,17 @@ void zqd_server::service_loop() {
 
 void zqd_server::work() {
     cudaSetDevice(device);
+    cudaStream_t ws = nullptr; // null if it cannot be had: the jobs then make their own
+    if (cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        ws = nullptr;
+    }
+    struct Drop {
+        cudaStream_t s;
+        ~Drop() {
+            if (s) cudaStreamDestroy(s);
+        }
+    } drop{ws};
     for (;;) {
         std::vector<Req> batch;
         {
@@ -492,7 +541,7 @@ void zqd_server::work() {
             stats.peak_device_bytes = peak;
             if (!queue.empty()) cv_work.notify_one();
         }
-        run_active(std::move(batch));
+        run_active(std::move(batch), ws);
     }
 }
 
@@ -500,12 +549,13 @@ extern "C" void zqd_server_config_init(zqd_server_config* cfg) {
     if (!cfg) return;
     *cfg = zqd_server_config{};
     cfg->struct_size = sizeof(zqd_server_config);
-    cfg->workers = 4;
+    cfg->workers = 8;
     cfg->max_batch = 16;
     cfg->stream_steps = 256;
     cfg->stream_rows = 1;
     cfg->max_events = 65536;
     cfg->persistent_lines = 1;
+    cfg->fetch_wavefunction = 1;
     cfg->service_ctas = 64;
     cfg->service_idle_us = 200.0;
 }
@@ -521,6 +571,8 @@ extern "C" int zqd_server_create(const zqd_server_config* cfg, zqd_server** out)
     if (!S) return zqd::fail(ZQD_ERR_OUT_OF_MEMORY, "host allocation failed");
     ZQD_CUDA(cudaGetDevice(&S->device));
     const size_t free_b = zqd::device_free_bytes();
+    S->free_bytes = free_b;
+    S->free_at = Clock::now();
     S->budget = cfg->device_budget_bytes ? (size_t)cfg->device_budget_bytes : free_b / 10 * 9;
     S->max_batch = std::max(1u, cfg->max_batch ? cfg->max_batch : 16u);
     S->stream_steps = cfg->stream_steps;
@@ -528,10 +580,15 @@ extern "C" int zqd_server_create(const zqd_server_config* cfg, zqd_server** out)
     S->max_events = std::max(1u, cfg->max_events ? cfg->max_events : 65536u);
     S->stats.device_budget_bytes = S->budget;
     S->use_service = cfg->persistent_lines != 0;
+    S->fetch_psi = cfg->fetch_wavefunction != 0;
     S->service_ctas = cfg->service_ctas;
     S->service_idle_us = cfg->service_idle_us > 0 ? cfg->service_idle_us : 200.0;
+    if (cudaStreamCreateWithFlags(&S->svc_io, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        S->svc_io = nullptr; // the service's requests make their own streams
+    }
     S->svc_thread = std::thread([s = S.get()] { s->service_loop(); });
-    const uint32_t nw = std::max(1u, cfg->workers ? cfg->workers : 4u);
+    const uint32_t nw = std::max(1u, cfg->workers ? cfg->workers : 8u);
     for (uint32_t i = 0; i < nw; ++i) S->workers.emplace_back([s = S.get()] { s->work(); });
     *out = S.release();
     return ZQD_OK;
@@ -663,5 +720,7 @@ extern "C" void zqd_server_destroy(zqd_server* S) {
     }
     S->svc_cv.notify_all();
     if (S->svc_thread.joinable()) S->svc_thread.join(); // every service request has completed
+    S->svc.clear();
+    if (S->svc_io) cudaStreamDestroy(S->svc_io);
     delete S;
 }

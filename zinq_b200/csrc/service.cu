@@ -45,9 +45,10 @@ int LineServiceHost::init(unsigned capacity, unsigned max_ctas, double idle_us) 
     std::memset(done_, 0, capacity * sizeof(int));
     std::memset(progress_, 0, capacity * sizeof(int));
     freed_.assign(capacity, 0);
-    ZQD_CUDA(dev_alloc((void**)&claim_, 2 * sizeof(unsigned)));
-    ZQD_CUDA(cudaMemset(claim_, 0, 2 * sizeof(unsigned)));
     ZQD_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    ZQD_CUDA(dev_alloc((void**)&claim_, 2 * sizeof(unsigned)));
+    ZQD_CUDA(cudaMemsetAsync(claim_, 0, 2 * sizeof(unsigned), st_));
+    ZQD_CUDA(cudaStreamSynchronize(st_));
     int dev = 0, sms = 148, khz = 1965000;
     ZQD_CUDA(cudaGetDevice(&dev));
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -105,9 +106,12 @@ int LineServiceHost::launch(unsigned grid) {
     return ZQD_OK;
 }
 
+// (with no service kernel alive, so the copy waits for nothing in the service's stream)
 unsigned LineServiceHost::claimed() {
     unsigned c[2] = {0, 0};
-    if (cudaMemcpy(c, claim_, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) cudaGetLastError();
+    if (cudaMemcpyAsync(c, claim_, sizeof(c), cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
+        cudaStreamSynchronize(st_) != cudaSuccess)
+        cudaGetLastError();
     return c[0];
 }
 
@@ -151,7 +155,9 @@ void LineServiceHost::close() {
 
 unsigned LineServiceHost::idle_exits() const {
     unsigned c[2] = {0, 0};
-    if (cudaMemcpy(c, claim_, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess) cudaGetLastError();
+    if (cudaMemcpyAsync(c, claim_, sizeof(c), cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
+        cudaStreamSynchronize(st_) != cudaSuccess)
+        cudaGetLastError();
     return c[1];
 }
 

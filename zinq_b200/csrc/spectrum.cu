@@ -65,14 +65,15 @@ int spectrum_device(cudaStream_t st, const double* d_hist, int hc, int col, size
     if (lp == 0) return ZQD_OK;
     double2 *acfpad = nullptr, *W = nullptr;
     double* sigma = nullptr;
+    // pool blocks in the job's stream (cudaFree would wait for every stream of the device)
     auto cleanup = [&]() {
-        if (acfpad) cudaFree(acfpad);
-        if (W) cudaFree(W);
-        if (sigma) cudaFree(sigma);
+        dev_free(acfpad, st);
+        dev_free(W, st);
+        dev_free(sigma, st);
     };
-    cudaError_t e = cudaMalloc(&acfpad, lp * sizeof(double2));
-    if (e == cudaSuccess && M) e = cudaMalloc(&W, M * sizeof(double2));
-    if (e == cudaSuccess && M) e = cudaMalloc(&sigma, M * sizeof(double));
+    cudaError_t e = dev_alloc((void**)&acfpad, lp * sizeof(double2), st);
+    if (e == cudaSuccess && M) e = dev_alloc((void**)&W, M * sizeof(double2), st);
+    if (e == cudaSuccess && M) e = dev_alloc((void**)&sigma, M * sizeof(double), st);
     if (e != cudaSuccess) {
         cleanup();
         return fail(ZQD_ERR_DEVICE_OOM, std::string("spectrum buffers: ") + cudaGetErrorString(e));

@@ -120,10 +120,10 @@ double time_shape(int d, int n, int S, bool fp32, const ShapeOverride& cand) {
 
 } // namespace
 
-int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out) {
+int job_create_shaped(Opts&& o, const ShapeOverride& shape, zqd_job** out, cudaStream_t stream) {
     t_forcing = true;
     t_forced = shape;
-    const int rc = job_create_opts(std::move(o), out);
+    const int rc = job_create_opts(std::move(o), out, stream);
     t_forcing = false;
     return rc;
 }

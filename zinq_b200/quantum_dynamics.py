@@ -448,9 +448,9 @@ class Server:
     """Request loop for streams of independent jobs (zqd_server_*): submit() returns a ticket at once,
     wait() returns (Result, latency in ms from submission to completion)."""
 
-    def __init__(self, workers: int = 4, max_batch: int = 16, device_budget_bytes: int = 0, stream_steps: int = 256,
+    def __init__(self, workers: int = 8, max_batch: int = 16, device_budget_bytes: int = 0, stream_steps: int = 256,
                  stream_rows: bool = True, max_events: int = 65536, persistent_lines: bool = True,
-                 service_ctas: int = 64, service_idle_us: float = 200.0):
+                 service_ctas: int = 64, service_idle_us: float = 200.0, fetch_wavefunction: bool = True):
         self._L = _abi.load()
         cfg = _abi.ZqdServerConfig()
         self._L.zqd_server_config_init(C.byref(cfg))
@@ -458,6 +458,7 @@ class Server:
         cfg.stream_steps, cfg.stream_rows, cfg.max_events = stream_steps, int(bool(stream_rows)), max_events
         cfg.persistent_lines, cfg.service_ctas = int(bool(persistent_lines)), service_ctas
         cfg.service_idle_us = service_idle_us
+        cfg.fetch_wavefunction = int(bool(fetch_wavefunction))
         self._h = C.c_void_p()
         check(self._L.zqd_server_create(C.byref(cfg), C.byref(self._h)))
         self._shapes = {}
@@ -521,7 +522,7 @@ class Server:
             pass
 
 
-def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers: int = 4, max_batch: int = 16,
+def serve_stream(opts: list, arrivals_s: list, precision: str = "fp32", workers: int = 8, max_batch: int = 16,
                  **server_kw):
     """Submits opts[i] at arrivals_s[i] seconds after the start (a feeder thread sleeps until each
     arrival), waits for all; returns (results, latencies_ms, wall_s from the first arrival to the
