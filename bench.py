@@ -604,7 +604,7 @@ def main():
     ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
                     help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
     ap.add_argument("--nd-case", nargs=3, metavar=("WORKLOAD", "PRECISION", "STEPS"), default=None,
-                    help="run one 2-D/3-D workload (c3 | c4 | c4itp | wide) for STEPS steps twice and exit; "
+                    help="run one 2-D/3-D workload (c3 | c3pop | c4 | c4itp | wide) for STEPS steps twice and exit; "
                          "for ncu captures")
     ap.add_argument("--table", action="store_true",
                     help="print per-configuration CPU (oracle) and GPU rates as one JSON line and exit")
@@ -629,7 +629,12 @@ def main():
         from zinq_b200 import quantum_dynamics as qd
 
         case, prec, steps = args.nd_case[0], args.nd_case[1], int(args.nd_case[2])
-        opt = {"c3": lambda: coupled_harmonic_2d(iters=steps), "c4": lambda: anharmonic_3d(steps, False),
+        def c3pop():  # the 512^2 three-state grid recording populations only (the serving stream's largest jobs)
+            o = coupled_harmonic_2d(iters=steps)
+            o["write"] = {"population": "P"}
+            return o
+
+        opt = {"c3": lambda: coupled_harmonic_2d(iters=steps), "c3pop": c3pop, "c4": lambda: anharmonic_3d(steps, False),
                "c4itp": lambda: anharmonic_3d(steps, True), "wide": lambda: wide_grid_2d(steps)}[case]()
         job = qd.Job(opt, prec)
         for _ in range(2):

@@ -313,6 +313,9 @@ typedef struct {
     uint32_t cluster_ctas, radix_log2, rows_per_cta, tile_lines;
     double us_per_step, default_us_per_step;
     uint32_t candidates;
+    /* out, N-D: the TMA-staged persistent passes' shapes, rows per row block and lines per tile
+       (0: the rules' choice, -1: the per-block kernel instead) */
+    int32_t tma_row_block, tma_tile_lines;
 } zqd_tune_entry;
 int zqd_autotune(zqd_tune_entry* entry);
 int zqd_tune_save(const char* path); /* text: one "ndim npoint nstate fp32 C radix_log2 rows tile" line per key */

@@ -53,4 +53,22 @@ def test_table_save_clear_load(tmp_path):
     qd.tune_save(tmp_path / "again.txt")
     assert lines == [ln for ln in open(tmp_path / "again.txt") if not ln.startswith("#")]
     if e["cluster_ctas"]:
-        assert lines == [f"1 256 1 1 {e['cluster_ctas']} {e['radix_log2']} 0 0\n"]
+        assert lines == [f"1 256 1 1 {e['cluster_ctas']} {e['radix_log2']} 0 0 0 0\n"]
+
+
+def test_tuned_nd_shape_round_trips_with_the_tma_fields(tmp_path):
+    e = qd.autotune(3, 32, 1, "fp64")
+    assert e["candidates"] >= 2 and e["us_per_step"] <= e["default_us_per_step"] * 1.0001
+    path = tmp_path / "tune.txt"
+    qd.tune_save(path)
+    lines = [ln.split() for ln in open(path) if not ln.startswith("#")]
+    if lines:  # a tuned shape beat the rules: all ten fields, the TMA pair as measured
+        assert len(lines) == 1 and len(lines[0]) == 10
+        assert [int(x) for x in lines[0][8:]] == [e["tma_row_block"], e["tma_tile_lines"]]
+    # an eight-field table (written before the TMA-staged passes) still loads
+    old = tmp_path / "old.txt"
+    old.write_text("2 64 1 0 0 0 2 4\n")
+    qd.tune_clear()
+    qd.tune_load(old)
+    qd.tune_save(tmp_path / "again.txt")
+    assert [ln for ln in open(tmp_path / "again.txt") if not ln.startswith("#")] == ["2 64 1 0 0 0 2 4 0 0\n"]

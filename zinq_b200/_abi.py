@@ -112,7 +112,7 @@ class ZqdTuneEntry(C.Structure):
     _fields_ = [("ndim", C.c_uint32), ("npoint", C.c_uint32), ("nstate", C.c_uint32), ("precision", C.c_int),
                 ("cluster_ctas", C.c_uint32), ("radix_log2", C.c_uint32), ("rows_per_cta", C.c_uint32),
                 ("tile_lines", C.c_uint32), ("us_per_step", C.c_double), ("default_us_per_step", C.c_double),
-                ("candidates", C.c_uint32)]
+                ("candidates", C.c_uint32), ("tma_row_block", C.c_int32), ("tma_tile_lines", C.c_int32)]
 
 
 class ZqdEvent(C.Structure):

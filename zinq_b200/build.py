@@ -19,7 +19,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-ccbin", "g++"]
 
-SOURCES = ["options.cu", "expr.cpp", "job.cu", "result.cu", "fft_seam.cu", "spectrum.cu", "serve.cu", "tune.cu", "service.cu", "measure.cu"]
+SOURCES = ["options.cu", "expr.cpp", "job.cu", "result.cu", "fft_seam.cu", "spectrum.cu", "serve.cu", "tune.cu", "service.cu", "measure.cu", "tma_map.cu"]
 # line_inst.cu is compiled once per (precision, number of electronic states)
 VARIANTS = [("line_inst.cu", f"line_{t[0]}{s}", [f"-DZQD_T={t}", f"-DZQD_S={s}", f"-DZQD_LAUNCH=launch_line_{t[0]}{s}",
                                                    f"-DZQD_SERVICE=launch_service_{t[0]}{s}"])

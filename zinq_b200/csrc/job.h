@@ -65,6 +65,8 @@ void service_job_rows(zqd_job* J, int rows);
 struct ShapeOverride {
     int C = 0, lrmax = 0; // 1-D: CTAs per cluster, log2 of the largest local radix
     int rows = 0, tile = 0; // N-D: rows of the last axis per row-pass CTA, lines per tile-pass CTA
+    int tma_w = 0;          // N-D: lines per TMA-staged tile (-1: the earlier tile kernel)
+    int tma_rows = 0;       // N-D: rows per TMA-staged row block (-1: the earlier row kernel)
 };
 bool lookup_shape(int d, int n, int S, bool fp32, ShapeOverride& out);
 // a job created with a given launch shape (the autotuner's candidates, the service's single CTAs)
@@ -100,6 +102,17 @@ struct zqd_job {
     zqd::DevBuf arena;                  // 1-D jobs: one pool block holding the buffers above (views)
     double min_gap = -1;                // ZQD_PRECISION_AUTO: smallest adiabatic gap on the grid (-1: not computed)
     int nd_rows = 1, nd_tile = 8, nd_row_threads = 32, nd_tile_threads = 32, nd_row_bufs = 2;
+    // N-D strided-axis passes through the TMA-staged persistent kernel: lines per tile (log2), CTAs,
+    // and one tensor map (CUtensorMap, 128 bytes) over psi per strided axis
+    bool nd_tma = false;
+    int nd_tma_logW = 0, nd_tma_ctas = 0;
+    alignas(64) unsigned char nd_maps[2][128] = {};
+    // the row pass's TMA-staged persistent form: rows per block (log2), CTAs, tensor map over psi
+    bool nd_row_tma = false;
+    bool nd_row_tma_phi = false; // the momentum-copy launches too (else they take the earlier kernel)
+    int nd_row_tma_logL = 0, nd_row_tma_ctas = 0;
+    alignas(64) unsigned char nd_row_map[128] = {};
+    alignas(64) unsigned char nd_row_map_phi[128] = {}; // the same over phi (the momentum copy)
     cudaGraphExec_t nd_graph = nullptr; // the whole N-D run, captured on its first call and replayed after
     bool nd_use_graph = true;           // false: launch directly (one-shot jobs skip the capture cost)
     float last_ms = 0;

@@ -5,6 +5,7 @@
 // A solve (src/quantum_dynamics.zig:860-950) is a stream-ordered sequence of
 // axis passes (nd_kernels.cuh); nothing returns to the host until the end.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -73,6 +74,7 @@ NdJob<T> describe(zqd_job* J) {
     D.tile = J->nd_tile;
     while ((1 << D.logtile) < J->nd_tile) ++D.logtile;
     D.stopped = J->flags.as<int>();
+    D.err = J->flags.as<int>() + 2;
     D.pot = J->pot.dev;
     return D;
 }
@@ -93,6 +95,23 @@ struct Launch {
         NdJob<T> d = D;
         d.wfn_out = wout;
         if (nostop) d.stopped = J->flags.as<int>() + 1; // a flag nothing sets
+        if (J->nd_row_tma && (!(mode & RM_PHI) || J->nd_row_tma_phi)) {
+            NdRowTma P{};
+            P.mode = mode;
+            P.obs = obs;
+            P.logL = J->nd_row_tma_logL;
+            P.nitems = (unsigned)(J->N / J->n >> P.logL);
+            P.ncols = (unsigned)nrow_blocks;
+            const size_t smem = ndr_smem_bytes<T>(S, 1 << P.logL, J->n);
+            const unsigned nt = (unsigned)((S * J->n << P.logL) / 8), nb = (unsigned)J->nd_row_tma_ctas;
+            const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_row_map);
+            const CUtensorMap* mphi = reinterpret_cast<const CUtensorMap*>(J->nd_row_map_phi);
+            auto kern = (mode & RM_PHI) ? (D.d == 2 ? nd_row_tma_kernel<T, 2, S, true> : nd_row_tma_kernel<T, 3, S, true>)
+                                        : (D.d == 2 ? nd_row_tma_kernel<T, 2, S, false> : nd_row_tma_kernel<T, 3, S, false>);
+            kern<<<nb, nt, smem, J->stream>>>(d, *map, *mphi, P, region, f);
+            ZQD_CUDA(cudaGetLastError());
+            return ZQD_OK;
+        }
         const size_t smem = nd_smem_bytes<T>(2, S * J->nd_rows, J->n);
         const unsigned nb = (unsigned)nrow_blocks, nt = (unsigned)J->nd_row_threads;
         if (row_narrow(nt)) {
@@ -115,14 +134,35 @@ struct Launch {
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
+    // the TMA-staged persistent form of a psi tile pass (modes TM_FWD, TM_KPHASE, TM_INV)
+    int tile_tma(int axis, uint32_t mode) {
+        const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_maps[axis]);
+        NdTma P{};
+        P.axis = axis;
+        P.mode = mode;
+        P.logW = J->nd_tma_logW;
+        const int lstride = D.logn * (D.d - 1 - axis);
+        int logN = 0;
+        while (((size_t)1 << logN) < J->N) ++logN;
+        P.logtiles = logN - D.logn - P.logW;
+        P.logO = logN - D.logn - lstride;
+        P.nitems = (unsigned)S << P.logtiles;
+        const size_t smem = ndt_smem_bytes<T>(1 << P.logW, J->n);
+        const unsigned threads = (unsigned)((J->n << P.logW) / 8);
+        if (D.d == 2) nd_tile_tma_kernel<T, 2><<<(unsigned)J->nd_tma_ctas, threads, smem, J->stream>>>(D, *map, P);
+        else nd_tile_tma_kernel<T, 3><<<(unsigned)J->nd_tma_ctas, threads, smem, J->stream>>>(D, *map, P);
+        ZQD_CUDA(cudaGetLastError());
+        return ZQD_OK;
+    }
+    int ptile(int axis, uint32_t mode) { return J->nd_tma ? tile_tma(axis, mode) : tile(axis, mode, 0); }
     // forward along axes d-2..1, forward + kinetic phase + inverse along axis 0, inverse along 1..d-2
     int step_tiles() {
         int rc;
         for (int a = D.d - 2; a >= 1; --a)
-            if ((rc = tile(a, TM_FWD, 0))) return rc;
-        if ((rc = tile(0, TM_FWD | TM_KPHASE | TM_INV, 0))) return rc;
+            if ((rc = ptile(a, TM_FWD))) return rc;
+        if ((rc = ptile(0, TM_FWD | TM_KPHASE | TM_INV))) return rc;
         for (int a = 1; a <= D.d - 2; ++a)
-            if ((rc = tile(a, TM_INV, 0))) return rc;
+            if ((rc = ptile(a, TM_INV))) return rc;
         return ZQD_OK;
     }
     double* scal() const { return J->book.as<NdBook>()->scal; }
@@ -157,6 +197,146 @@ struct Launch {
         return tile(0, TM_FWD | TM_KOBS | TM_PHI, K, nostop, f);
     }
 };
+
+// The TMA-staged tile pass: lines per tile W (a power of two, W <= n) with rows of W c >= 16
+// bytes (an even number of 8-byte words), W n / 8 threads (whole warps, at most 512) and two stages within the
+// shared-memory budget; by default the widest W up to 64-byte rows whose grid still gives every
+// resident CTA two tiles.  w_override (the autotuner's candidate or table entry): 0 keeps the
+// default, -1 keeps the earlier tile kernel, else W.  ZQD_ND_TMA=0 in the environment also keeps it.
+int setup_tma(zqd_job* J, int w_override) {
+    constexpr int c = (int)sizeof(cx<T>), E = c / 8;
+    const int n = J->n, d = J->d;
+    const size_t budget = 200 * 1024;
+    J->nd_tma = false;
+    const char* env = getenv("ZQD_ND_TMA");
+    if ((env && env[0] == '0') || w_override < 0) return ZQD_OK;
+    int dev = 0, sms = 148;
+    ZQD_CUDA(cudaGetDevice(&dev));
+    ZQD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (auto f : {nd_tile_tma_kernel<T, 2>, nd_tile_tma_kernel<T, 3>})
+        ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+    auto fits = [&](int W) {
+        return W >= 1 && W <= n && (E * W) % 2 == 0 && (size_t)W * n / 8 <= 512 && ((size_t)W * n / 8) % 32 == 0 &&
+               ndt_smem_bytes<T>(W, n) <= budget;
+    };
+    auto ctas_for = [&](int W, int& ctas) -> int {
+        const int threads = W * n / 8;
+        int per_sm = 0;
+        ZQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, d == 2 ? (const void*)nd_tile_tma_kernel<T, 2> : (const void*)nd_tile_tma_kernel<T, 3>, threads,
+            ndt_smem_bytes<T>(W, n)));
+        ctas = std::max(1, per_sm) * sms;
+        return ZQD_OK;
+    };
+    const size_t lines = J->N / (size_t)n; // lines of one state along any axis
+    int W = 0;
+    const char* ew = getenv("ZQD_TMA_W");
+    if (w_override > 0) W = w_override;
+    else if (ew && atoi(ew) > 0) W = atoi(ew);
+    if (W) {
+        if (!fits(W) || lines % (size_t)W) return fail(ZQD_ERR_UNSUPPORTED, "TMA TILE SHAPE OUTSIDE THE KERNEL'S LIMITS");
+    } else {
+        for (int w = std::max(1, 64 / c); w >= 1 && !W; w >>= 1) {
+            if (!fits(w) || lines % (size_t)w) continue;
+            int ctas = 0, rc;
+            if ((rc = ctas_for(w, ctas))) return rc;
+            if ((size_t)S * (lines / w) >= 2 * (size_t)ctas || !fits(w / 2)) W = w;
+        }
+        if (!W) return ZQD_OK; // no shape fits: the earlier tile kernel runs
+    }
+    int logW = 0;
+    while ((1 << logW) < W) ++logW;
+    int ctas = 0, rc;
+    if ((rc = ctas_for(W, ctas))) return rc;
+    const size_t items = (size_t)S * (lines / W);
+    J->nd_tma_ctas = (int)std::min<size_t>(items, (size_t)ctas);
+    J->nd_tma_logW = logW;
+    int logn = 0;
+    while ((1 << logn) < n) ++logn;
+    for (int a = 0; a + 1 < d; ++a) {
+        const int lstride = logn * (d - 1 - a);
+        const uint64_t st = (uint64_t)1 << lstride, O = J->N / ((uint64_t)n * st);
+        const uint64_t dims[3] = {(uint64_t)E * st, (uint64_t)n, (uint64_t)S * O};
+        const uint32_t box[3] = {(uint32_t)(E * W), (uint32_t)std::min(n, 256), 1};
+        const int l2 = W * c >= 128 ? 128 : 0;
+        const int e = encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_maps[a]), J->psi_save.p, dims, st * c,
+                                    (uint64_t)n * st * c, box, l2);
+        if (e) return fail(ZQD_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the tile pass");
+    }
+    J->nd_tma = true;
+    return ZQD_OK;
+}
+
+// The TMA-staged row pass: L rows (a power of two dividing N/n) per block with L n c >= 1024 bytes
+// (the stages keep the 128-byte swizzle's 1024-byte alignment), S L n / 8 threads (whole warps, at
+// most 256: the sweep, the sums and the momentum copy keep their registers) and two stages within the budget; by default the largest L up to
+// about 2048 points per block whose grid still gives every resident CTA two blocks.  The grid is
+// at most the earlier kernel's block count (the width of the partial-sum regions).
+// l_override: 0 keeps the default, -1 keeps the earlier row kernel, else L.  ZQD_ND_TMA=0 also
+// keeps it.
+int setup_row_tma(zqd_job* J, int l_override, size_t ncols) {
+    constexpr int c = (int)sizeof(cx<T>);
+    const int n = J->n, d = J->d;
+    const size_t budget = 200 * 1024, lines = J->N / (size_t)n;
+    J->nd_row_tma = false;
+    const char* env = getenv("ZQD_ND_TMA");
+    if ((env && env[0] == '0') || l_override < 0) return ZQD_OK;
+    int dev = 0, sms = 148;
+    ZQD_CUDA(cudaGetDevice(&dev));
+    ZQD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>, nd_row_tma_kernel<T, 2, S, true>,
+                   nd_row_tma_kernel<T, 3, S, true>})
+        ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+    auto threads_of = [&](int L) { return (size_t)S * L * n / 8; };
+    auto fits = [&](int L) {
+        const size_t t = threads_of(L);
+        // whole warps: the block reduction's shuffles run on full warps
+        return L >= 1 && (size_t)L <= lines && lines % (size_t)L == 0 && (size_t)L * n * c >= 1024 && t % 32 == 0 &&
+               t <= (size_t)NDR_THREADS && ndr_smem_bytes<T>(S, L, n) <= budget;
+    };
+    auto ctas_for = [&](int L, int& ctas) -> int {
+        const unsigned nt = (unsigned)threads_of(L);
+        const void* f = d == 2 ? (const void*)nd_row_tma_kernel<T, 2, S, false> : (const void*)nd_row_tma_kernel<T, 3, S, false>;
+        int per_sm = 0;
+        ZQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, (int)nt, ndr_smem_bytes<T>(S, L, n)));
+        ctas = std::max(1, per_sm) * sms;
+        return ZQD_OK;
+    };
+    int L = 0;
+    const char* el = getenv("ZQD_TMA_ROWS");
+    if (l_override > 0) L = l_override;
+    else if (el && atoi(el) > 0) L = atoi(el);
+    if (L) {
+        if (!fits(L)) return fail(ZQD_ERR_UNSUPPORTED, "TMA ROW-BLOCK SHAPE OUTSIDE THE KERNEL'S LIMITS");
+    } else {
+        for (int l = std::max(1, 2048 / (S * n)); l >= 1 && !L; l >>= 1) {
+            if (!fits(l)) continue;
+            int ctas = 0, rc;
+            if ((rc = ctas_for(l, ctas))) return rc;
+            if (lines / l >= 2 * (size_t)ctas || !fits(l / 2)) L = l;
+        }
+        if (!L) return ZQD_OK; // no shape fits: the earlier row kernel runs
+    }
+    int logL = 0;
+    while ((1 << logL) < L) ++logL;
+    int ctas = 0, rc;
+    if ((rc = ctas_for(L, ctas))) return rc;
+    J->nd_row_tma_ctas = (int)std::min<size_t>(std::min<size_t>(lines / L, (size_t)ctas), ncols);
+    J->nd_row_tma_logL = logL;
+    const uint64_t rows_total = (uint64_t)S * J->N * c / 128;
+    const uint64_t dims[3] = {16, rows_total, 1};
+    const uint32_t box[3] = {16, (uint32_t)std::min<uint64_t>(256, (uint64_t)L * n * c / 128), 1};
+    if (encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_row_map), J->psi_save.p, dims, 128, rows_total * 128, box, 256,
+                      true) ||
+        encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_row_map_phi), J->phi.p, dims, 128, rows_total * 128, box, 256,
+                      true))
+        return fail(ZQD_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the row pass");
+    // the momentum-copy form holds the end-of-step state in registers besides the sweep's: with one
+    // state it keeps up with the per-block kernel, with several it does not (one CTA per SM)
+    J->nd_row_tma_phi = S == 1;
+    J->nd_row_tma = true;
+    return ZQD_OK;
+}
 
 } // namespace
 
@@ -232,7 +412,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
         J->h2d += (size_t)S * N * c;
     }
     if ((rc = J->book.alloc(sizeof(NdBook), J->stream))) return rc;
-    if ((rc = J->flags.alloc(2 * sizeof(int), J->stream))) return rc;
+    if ((rc = J->flags.alloc(4 * sizeof(int), J->stream))) return rc; // stopped, never set, TMA error, spare
     const size_t rows = (size_t)o.iterations + 1;
     if ((rc = J->hist.alloc((size_t)J->nsolve * rows * J->hc * sizeof(double), J->stream))) return rc;
     if ((rc = J->fin.alloc((size_t)J->nsolve * J->hc * sizeof(double), J->stream))) return rc;
@@ -243,7 +423,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
     std::vector<Tab<T>> twt(n);
     for (int t = 0; t < n; ++t) twt[t] = mktab<T>(tw[2 * t], tw[2 * t + 1]);
     ZQD_CUDA(cudaMemcpyAsync(J->tw.p, twt.data(), (size_t)n * tb, cudaMemcpyHostToDevice, J->stream));
-    ZQD_CUDA(cudaMemsetAsync(J->flags.p, 0, 2 * sizeof(int), J->stream));
+    ZQD_CUDA(cudaMemsetAsync(J->flags.p, 0, 4 * sizeof(int), J->stream));
     ZQD_CUDA(cudaMemsetAsync(J->hist.p, 0xff, J->hist.bytes, J->stream)); // NaN until written
     J->h2d += (size_t)n * tb + J->pot.bytes;
     NdJob<T> D = describe(J);
@@ -257,6 +437,8 @@ int ZQD_ND_CREATE(zqd_job* J) {
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
     for (auto f : {nd_tile_kernel<T, 2>, nd_tile_kernel<T, 3>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
+    if ((rc = setup_tma(J, ov.tma_w))) return rc;
+    if ((rc = setup_row_tma(J, ov.tma_rows, nrow_blocks))) return rc;
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     return ZQD_OK;
 }
@@ -407,6 +589,17 @@ int enqueue(zqd_job* J) {
 }
 } // namespace
 
+// The TMA-staged passes record a load that never landed in flags[2] (the job's buffers are
+// then suspect): report it as a device error.
+static int check_tma(zqd_job* J) {
+    if (!J->nd_tma && !J->nd_row_tma) return ZQD_OK;
+    int e = 0;
+    ZQD_CUDA(cudaMemcpyAsync(&e, J->flags.as<int>() + 2, sizeof(int), cudaMemcpyDeviceToHost, J->stream));
+    ZQD_CUDA(cudaStreamSynchronize(J->stream));
+    J->d2h += sizeof(int);
+    return e ? fail(ZQD_ERR_DEVICE, "A TMA LOAD OF AN AXIS PASS DID NOT COMPLETE WITHIN ITS WAIT BUDGET") : ZQD_OK;
+}
+
 // Rows i0..i1 of solve s (zqd_job_step), launched directly; then, if the solve ended (its last
 // step, or stop_norm), its final observables.  *rows: rows of the solve's history written so far.
 int ZQD_ND_STEP(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
@@ -426,6 +619,7 @@ int ZQD_ND_STEP(zqd_job* J, int s, int i0, int i1, int* rows, int* ended) {
     J->d2h += sizeof(flags);
     *rows = flags[1];
     *ended = flags[0] || i1 >= q.iters;
+    if ((rc = check_tma(J))) return rc;
     if (*ended && (rc = q.epilogue(s))) return rc;
     ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
@@ -445,7 +639,7 @@ int ZQD_ND_RUN(zqd_job* J) {
         ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
         ZQD_CUDA(cudaStreamSynchronize(J->stream));
         ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
-        return ZQD_OK;
+        return check_tma(J);
     }
     if (!J->nd_graph) {
         ZQD_CUDA(cudaStreamBeginCapture(J->stream, cudaStreamCaptureModeThreadLocal));
@@ -467,7 +661,7 @@ int ZQD_ND_RUN(zqd_job* J) {
     ZQD_CUDA(cudaEventRecord(J->ev1, J->stream));
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     ZQD_CUDA(cudaEventElapsedTime(&J->last_ms, J->ev0, J->ev1));
-    return ZQD_OK;
+    return check_tma(J);
 }
 
 } // namespace zqd

@@ -21,6 +21,7 @@
 #include "cx.cuh"
 #include "line_kernel.cuh"
 #include "physics.cuh"
+#include "tma.cuh"
 
 namespace zqd {
 
@@ -67,6 +68,7 @@ template <typename T> struct NdJob {
     int rows_per_cta; // row pass: rows of the last axis per CTA
     int tile, logtile; // tile pass: lines per CTA (a power of two) and its log2
     int* stopped;     // set by the finalize kernel when stop_norm ends the solve
+    int* err;         // set when a TMA load did not land within its wait budget
     PotDev pot;
 };
 
@@ -661,9 +663,10 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
 // points in batches of four and loads the global inputs of the whole batch first (its
 // loads would otherwise wait one after the other); several states keep one point at a
 // time within the registers.  Returns after a barrier.
-template <typename T, int D, int S, int NV>
-__device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T>* phi_src, int ldp, int L, size_t row0,
-                                             uint32_t mode, uint32_t obs, double (&acc)[NV]) {
+// bx(line, x): where point x of line s L + l sits in buf (and phi_src)
+template <typename T, int D, int S, int NV, typename BX>
+__device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T>* phi_src, const BX& bx, int L, size_t row0,
+                                             uint32_t mode, uint32_t obs, double (&acc)[NV], bool wfn = true) {
     using SL = Slots<D, S>;
     constexpr int SB = S == 1 ? 4 : 1;
     using Aux = NdAux<T, S, (SB > 1)>;
@@ -673,7 +676,8 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
     NdNeed nd;
     nd.R = mode & (RM_REND | RM_RSTART);
     nd.w = J.track && nd.R;
-    nd.U = adia && (nd.w || (obsv && (obs & WM_POP)) || J.wfn_out);
+    const bool wout = wfn && J.wfn_out;
+    nd.U = adia && (nd.w || (obsv && (obs & WM_POP)) || wout);
     nd.V = obsv && (obs & (WM_EPOT | WM_ETOT));
     nd.z0 = obsv && (obs & WM_ACF);
     for (int it0 = threadIdx.x; it0 < pts; it0 += SB * nt) {
@@ -689,7 +693,7 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
             const size_t g = row0 + it;
             cx<T> v[S];
 #pragma unroll
-            for (int s = 0; s < S; ++s) v[s] = buf[(s * L + l) * ldp + padx<T>(x)];
+            for (int s = 0; s < S; ++s) v[s] = buf[bx(s * L + l, x)];
             if (mode & RM_INV)
 #pragma unroll
                 for (int s = 0; s < S; ++s) v[s] = scale<T>(v[s], inv_n);
@@ -698,7 +702,7 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
                 a[b].R.apply(v);
             }
             if (obsv) nd_observe<T, D, S>(J, v, g, obs, a[b], acc);
-            if (J.wfn_out) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
+            if (wout) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
 #pragma unroll
                 for (int i = 0; i < S; ++i) {
                     cx<T> y = v[i];
@@ -717,13 +721,13 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
             }
             if (phi_src)
 #pragma unroll
-                for (int s = 0; s < S; ++s) phi_src[(s * L + l) * ldp + padx<T>(x)] = v[s];
+                for (int s = 0; s < S; ++s) phi_src[bx(s * L + l, x)] = v[s];
             if (mode & RM_RSTART) {
                 if (J.track) nd_absorbed<T, S, SL::absn>(J, v, g, a[b], acc);
                 a[b].R.apply(v);
             }
 #pragma unroll
-            for (int s = 0; s < S; ++s) buf[(s * L + l) * ldp + padx<T>(x)] = v[s];
+            for (int s = 0; s < S; ++s) buf[bx(s * L + l, x)] = v[s];
         }
     }
     __syncthreads();
@@ -782,7 +786,8 @@ __global__ void __launch_bounds__(MAXT)
         double acc[SL::count];
 #pragma unroll
         for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
-        nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr, ldp, L, row0, mode, obs, acc);
+        nd_row_sweep<T, D, S>(J, cur, (mode & RM_PHI) ? oth : nullptr,
+                              [ldp](int line, int x) { return line * ldp + padx<T>(x); }, L, row0, mode, obs, acc);
         if (mode & (RM_OBS | RM_REND | RM_RSTART)) {
             // the slots this launch accumulates (nd_observe adds norm always, the rest by mask)
             constexpr uint32_t sm = (1u << S) - 1u;
@@ -960,6 +965,420 @@ __global__ void __launch_bounds__(512)
             for (int r = 0; r < 8; ++r) data[c0 + ((size_t)(i + (r << logm)) << lstride) + g] = v[k][r];
         }
     }
+}
+
+// ------------------------------------------------------------ tile pass, TMA-staged and persistent
+// A tile is W consecutive lines of one state along a strided axis, held as the TMA box lands:
+// element t of line g at t * W + g (rows of W * c bytes).  Each CTA loops over the tiles
+// k = blockIdx.x + j * gridDim.x; while it transforms tile j in one stage buffer, the TMA load
+// of tile j + 1 fills the other, and tile j leaves through a TMA store.  The radix passes run in
+// place in the stage buffer (every thread reads its inputs, a barrier, then the writes), so a
+// tile needs no second line buffer; the first and last radix-8 passes stay in registers.
+constexpr int NDT_STAGES = 2;
+constexpr long long NDT_WAIT_CYCLES = 4000000000LL; // ~2 s: a TMA load that has not landed by then has failed
+
+struct NdTma {
+    int axis;
+    uint32_t mode;  // TM_FWD, TM_KPHASE, TM_INV
+    int logW;       // lines per tile
+    int logtiles;   // tiles per state
+    int logO;       // outer lines (planes of the tensor map) per state
+    unsigned nitems; // tiles of all states
+};
+
+template <typename T> __host__ __device__ inline size_t ndt_stage_bytes(int W, int n) { return (size_t)W * n * sizeof(cx<T>); }
+// stages, twiddles (W_n, then both directions' middle-pass tables), the stage mbarriers, and
+// 128 bytes of slack to align the stages
+template <typename T> __host__ __device__ inline size_t ndt_smem_bytes(int W, int n) {
+    return 128 + (size_t)NDT_STAGES * ndt_stage_bytes<T>(W, n) + (size_t)(n + 2 * nd_mid_tw(n)) * sizeof(Tab<T>) +
+           NDT_STAGES * sizeof(uint64_t);
+}
+
+// Where element t of line g of a stage sits, and which (line, butterfly) pair item `it` of a
+// pass handles.  IxTile: the strided-axis tile, t-major as the TMA box lands (t W + g), lines
+// fastest across threads.  IxRow: lines of the last axis, line-major (g n + t) under the 128-byte
+// TMA swizzle (16-byte chunk j of 128-byte row q stored at chunk j ^ (q mod 8)), points fastest.
+struct IxTile {
+    int logW;
+    __device__ __forceinline__ int at(int g, int t) const { return (t << logW) + g; }
+    __device__ __forceinline__ void item(int it, int logi, int& g, int& i) const {
+        g = it & ((1 << logW) - 1);
+        i = it >> logW;
+        (void)logi;
+    }
+};
+template <typename T> struct IxRow {
+    int logn;
+    __device__ __forceinline__ int operator()(int g, int t) const { return at(g, t); }
+    __device__ __forceinline__ int at(int g, int t) const {
+        const int e = (g << logn) + t;
+        if constexpr (sizeof(cx<T>) == 16) return e ^ ((e >> 3) & 7);
+        else return e ^ (((e >> 4) & 7) << 1);
+    }
+    __device__ __forceinline__ void item(int it, int logi, int& g, int& i) const {
+        i = it & ((1 << logi) - 1);
+        g = it >> logi;
+    }
+};
+
+// In-place radix-R Stockham pass over a stage's lines.  Butterfly (g, i), i < n/R, reads
+// elements i + r n/R and writes o0 + r p; all reads come before the barrier, all writes after
+// it.  twp: W_n^(r kk n/(p R)) at [(r - 1) p + kk].
+template <typename T, int R, int SIGN, typename IX>
+__device__ __forceinline__ void ndt_pass(cx<T>* buf, const IX& ix, int logn, int p, const Tab<T>* __restrict__ twp) {
+    constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : 3;
+    constexpr int B = 8 / R; // butterflies per thread (the CTA has one thread per 8 points)
+    const int logmr = logn - LR, nt = blockDim.x;
+    cx<T> v[B][R];
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        int g, i;
+        ix.item(threadIdx.x + b * nt, logmr, g, i);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = buf[ix.at(g, i + (r << logmr))];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        int g, i;
+        ix.item(threadIdx.x + b * nt, logmr, g, i);
+        const int kk = i & (p - 1);
+        if (p > 1) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[b][r] = tmul<SIGN>(v[b][r], twp[(r - 1) * p + kk]);
+        }
+        dft<R, SIGN, T>(v[b]);
+        const int o0 = ((i - kk) << LR) + kk;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[ix.at(g, o0 + r * p)] = v[b][r];
+    }
+    __syncthreads();
+}
+
+// One n-point transform of a stage's lines, in place.  In: v[r] = element i + r n/8 of line g
+// (the thread's item).  Out: the same elements of the transformed line.  The buffer's contents
+// are free on entry (the barrier before the first write lets every thread finish reading it)
+// and hold nothing of value on return.
+template <typename T, int SIGN, typename IX>
+__device__ __forceinline__ void ndt_fft(cx<T> (&v)[8], cx<T>* buf, const IX& ix, int logn, const Tab<T>* __restrict__ twm) {
+    dft<8, SIGN, T>(v);
+    if (logn == 3) return;
+    const NdSched sc = nd_sched(logn);
+    const int logm = logn - 3;
+    int g, i;
+    ix.item(threadIdx.x, logm, g, i);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 8; ++r) buf[ix.at(g, (i << 3) + r)] = v[r]; // first pass, p = 1: outputs at 8 i + r
+    __syncthreads();
+    const Tab<T>* twd = twm + (1 << logn) + (SIGN > 0 ? nd_mid_tw(1 << logn) : 0);
+    int logp = 3, tbase = 0;
+    for (int j = 0; j < sc.nmid; ++j) {
+        const int lr = sc.lr(j, SIGN > 0 && sc.last8), p = 1 << logp;
+        if (lr == 3) ndt_pass<T, 8, SIGN>(buf, ix, logn, p, twd + tbase);
+        else if (lr == 2) ndt_pass<T, 4, SIGN>(buf, ix, logn, p, twd + tbase);
+        else ndt_pass<T, 2, SIGN>(buf, ix, logn, p, twd + tbase);
+        tbase += ((1 << lr) - 1) * p;
+        logp += lr;
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = buf[ix.at(g, i + (r << logm))];
+    if (sc.last8) { // last radix-8 pass, p = n/8: twiddle W_n^(r i)
+#pragma unroll
+        for (int r = 1; r < 8; ++r) v[r] = tmul<SIGN>(v[r], twm[r * i]);
+        dft<8, SIGN, T>(v);
+    }
+}
+
+// map: 3-D tensor map of this axis over psi in 8-byte words: [E * stride] words (the inner
+// lines), [n] rows along the axis, [S * O] planes (outer index and state); box [E W, min(n, 256), 1]
+template <typename T, int D>
+__global__ void __launch_bounds__(512)
+    nd_tile_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map, const NdTma P) {
+    if (*J.stopped) return;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    const int n = J.n, logn = J.logn, logm = logn - 3, logW = P.logW, W = 1 << logW;
+    const int lstride = logn * (D - 1 - P.axis);
+    constexpr int E = (int)(sizeof(cx<T>) / 8);
+    const size_t sb = ndt_stage_bytes<T>(W, n);
+    cx<T>* stage0 = reinterpret_cast<cx<T>*>(base);
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(base + NDT_STAGES * sb);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(twm + n + 2 * nd_mid_tw(n));
+    const int tid = threadIdx.x, g = tid & (W - 1), i = tid >> logW;
+    const int rows = n < 256 ? n : 256;
+    // tile k: state s = k >> logtiles, lines l0 = (k mod tiles) W of that state; box origin
+    // x = E (l0 mod stride) words, plane z = s O + l0 / stride
+    auto origin = [&](unsigned k, int& x, int& z, size_t& gbase) {
+        const unsigned s = k >> P.logtiles;
+        const size_t l0 = (size_t)(k & ((1u << P.logtiles) - 1u)) << logW;
+        const size_t inner0 = l0 & (((size_t)1 << lstride) - 1), outer = l0 >> lstride;
+        x = E * (int)inner0;
+        z = (int)(((size_t)s << P.logO) + outer);
+        gbase = ((outer << logn) << lstride) + inner0; // grid index of element 0 of the tile's line 0
+    };
+    auto issue = [&](unsigned k, int st) {
+        int x, z;
+        size_t gb;
+        origin(k, x, z, gb);
+        cx<T>* dst = stage0 + (size_t)st * W * n;
+        mbar_arrive_expect_tx(&bars[st], (unsigned)sb);
+        for (int y = 0; y < n; y += rows) tma_load_3d(dst + (size_t)y * W, &map, x, y, z, &bars[st]);
+    };
+    if (tid == 0) {
+        prefetch_tensormap(&map);
+#pragma unroll
+        for (int s = 0; s < NDT_STAGES; ++s) mbar_init(&bars[s], 1);
+        fence_barrier_init();
+    }
+    for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    nd_stage_mid_tw<T>(J.tw, twm + n, logn);
+    __syncthreads();
+    if (tid == 0 && blockIdx.x < P.nitems) issue(blockIdx.x, 0);
+    int j = 0;
+    for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
+        const int st = j & 1;
+        const unsigned kn = k + gridDim.x;
+        if (tid == 0 && kn < P.nitems) {
+            bulk_wait_read_all(); // the store of tile j - 1 has read the other stage
+            issue(kn, st ^ 1);
+        }
+        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, NDT_WAIT_CYCLES);
+        if (!__syncthreads_and(ok)) { // the load never landed: record it, let the prefetch land, stop
+            if (tid == 0) {
+                atomicExch(J.err, 1);
+                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, NDT_WAIT_CYCLES);
+            }
+            break;
+        }
+        cx<T>* buf = stage0 + (size_t)st * W * n;
+        int x, z;
+        size_t gbase;
+        origin(k, x, z, gbase);
+        const IxTile ix{logW};
+        cx<T> v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = buf[ix.at(g, i + (r << logm))];
+        if (P.mode & TM_FWD) ndt_fft<T, -1>(v, buf, ix, logn, twm);
+        if (P.mode & TM_KPHASE) {
+            // exp(Complex(0, -K) * dt), K = sum_j k_j^2 / (2 m_j) (quantum_dynamics.zig:397-399), as the
+            // product of per-axis factors: the line's other axes once, then one product per element
+            const size_t gl = gbase + g;
+            double2 fl = make_double2(1.0, 0.0);
+#pragma unroll
+            for (int a = 0; a < D; ++a)
+                if (a != P.axis) {
+                    const double2 e = J.kphase[a * n + axis_index<D>(gl, a, logn)];
+                    fl = make_double2(__dsub_rn(__dmul_rn(fl.x, e.x), __dmul_rn(fl.y, e.y)),
+                                      __dadd_rn(__dmul_rn(fl.x, e.y), __dmul_rn(fl.y, e.x)));
+                }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const double2 f0 = J.kphase[P.axis * n + i + (r << logm)];
+                const double2 f = make_double2(__dsub_rn(__dmul_rn(f0.x, fl.x), __dmul_rn(f0.y, fl.y)),
+                                               __dadd_rn(__dmul_rn(f0.x, fl.y), __dmul_rn(f0.y, fl.x)));
+                v[r] = tmul<-1>(v[r], mktab<T>(f.x, f.y));
+            }
+        }
+        if (P.mode & TM_INV) ndt_fft<T, 1>(v, buf, ix, logn, twm);
+        __syncthreads(); // every thread's last-pass reads are done
+#pragma unroll
+        for (int r = 0; r < 8; ++r) buf[ix.at(g, i + (r << logm))] = v[r];
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            for (int y = 0; y < n; y += rows) tma_store_3d(&map, x, y, z, buf + (size_t)y * W);
+            bulk_commit();
+        }
+    }
+    if (tid == 0) bulk_wait_all();
+}
+
+// ------------------------------------------------------------ row pass, TMA-staged and persistent
+// An item is a block of L rows of the last axis with all S states (the row pass's unit of work);
+// its stage holds line g = s L + l (g n + t, 128-byte swizzled, IxRow) as the TMA boxes land.
+// Each CTA loops over the blocks k = blockIdx.x + j * gridDim.x with the next block's load in
+// flight and the next block's propagator table prefetched into L2.  The observables' sums run
+// over all of a CTA's blocks and are written once, at column blockIdx.x of the partial array;
+// the columns no CTA owns are written as zero so that the region stays whole.  Modes: any
+// combination of the row-pass modes.  RM_PHI keeps the end-of-step state in registers while the
+// start of the next step is applied, and transforms it through the stage after the psi store has
+// read it; it leaves through map_phi.
+struct NdRowTma {
+    uint32_t mode, obs;
+    int logL;        // rows per block
+    unsigned nitems; // blocks
+    unsigned ncols;  // columns of the partial-sum region (the earlier kernel's block count)
+};
+
+template <typename T> __host__ __device__ inline size_t ndr_stage_bytes(int S, int L, int n) {
+    return (size_t)S * L * n * sizeof(cx<T>);
+}
+// 1024 bytes of slack to align the stages (the 128-byte swizzle repeats every 1024 bytes), the
+// stages, the twiddles, the stage mbarriers
+template <typename T> __host__ __device__ inline size_t ndr_smem_bytes(int S, int L, int n) {
+    return 1024 + (size_t)NDT_STAGES * ndr_stage_bytes<T>(S, L, n) + (size_t)(n + 2 * nd_mid_tw(n)) * sizeof(Tab<T>) +
+           NDT_STAGES * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(p)), "r"(bytes) : "memory");
+}
+
+// map: 3-D tensor map over psi as rows of 128 bytes: [16 words] x [S N c / 128 rows] x [1],
+// box [16, min(256, L n c / 128), 1], 128-byte swizzle
+// The TMA row pass's CTA size bound.  Two CTAs per SM (128 registers) for the plain forms; the
+// form with the momentum copy keeps one (its registers hold the end-of-step state as well).
+constexpr int NDR_THREADS = 256;
+
+template <typename T, int D, int S, bool PHI>
+__global__ void __launch_bounds__(NDR_THREADS, PHI ? 1 : 2)
+    nd_row_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map,
+                      const __grid_constant__ CUtensorMap map_phi, const NdRowTma P, size_t part_base,
+                      const __grid_constant__ NdFin F) {
+    if (*J.stopped) return;
+    using SL = Slots<D, S>;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    const int n = J.n, logn = J.logn, logm = logn - 3, L = 1 << P.logL;
+    const size_t sb = ndr_stage_bytes<T>(S, L, n), blk = (size_t)L * n; // points of one state in a block
+    cx<T>* stage0 = reinterpret_cast<cx<T>*>(base);
+    Tab<T>* twm = reinterpret_cast<Tab<T>*>(base + NDT_STAGES * sb);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(twm + n + 2 * nd_mid_tw(n));
+    const int tid = threadIdx.x;
+    const unsigned rows_state = (unsigned)(blk * sizeof(cx<T>) / 128), rows_box = rows_state < 256 ? rows_state : 256;
+    const uint32_t mode = PHI ? P.mode : (P.mode & ~(uint32_t)RM_PHI);
+    const bool needR = mode & (RM_REND | RM_RSTART);
+    auto issue = [&](unsigned k, int st) {
+        unsigned char* dst = base + (size_t)st * sb;
+        mbar_arrive_expect_tx(&bars[st], (unsigned)sb);
+        for (int s = 0; s < S; ++s) {
+            const size_t row = ((size_t)s * J.N + (size_t)k * blk) * sizeof(cx<T>) / 128;
+            for (unsigned y = 0; y < rows_state; y += rows_box)
+                tma_load_3d(dst + ((size_t)s * rows_state + y) * 128, &map, 0, (int)(row + y), 0, &bars[st]);
+        }
+        if (needR) // the block's propagator entries, for the sweep's loads
+            for (int c = 0; c < S * (S + 1) / 2; ++c) prefetch_l2(J.R + (size_t)c * J.N + (size_t)k * blk, (unsigned)(blk * sizeof(Tab<T>)));
+    };
+    if (tid == 0) {
+        prefetch_tensormap(&map);
+#pragma unroll
+        for (int s = 0; s < NDT_STAGES; ++s) mbar_init(&bars[s], 1);
+        fence_barrier_init();
+    }
+    for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
+    nd_stage_mid_tw<T>(J.tw, twm + n, logn);
+    __syncthreads();
+    double acc[SL::count];
+#pragma unroll
+    for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
+    const IxRow<T> ix{logn};
+    int g, i;
+    ix.item(tid, logm, g, i);
+    if (tid == 0 && blockIdx.x < P.nitems) issue(blockIdx.x, 0);
+    bool failed = false;
+    int j = 0;
+    for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
+        const int st = j & 1;
+        const unsigned kn = k + gridDim.x;
+        if (j > 0) __syncthreads(); // every thread is done with block j - 1's stage (a block need not be stored)
+        if (tid == 0 && kn < P.nitems) {
+            bulk_wait_read_all(); // the store of block j - 1 has read the other stage
+            issue(kn, st ^ 1);
+        }
+        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, NDT_WAIT_CYCLES);
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) {
+                atomicExch(J.err, 1);
+                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, NDT_WAIT_CYCLES);
+            }
+            failed = true;
+            break;
+        }
+        cx<T>* buf = stage0 + (size_t)st * S * blk;
+        const size_t row0 = (size_t)k * blk;
+        cx<T> v[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[r] = buf[ix.at(g, i + (r << logm))];
+        if (mode & RM_INV) ndt_fft<T, 1>(v, buf, ix, logn, twm);
+        cx<T> w[8]; // RM_PHI: the end-of-step state, for its forward transform into phi
+        if (mode & (RM_INV | RM_REND | RM_OBS | RM_RSTART | RM_PHI)) { // per-point stages in natural order
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 8; ++r) buf[ix.at(g, i + (r << logm))] = v[r];
+            __syncthreads();
+            if (PHI) { // end of step i, the copy, then the start of step i+1
+                nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, mode & ~(uint32_t)RM_RSTART, P.obs, acc);
+#pragma unroll
+                for (int r = 0; r < 8; ++r) w[r] = buf[ix.at(g, i + (r << logm))];
+                if (mode & RM_RSTART) {
+                    __syncthreads();
+                    nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, RM_RSTART, 0u, acc, false);
+                }
+            } else {
+                nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, mode, P.obs, acc);
+            }
+            if (mode & (RM_FWD | RM_STORE))
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[r] = buf[ix.at(g, i + (r << logm))];
+        }
+        if (mode & RM_FWD) ndt_fft<T, -1>(v, buf, ix, logn, twm);
+        if (mode & RM_STORE) {
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 8; ++r) buf[ix.at(g, i + (r << logm))] = v[r];
+            fence_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                for (int s = 0; s < S; ++s) {
+                    const size_t row = ((size_t)s * J.N + row0) * sizeof(cx<T>) / 128;
+                    for (unsigned y = 0; y < rows_state; y += rows_box)
+                        tma_store_3d(&map, 0, (int)(row + y), 0,
+                                     reinterpret_cast<unsigned char*>(buf) + ((size_t)s * rows_state + y) * 128);
+                }
+                bulk_commit();
+            }
+        }
+        if (PHI) { // forward transform of the end-of-step copy, through the same stage, into phi
+            if (tid == 0) bulk_wait_read_all(); // the psi store has read the stage
+            ndt_fft<T, -1>(w, buf, ix, logn, twm);
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < 8; ++r) buf[ix.at(g, i + (r << logm))] = w[r];
+            fence_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                for (int s = 0; s < S; ++s) {
+                    const size_t row = ((size_t)s * J.N + row0) * sizeof(cx<T>) / 128;
+                    for (unsigned y = 0; y < rows_state; y += rows_box)
+                        tma_store_3d(&map_phi, 0, (int)(row + y), 0,
+                                     reinterpret_cast<unsigned char*>(buf) + ((size_t)s * rows_state + y) * 128);
+                }
+                bulk_commit();
+            }
+        }
+    }
+    if (tid == 0) bulk_wait_all();
+    if (failed) return;
+    if (mode & (RM_OBS | RM_REND | RM_RSTART)) {
+        constexpr uint32_t sm = (1u << S) - 1u;
+        uint32_t act = 1u << SL::norm;
+        if (mode & RM_OBS) {
+            if (P.obs & WM_POS) act |= ((1u << D) - 1u) << SL::pos;
+            if (P.obs & (WM_EPOT | WM_ETOT)) act |= 1u << SL::epot;
+            if (P.obs & WM_ACF) act |= 3u << SL::acf;
+            if (P.obs & WM_POP) act |= sm << SL::pop;
+        }
+        if (J.track) act |= (sm << SL::abs) | (sm << SL::absn);
+        block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x, act);
+        for (size_t col = blockIdx.x + gridDim.x; col < P.ncols; col += gridDim.x) // columns no CTA owns
+            for (int v = tid; v < SL::count; v += blockDim.x) {
+                const size_t o = ((size_t)v * J.nparts + part_base + col) * 2;
+                J.part[o] = 0.0;
+                J.part[o + 1] = 0.0;
+            }
+    }
+    if (F.enabled && nd_last_cta(&F.book->counter, gridDim.x)) nd_finalize_cta(J, F);
 }
 
 // per-axis kinetic phase exp(Complex(0, -k_i^2 / (2 m_j)) * dt) (Propagator.init, quantum_dynamics.zig:397-399)

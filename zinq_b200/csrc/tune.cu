@@ -2,7 +2,9 @@
 //
 // The kernels take their shape from fixed rules unless this table holds a measured choice:
 //   1-D  resident line kernel: CTAs per cluster C (1..16) and the largest local radix (4 or 8);
-//   N-D  axis passes: rows of the last axis per row-pass CTA and lines per tile-pass CTA.
+//   N-D  axis passes: rows per block and lines per tile of the TMA-staged persistent passes (or
+//        the per-block kernels instead), and rows of the last axis per per-block row CTA (the
+//        launches that take the per-block kernel).
 // zqd_autotune times every candidate the kernels accept on the current device (a synthetic job of
 // the key's size: harmonic diagonal, constant couplings, populations recorded every step; the
 // propagation's device time from CUDA events, best of three runs) and records the fastest.  The
@@ -50,7 +52,9 @@ int load_file(const char* path, bool replace) {
         if (line[0] == '#' || line[0] == '\n') continue;
         int d, n, S, fp32;
         ShapeOverride s;
-        if (std::sscanf(line, "%d %d %d %d %d %d %d %d", &d, &n, &S, &fp32, &s.C, &s.lrmax, &s.rows, &s.tile) != 8) {
+        const int got_fields = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d", &d, &n, &S, &fp32, &s.C, &s.lrmax, &s.rows,
+                                           &s.tile, &s.tma_rows, &s.tma_w);
+        if (got_fields != 8 && got_fields != 10) { // 8: a table written before the TMA-staged passes
             std::fclose(f);
             return fail(ZQD_ERR_INVALID_INPUT, std::string("tuning table ") + path + ": bad line " + std::to_string(lineno));
         }
@@ -168,27 +172,54 @@ extern "C" int zqd_autotune(zqd_tune_entry* e) {
         r8.C = 16;
         r8.lrmax = 3;
         cands.push_back(r8);
-    } else {
-        for (int L = 1; L <= 64; L <<= 1)
-            for (int Tn = 1; Tn <= 16; Tn <<= 1) {
-                ShapeOverride s;
-                s.rows = L;
-                s.tile = Tn;
-                cands.push_back(s);
-            }
     }
     const double def = time_shape(d, n, S, fp32, ShapeOverride{}); // the rules' own choice
     if (def < 0) return fail(ZQD_ERR_UNSUPPORTED, "THE KERNELS DO NOT SUPPORT THIS KEY");
     ShapeOverride best{};
     double best_us = def;
     uint32_t tried = 0;
-    for (const ShapeOverride& c : cands) {
+    auto consider = [&](const ShapeOverride& c) {
         const double us = time_shape(d, n, S, fp32, c);
-        if (us < 0) continue;
+        if (us < 0) return;
         ++tried;
         if (us < best_us) {
             best_us = us;
             best = c;
+        }
+    };
+    if (d == 1) {
+        for (const ShapeOverride& c : cands) consider(c);
+    } else {
+        // one field at a time, each from the best shape so far: the row pass's blocks (or the
+        // per-block row kernel with its rows per CTA), then the tile pass's lines (or the
+        // per-block tile kernel with its lines per CTA)
+        const ShapeOverride base0 = best;
+        for (int L : {-1, 1, 2, 4, 8, 16, 32, 64}) {
+            ShapeOverride c = base0;
+            c.tma_rows = L;
+            consider(c);
+        }
+        if (best.tma_rows < 0) {
+            const ShapeOverride base1 = best;
+            for (int L = 1; L <= 64; L <<= 1) {
+                ShapeOverride c = base1;
+                c.rows = L;
+                consider(c);
+            }
+        }
+        const ShapeOverride base2 = best;
+        for (int W : {-1, 1, 2, 4, 8, 16}) {
+            ShapeOverride c = base2;
+            c.tma_w = W;
+            consider(c);
+        }
+        if (best.tma_w < 0) {
+            const ShapeOverride base3 = best;
+            for (int Tn = 1; Tn <= 16; Tn <<= 1) {
+                ShapeOverride c = base3;
+                c.tile = Tn;
+                consider(c);
+            }
         }
     }
     e->default_us_per_step = def;
@@ -198,9 +229,11 @@ extern "C" int zqd_autotune(zqd_tune_entry* e) {
     e->radix_log2 = (uint32_t)best.lrmax;
     e->rows_per_cta = (uint32_t)best.rows;
     e->tile_lines = (uint32_t)best.tile;
+    e->tma_row_block = best.tma_rows;
+    e->tma_tile_lines = best.tma_w;
     Table& t = table();
     std::lock_guard<std::mutex> lk(t.mu);
-    if (best.C || best.rows || best.tile) t.shapes[std::make_tuple(d, n, S, fp32 ? 1 : 0)] = best;
+    if (best.C || best.rows || best.tile || best.tma_rows || best.tma_w) t.shapes[std::make_tuple(d, n, S, fp32 ? 1 : 0)] = best;
     else t.shapes.erase(std::make_tuple(d, n, S, fp32 ? 1 : 0)); // the rules' shape won
     return ZQD_OK;
 }
@@ -211,12 +244,13 @@ extern "C" int zqd_tune_save(const char* path) {
     std::lock_guard<std::mutex> lk(t.mu);
     FILE* f = std::fopen(path, "w");
     if (!f) return fail(ZQD_ERR_INVALID_INPUT, std::string("cannot write ") + path);
-    std::fprintf(f, "# ndim npoint nstate fp32 cluster_ctas radix_log2 rows_per_cta tile_lines (0: the rules' choice)\n");
+    std::fprintf(f, "# ndim npoint nstate fp32 cluster_ctas radix_log2 rows_per_cta tile_lines tma_row_block tma_tile_lines"
+                    " (0: the rules' choice; -1: the per-block kernel)\n");
     for (auto& kv : t.shapes) {
         const Key& k = kv.first;
         const ShapeOverride& s = kv.second;
-        std::fprintf(f, "%d %d %d %d %d %d %d %d\n", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k), s.C,
-                     s.lrmax, s.rows, s.tile);
+        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d\n", std::get<0>(k), std::get<1>(k), std::get<2>(k), std::get<3>(k),
+                     s.C, s.lrmax, s.rows, s.tile, s.tma_rows, s.tma_w);
     }
     std::fclose(f);
     return ZQD_OK;
