@@ -64,6 +64,9 @@ struct Opts {
     // derived
     int pot_nd = 0, pot_ns = 0;
     bool pot_td = false;
+    // set by the job server: resident CTAs per SM that an N-D job's persistent (TMA-staged) tile
+    // pass uses, so that the jobs it runs side by side can interleave (0: as many as fit)
+    int tma_ctas_per_sm = 0;
 };
 
 int copy_options(const zqd_options* in, Opts& o);

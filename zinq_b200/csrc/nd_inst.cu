@@ -84,6 +84,15 @@ NdJob<T> describe(zqd_job* J) {
 // and two 256-thread CTAs per SM hide more latency than extra registers would.
 inline bool row_narrow(unsigned threads) { return S > 1 && threads <= 256; }
 
+using RowTmaKernel = void (*)(NdJob<T>, CUtensorMap, CUtensorMap, NdRowTma, size_t, NdFin);
+// the 512-thread plain form of the TMA row kernel (one or two states), or null
+inline RowTmaKernel row_tma_wide(int d) {
+    if constexpr (S <= 2)
+        return d == 2 ? nd_row_tma_kernel<T, 2, S, false, NDR_THREADS_WIDE> : nd_row_tma_kernel<T, 3, S, false, NDR_THREADS_WIDE>;
+    else
+        return nullptr;
+}
+
 struct Launch {
     zqd_job* J;
     NdJob<T> D;
@@ -101,13 +110,13 @@ struct Launch {
             P.obs = obs;
             P.logL = J->nd_row_tma_logL;
             P.nitems = (unsigned)(J->N / J->n >> P.logL);
-            P.ncols = (unsigned)nrow_blocks;
             const size_t smem = ndr_smem_bytes<T>(S, 1 << P.logL, J->n);
             const unsigned nt = (unsigned)((S * J->n << P.logL) / 8), nb = (unsigned)J->nd_row_tma_ctas;
             const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_row_map);
             const CUtensorMap* mphi = reinterpret_cast<const CUtensorMap*>(J->nd_row_map_phi);
             auto kern = (mode & RM_PHI) ? (D.d == 2 ? nd_row_tma_kernel<T, 2, S, true> : nd_row_tma_kernel<T, 3, S, true>)
                                         : (D.d == 2 ? nd_row_tma_kernel<T, 2, S, false> : nd_row_tma_kernel<T, 3, S, false>);
+            if (nt > (unsigned)NDR_THREADS) kern = row_tma_wide(D.d);
             kern<<<nb, nt, smem, J->stream>>>(d, *map, *mphi, P, region, f);
             ZQD_CUDA(cudaGetLastError());
             return ZQD_OK;
@@ -198,6 +207,10 @@ struct Launch {
     }
 };
 
+// resident CTAs per SM the tile pass's persistent grid may use: the job server's setting, else
+// all that fit (the tile pass reduces nothing, so its grid changes no result)
+inline int tma_ctas_per_sm_cap(const zqd_job* J) { return J->o.tma_ctas_per_sm > 0 ? J->o.tma_ctas_per_sm : 1 << 20; }
+
 // The TMA-staged tile pass: lines per tile W (a power of two, W <= n) with rows of W c >= 16
 // bytes (an even number of 8-byte words), W n / 8 threads (whole warps, at most 512) and two stages within the
 // shared-memory budget; by default the widest W up to 64-byte rows whose grid still gives every
@@ -225,7 +238,7 @@ int setup_tma(zqd_job* J, int w_override) {
         ZQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &per_sm, d == 2 ? (const void*)nd_tile_tma_kernel<T, 2> : (const void*)nd_tile_tma_kernel<T, 3>, threads,
             ndt_smem_bytes<T>(W, n)));
-        ctas = std::max(1, per_sm) * sms;
+        ctas = std::max(1, std::min(per_sm, tma_ctas_per_sm_cap(J))) * sms;
         return ZQD_OK;
     };
     const size_t lines = J->N / (size_t)n; // lines of one state along any axis
@@ -258,7 +271,7 @@ int setup_tma(zqd_job* J, int w_override) {
         const uint64_t st = (uint64_t)1 << lstride, O = J->N / ((uint64_t)n * st);
         const uint64_t dims[3] = {(uint64_t)E * st, (uint64_t)n, (uint64_t)S * O};
         const uint32_t box[3] = {(uint32_t)(E * W), (uint32_t)std::min(n, 256), 1};
-        const int l2 = W * c >= 128 ? 128 : 0;
+        const int l2 = W * c >= 128 ? 128 : 0; // (promotion measured no faster on narrower rows)
         const int e = encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_maps[a]), J->psi_save.p, dims, st * c,
                                     (uint64_t)n * st * c, box, l2);
         if (e) return fail(ZQD_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the tile pass");
@@ -269,12 +282,14 @@ int setup_tma(zqd_job* J, int w_override) {
 
 // The TMA-staged row pass: L rows (a power of two dividing N/n) per block with L n c >= 1024 bytes
 // (the stages keep the 128-byte swizzle's 1024-byte alignment), S L n / 8 threads (whole warps, at
-// most 256: the sweep, the sums and the momentum copy keep their registers) and two stages within the budget; by default the largest L up to
-// about 2048 points per block whose grid still gives every resident CTA two blocks.  The grid is
-// at most the earlier kernel's block count (the width of the partial-sum regions).
+// most 256, or 512 for one or two states on lines too long for 256; the momentum copy then takes
+// the per-block kernel) and two stages within the budget; by default the largest L of at most 256
+// threads (the wide form only where no 256-thread block fits).  The grid takes every resident CTA
+// (jobs created by the server too: its observables' sums are grouped per CTA, so a job's results
+// depend on its grid, which must not change with where it runs).
 // l_override: 0 keeps the default, -1 keeps the earlier row kernel, else L.  ZQD_ND_TMA=0 also
 // keeps it.
-int setup_row_tma(zqd_job* J, int l_override, size_t ncols) {
+int choose_row_tma(zqd_job* J, int l_override) {
     constexpr int c = (int)sizeof(cx<T>);
     const int n = J->n, d = J->d;
     const size_t budget = 200 * 1024, lines = J->N / (size_t)n;
@@ -287,16 +302,22 @@ int setup_row_tma(zqd_job* J, int l_override, size_t ncols) {
     for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>, nd_row_tma_kernel<T, 2, S, true>,
                    nd_row_tma_kernel<T, 3, S, true>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+    for (int dd : {2, 3})
+        if (RowTmaKernel f = row_tma_wide(dd))
+            ZQD_CUDA(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     auto threads_of = [&](int L) { return (size_t)S * L * n / 8; };
     auto fits = [&](int L) {
         const size_t t = threads_of(L);
         // whole warps: the block reduction's shuffles run on full warps
         return L >= 1 && (size_t)L <= lines && lines % (size_t)L == 0 && (size_t)L * n * c >= 1024 && t % 32 == 0 &&
-               t <= (size_t)NDR_THREADS && ndr_smem_bytes<T>(S, L, n) <= budget;
+               (t <= (size_t)NDR_THREADS || (t <= (size_t)NDR_THREADS_WIDE && row_tma_wide(d))) &&
+               ndr_smem_bytes<T>(S, L, n) <= budget;
     };
     auto ctas_for = [&](int L, int& ctas) -> int {
         const unsigned nt = (unsigned)threads_of(L);
-        const void* f = d == 2 ? (const void*)nd_row_tma_kernel<T, 2, S, false> : (const void*)nd_row_tma_kernel<T, 3, S, false>;
+        const void* f = nt > (unsigned)NDR_THREADS ? (const void*)row_tma_wide(d)
+                        : d == 2                   ? (const void*)nd_row_tma_kernel<T, 2, S, false>
+                                                   : (const void*)nd_row_tma_kernel<T, 3, S, false>;
         int per_sm = 0;
         ZQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, (int)nt, ndr_smem_bytes<T>(S, L, n)));
         ctas = std::max(1, per_sm) * sms;
@@ -308,21 +329,28 @@ int setup_row_tma(zqd_job* J, int l_override, size_t ncols) {
     else if (el && atoi(el) > 0) L = atoi(el);
     if (L) {
         if (!fits(L)) return fail(ZQD_ERR_UNSUPPORTED, "TMA ROW-BLOCK SHAPE OUTSIDE THE KERNEL'S LIMITS");
-    } else {
-        for (int l = std::max(1, 2048 / (S * n)); l >= 1 && !L; l >>= 1) {
-            if (!fits(l)) continue;
-            int ctas = 0, rc;
-            if ((rc = ctas_for(l, ctas))) return rc;
-            if (lines / l >= 2 * (size_t)ctas || !fits(l / 2)) L = l;
-        }
+    } else { // the largest block of at most 256 threads (measured: fewer, larger CTAs win), else the wide form
+        for (int l = std::max(1, 4096 / (S * n)); l >= 1 && !L; l >>= 1)
+            if (fits(l) && (threads_of(l) <= (size_t)NDR_THREADS || !fits(l / 2))) L = l;
         if (!L) return ZQD_OK; // no shape fits: the earlier row kernel runs
     }
     int logL = 0;
     while ((1 << logL) < L) ++logL;
     int ctas = 0, rc;
     if ((rc = ctas_for(L, ctas))) return rc;
-    J->nd_row_tma_ctas = (int)std::min<size_t>(std::min<size_t>(lines / L, (size_t)ctas), ncols);
+    J->nd_row_tma_ctas = (int)std::min<size_t>(lines / L, (size_t)ctas);
     J->nd_row_tma_logL = logL;
+    // the momentum-copy form holds the end-of-step state in registers besides the sweep's: with one
+    // state it keeps up with the per-block kernel, with several it does not (one CTA per SM)
+    J->nd_row_tma_phi = S == 1 && threads_of(L) <= (size_t)NDR_THREADS;
+    J->nd_row_tma = true;
+    return ZQD_OK;
+}
+
+// the row pass's tensor maps over psi and phi (after they are allocated)
+int encode_row_tma(zqd_job* J) {
+    constexpr int c = (int)sizeof(cx<T>);
+    const int L = 1 << J->nd_row_tma_logL, n = J->n;
     const uint64_t rows_total = (uint64_t)S * J->N * c / 128;
     const uint64_t dims[3] = {16, rows_total, 1};
     const uint32_t box[3] = {16, (uint32_t)std::min<uint64_t>(256, (uint64_t)L * n * c / 128), 1};
@@ -331,10 +359,6 @@ int setup_row_tma(zqd_job* J, int l_override, size_t ncols) {
         encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_row_map_phi), J->phi.p, dims, 128, rows_total * 128, box, 256,
                       true))
         return fail(ZQD_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the row pass");
-    // the momentum-copy form holds the end-of-step state in registers besides the sweep's: with one
-    // state it keeps up with the per-block kernel, with several it does not (one CTA per SM)
-    J->nd_row_tma_phi = S == 1;
-    J->nd_row_tma = true;
     return ZQD_OK;
 }
 
@@ -386,9 +410,22 @@ int ZQD_ND_CREATE(zqd_job* J) {
         }
     }
     J->nd_tile_threads = std::max(32, (Tn * n / 8 + 31) / 32 * 32);
+    int rc;
+    // The TMA-staged row pass, where a shape fits: the per-block row kernel (the launches the TMA
+    // form does not take) uses the same rows per block, so both write every column of a partial-sum
+    // region, one column per block.
+    if ((rc = choose_row_tma(J, ov.tma_rows))) return rc;
+    if (J->nd_row_tma) {
+        const int Lt = 1 << J->nd_row_tma_logL;
+        if (S * Lt * n / 8 <= max_items && nd_smem_bytes<T>(J->nd_row_bufs, S * Lt, n) <= (size_t)budget) {
+            J->nd_rows = L = Lt;
+            J->nd_row_threads = std::max(32, (S * L * n / 8 + 31) / 32 * 32);
+        } else {
+            J->nd_row_tma = false;
+        }
+    }
     const size_t nrow_blocks = N / n / L, ntile_blocks = N / n / Tn;
     const size_t nparts = 3 * nrow_blocks + S * ntile_blocks + 1024;
-    int rc;
     if ((rc = J->psi_save.alloc((size_t)S * N * c, J->stream))) return rc;
     if ((rc = J->phi.alloc((size_t)S * N * c, J->stream))) return rc;
     if ((o.has_spectrum || (o.write_mask & ZQD_WRITE_ACF)) && (rc = J->psi0.alloc((size_t)S * N * c, J->stream))) return rc;
@@ -438,7 +475,7 @@ int ZQD_ND_CREATE(zqd_job* J) {
     for (auto f : {nd_tile_kernel<T, 2>, nd_tile_kernel<T, 3>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, budget));
     if ((rc = setup_tma(J, ov.tma_w))) return rc;
-    if ((rc = setup_row_tma(J, ov.tma_rows, nrow_blocks))) return rc;
+    if (J->nd_row_tma && (rc = encode_row_tma(J))) return rc;
     ZQD_CUDA(cudaStreamSynchronize(J->stream));
     return ZQD_OK;
 }

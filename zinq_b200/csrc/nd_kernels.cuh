@@ -1199,16 +1199,16 @@ __global__ void __launch_bounds__(512)
 // its stage holds line g = s L + l (g n + t, 128-byte swizzled, IxRow) as the TMA boxes land.
 // Each CTA loops over the blocks k = blockIdx.x + j * gridDim.x with the next block's load in
 // flight and the next block's propagator table prefetched into L2.  The observables' sums run
-// over all of a CTA's blocks and are written once, at column blockIdx.x of the partial array;
-// the columns no CTA owns are written as zero so that the region stays whole.  Modes: any
+// over all of a CTA's blocks and are written once, at column blockIdx.x of the partial array
+// (the grid's size is fixed per job and device); the columns no CTA owns are written as zero so
+// that the region stays whole.  Modes: any
 // combination of the row-pass modes.  RM_PHI keeps the end-of-step state in registers while the
 // start of the next step is applied, and transforms it through the stage after the psi store has
 // read it; it leaves through map_phi.
 struct NdRowTma {
     uint32_t mode, obs;
     int logL;        // rows per block
-    unsigned nitems; // blocks
-    unsigned ncols;  // columns of the partial-sum region (the earlier kernel's block count)
+    unsigned nitems; // blocks, and columns of the partial-sum region
 };
 
 template <typename T> __host__ __device__ inline size_t ndr_stage_bytes(int S, int L, int n) {
@@ -1227,12 +1227,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
 
 // map: 3-D tensor map over psi as rows of 128 bytes: [16 words] x [S N c / 128 rows] x [1],
 // box [16, min(256, L n c / 128), 1], 128-byte swizzle
-// The TMA row pass's CTA size bound.  Two CTAs per SM (128 registers) for the plain forms; the
-// form with the momentum copy keeps one (its registers hold the end-of-step state as well).
-constexpr int NDR_THREADS = 256;
+// The TMA row pass's CTA size bound MAXT: 256 threads, two CTAs per SM (128 registers) for the
+// plain forms, one for the form with the momentum copy (its registers hold the end-of-step state
+// as well); 512 threads, one CTA per SM (128 registers), for the plain forms of one or two
+// states on long lines.
+constexpr int NDR_THREADS = 256, NDR_THREADS_WIDE = 512;
 
-template <typename T, int D, int S, bool PHI>
-__global__ void __launch_bounds__(NDR_THREADS, PHI ? 1 : 2)
+template <typename T, int D, int S, bool PHI, int MAXT = NDR_THREADS>
+__global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? 2 : 1)
     nd_row_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map,
                       const __grid_constant__ CUtensorMap map_phi, const NdRowTma P, size_t part_base,
                       const __grid_constant__ NdFin F) {
@@ -1269,6 +1271,18 @@ __global__ void __launch_bounds__(NDR_THREADS, PHI ? 1 : 2)
     for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
     nd_stage_mid_tw<T>(J.tw, twm + n, logn);
     __syncthreads();
+    const bool sums = mode & (RM_OBS | RM_REND | RM_RSTART);
+    uint32_t act = 1u << SL::norm; // the slots this launch accumulates (nd_observe adds norm always)
+    {
+        constexpr uint32_t sm = (1u << S) - 1u;
+        if (mode & RM_OBS) {
+            if (P.obs & WM_POS) act |= ((1u << D) - 1u) << SL::pos;
+            if (P.obs & (WM_EPOT | WM_ETOT)) act |= 1u << SL::epot;
+            if (P.obs & WM_ACF) act |= 3u << SL::acf;
+            if (P.obs & WM_POP) act |= sm << SL::pop;
+        }
+        if (J.track) act |= (sm << SL::abs) | (sm << SL::absn);
+    }
     double acc[SL::count];
 #pragma unroll
     for (int q = 0; q < SL::count; ++q) acc[q] = 0.0;
@@ -1360,18 +1374,9 @@ __global__ void __launch_bounds__(NDR_THREADS, PHI ? 1 : 2)
     }
     if (tid == 0) bulk_wait_all();
     if (failed) return;
-    if (mode & (RM_OBS | RM_REND | RM_RSTART)) {
-        constexpr uint32_t sm = (1u << S) - 1u;
-        uint32_t act = 1u << SL::norm;
-        if (mode & RM_OBS) {
-            if (P.obs & WM_POS) act |= ((1u << D) - 1u) << SL::pos;
-            if (P.obs & (WM_EPOT | WM_ETOT)) act |= 1u << SL::epot;
-            if (P.obs & WM_ACF) act |= 3u << SL::acf;
-            if (P.obs & WM_POP) act |= sm << SL::pop;
-        }
-        if (J.track) act |= (sm << SL::abs) | (sm << SL::absn);
+    if (sums) {
         block_partials<SL::count>(acc, 0, J.part, J.nparts, part_base + blockIdx.x, act);
-        for (size_t col = blockIdx.x + gridDim.x; col < P.ncols; col += gridDim.x) // columns no CTA owns
+        for (size_t col = blockIdx.x + gridDim.x; col < P.nitems; col += gridDim.x) // columns no CTA owns
             for (int v = tid; v < SL::count; v += blockDim.x) {
                 const size_t o = ((size_t)v * J.nparts + part_base + col) * 2;
                 J.part[o] = 0.0;

@@ -261,6 +261,8 @@ void zqd_server::run_active(std::vector<Req> group, cudaStream_t st) {
     const uint64_t key = group.front()->group_key;
     auto create = [&](const Req& q) -> bool {
         zqd::Opts o = q->o;
+        // several workers' jobs share the device: one resident CTA per SM for the persistent tile pass
+        o.tma_ctas_per_sm = 1;
         const int rc = zqd::job_create_opts(std::move(o), &q->job, st);
         if (rc) {
             finish(q, rc, zqd::last_error(), nullptr);
