@@ -125,6 +125,40 @@ def nd_bytes_per_step(opt, c):
     return b
 
 
+def nd_bytes_moved(opt, c):
+    """Bytes the N-D kernels themselves read and write in one step (each array once per pass):
+    the row pass reads and writes psi and reads the upper triangle of R (16-byte entries in both
+    forms: FP32 keeps an FP64-accurate hi + lo pair), the autocorrelation reference, the CAP weight
+    and the eigenvectors where they are used (imaginary time and stop_norm split it into three
+    launches, and imaginary time renormalises); every tile pass (one in 2-D, three in 3-D) reads
+    and writes psi; a step that records momentum observables also writes phi and runs the momentum
+    tile passes over it."""
+    d = len(opt["grid"]["bounds"])
+    N = opt["grid"]["npoint"] ** d
+    S = len(opt["potential"]["custom"]["matrix"])
+    w = opt.get("write") or {}
+    nsym = S * (S + 1) // 2
+    b = N * (2 * S * c + nsym * 16)
+    if "acf" in w:
+        b += N * S * c
+    if opt.get("absorbing_potential", {}).get("track_population"):
+        b += N * 8
+    if opt.get("adiabatic") and S > 1 and "population" in w:
+        b += N * S * S * 8
+    if any(k in w for k in ("potential_energy", "total_energy")):
+        b += N * S * (S + 1) // 2 * 8
+    if opt.get("imaginary") or opt.get("absorbing_potential", {}).get("stop_norm"):
+        # the row pass runs in three launches (end of step, observables, start of the next step)
+        b += 3 * N * S * c + nsym * 16 * N
+        if opt.get("imaginary"):
+            b += 3 * N * S * c  # renormalisation: the norm's sums, then psi rescaled
+    tile_passes = 1 if d == 2 else 3
+    b += tile_passes * 2 * S * N * c
+    if any(k in w for k in ("kinetic_energy", "momentum", "total_energy")):
+        b += N * S * c + (2 * (d - 2) + 1) * S * N * c  # phi written; momentum tile passes
+    return b
+
+
 def nd_units(opt):
     d = len(opt["grid"]["bounds"])
     return opt["grid"]["npoint"] ** d * len(opt["potential"]["custom"]["matrix"]) * opt["iterations"]
@@ -288,11 +322,17 @@ def nd_legs(qd, torch, flush, reps=2):
             ms = statistics.mean(ts)
             c = 16 if prec == "fp64" else 8
             bstep = nd_bytes_per_step(opt, c)
+            bmoved = nd_bytes_moved(opt, c)
             achieved = bstep * opt["iterations"] / (ms / 1e3) / 1e9
+            moved = bmoved * opt["iterations"] / (ms / 1e3) / 1e9
             leg[prec] = {"value": nd_units(opt) / (ms / 1e3), "unit": UNIT, "ms_per_run": ms,
                          "us_per_step": 1e3 * ms / opt["iterations"],
                          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                      "frac": achieved / peak, "bytes_per_step": bstep, "peak_kind": peak_kind}}
+                                      "frac": achieved / peak, "bytes_per_step": bstep, "peak_kind": peak_kind,
+                                      "moved": {"bytes_per_step": bmoved, "achieved": moved, "frac": moved / peak,
+                                                "note": "the bytes the kernels read and write per step "
+                                                        "(bench.nd_bytes_moved); DRAM traffic is lower where the "
+                                                        "working set stays in the 126 MB L2"}}}
             h = job.result(want_wavefunction=False).observables[0].history
             if "population" in h:
                 pops[prec] = h["population"]

@@ -106,7 +106,9 @@ struct zqd_job {
     // and one tensor map (CUtensorMap, 128 bytes) over psi per strided axis
     bool nd_tma = false;
     int nd_tma_logW = 0, nd_tma_ctas = 0;
+    int nd_tma_ctas_full = 0; // the momentum-sum launches' grid: every resident CTA (never capped)
     alignas(64) unsigned char nd_maps[2][128] = {};
+    alignas(64) unsigned char nd_maps_phi[2][128] = {}; // the same over phi (the momentum passes)
     // the row pass's TMA-staged persistent form: rows per block (log2), CTAs, tensor map over psi
     bool nd_row_tma = false;
     bool nd_row_tma_phi = false; // the momentum-copy launches too (else they take the earlier kernel)

@@ -143,9 +143,12 @@ struct Launch {
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
-    // the TMA-staged persistent form of a psi tile pass (modes TM_FWD, TM_KPHASE, TM_INV)
-    int tile_tma(int axis, uint32_t mode) {
-        const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_maps[axis]);
+    // the TMA-staged persistent form of a tile pass: over psi (modes TM_FWD, TM_KPHASE, TM_INV) or
+    // over phi (TM_FWD, or TM_FWD | TM_KOBS: the momentum sums into region `region`, finalized by f)
+    int tile_tma(int axis, uint32_t mode, bool phi = false, size_t region = 0, bool nostop = false, NdFin f = NdFin{}) {
+        NdJob<T> d = D;
+        if (nostop) d.stopped = J->flags.as<int>() + 1;
+        const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(phi ? J->nd_maps_phi[axis] : J->nd_maps[axis]);
         NdTma P{};
         P.axis = axis;
         P.mode = mode;
@@ -156,10 +159,15 @@ struct Launch {
         P.logtiles = logN - D.logn - P.logW;
         P.logO = logN - D.logn - lstride;
         P.nitems = (unsigned)S << P.logtiles;
+        P.ncols = (unsigned)(S * ntile_blocks); // the momentum region's width
         const size_t smem = ndt_smem_bytes<T>(1 << P.logW, J->n);
         const unsigned threads = (unsigned)((J->n << P.logW) / 8);
-        if (D.d == 2) nd_tile_tma_kernel<T, 2><<<(unsigned)J->nd_tma_ctas, threads, smem, J->stream>>>(D, *map, P);
-        else nd_tile_tma_kernel<T, 3><<<(unsigned)J->nd_tma_ctas, threads, smem, J->stream>>>(D, *map, P);
+        // the momentum sums are grouped per CTA: that launch's grid is the job's own (never the
+        // server's cap) and fits the region
+        const unsigned grid = (mode & TM_KOBS) ? (unsigned)std::min<size_t>((size_t)J->nd_tma_ctas_full, P.ncols)
+                                               : (unsigned)J->nd_tma_ctas;
+        if (D.d == 2) nd_tile_tma_kernel<T, 2><<<grid, threads, smem, J->stream>>>(d, *map, P, region, f);
+        else nd_tile_tma_kernel<T, 3><<<grid, threads, smem, J->stream>>>(d, *map, P, region, f);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -201,6 +209,11 @@ struct Launch {
     // momentum observables of phi (the forward transform along the last axis is already done)
     int kobs(bool nostop, NdFin f) {
         int rc;
+        if (J->nd_tma) {
+            for (int a = D.d - 2; a >= 1; --a)
+                if ((rc = tile_tma(a, TM_FWD, true, 0, nostop))) return rc;
+            return tile_tma(0, TM_FWD | TM_KOBS, true, K, nostop, f);
+        }
         for (int a = D.d - 2; a >= 1; --a)
             if ((rc = tile(a, TM_FWD | TM_PHI, 0, nostop))) return rc;
         return tile(0, TM_FWD | TM_KOBS | TM_PHI, K, nostop, f);
@@ -212,10 +225,10 @@ struct Launch {
 inline int tma_ctas_per_sm_cap(const zqd_job* J) { return J->o.tma_ctas_per_sm > 0 ? J->o.tma_ctas_per_sm : 1 << 20; }
 
 // The TMA-staged tile pass: lines per tile W (a power of two, W <= n) with rows of W c >= 16
-// bytes (an even number of 8-byte words), W n / 8 threads (whole warps, at most 512) and two stages within the
-// shared-memory budget; by default the widest W up to 64-byte rows whose grid still gives every
-// resident CTA two tiles.  w_override (the autotuner's candidate or table entry): 0 keeps the
-// default, -1 keeps the earlier tile kernel, else W.  ZQD_ND_TMA=0 in the environment also keeps it.
+// bytes (an even number of 8-byte words), W n / 8 threads (whole warps, at most 512) and two
+// stages within the shared-memory budget; by default the widest W up to 64-byte rows.  w_override
+// (the autotuner's candidate or table entry): 0 keeps the default, -1 keeps the earlier tile
+// kernel, else W.  ZQD_ND_TMA=0 in the environment also keeps it.
 int setup_tma(zqd_job* J, int w_override) {
     constexpr int c = (int)sizeof(cx<T>), E = c / 8;
     const int n = J->n, d = J->d;
@@ -232,13 +245,15 @@ int setup_tma(zqd_job* J, int w_override) {
         return W >= 1 && W <= n && (E * W) % 2 == 0 && (size_t)W * n / 8 <= 512 && ((size_t)W * n / 8) % 32 == 0 &&
                ndt_smem_bytes<T>(W, n) <= budget;
     };
+    // resident CTAs on the device for a W (the job's own count: the shape, and with it every result,
+    // must not depend on the server's cap, which only trims the grid of the passes that sum nothing)
     auto ctas_for = [&](int W, int& ctas) -> int {
         const int threads = W * n / 8;
         int per_sm = 0;
         ZQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &per_sm, d == 2 ? (const void*)nd_tile_tma_kernel<T, 2> : (const void*)nd_tile_tma_kernel<T, 3>, threads,
             ndt_smem_bytes<T>(W, n)));
-        ctas = std::max(1, std::min(per_sm, tma_ctas_per_sm_cap(J))) * sms;
+        ctas = std::max(1, per_sm) * sms;
         return ZQD_OK;
     };
     const size_t lines = J->N / (size_t)n; // lines of one state along any axis
@@ -249,12 +264,8 @@ int setup_tma(zqd_job* J, int w_override) {
     if (W) {
         if (!fits(W) || lines % (size_t)W) return fail(ZQD_ERR_UNSUPPORTED, "TMA TILE SHAPE OUTSIDE THE KERNEL'S LIMITS");
     } else {
-        for (int w = std::max(1, 64 / c); w >= 1 && !W; w >>= 1) {
-            if (!fits(w) || lines % (size_t)w) continue;
-            int ctas = 0, rc;
-            if ((rc = ctas_for(w, ctas))) return rc;
-            if ((size_t)S * (lines / w) >= 2 * (size_t)ctas || !fits(w / 2)) W = w;
-        }
+        for (int w = std::max(1, 64 / c); w >= 1 && !W; w >>= 1) // measured: 32- to 64-byte rows win
+            if (fits(w) && lines % (size_t)w == 0) W = w;
         if (!W) return ZQD_OK; // no shape fits: the earlier tile kernel runs
     }
     int logW = 0;
@@ -262,7 +273,9 @@ int setup_tma(zqd_job* J, int w_override) {
     int ctas = 0, rc;
     if ((rc = ctas_for(W, ctas))) return rc;
     const size_t items = (size_t)S * (lines / W);
-    J->nd_tma_ctas = (int)std::min<size_t>(items, (size_t)ctas);
+    J->nd_tma_ctas_full = (int)std::min<size_t>(items, (size_t)ctas);
+    const int per_sm = ctas / sms;
+    J->nd_tma_ctas = (int)std::min<size_t>(items, (size_t)std::min(per_sm, tma_ctas_per_sm_cap(J)) * sms);
     J->nd_tma_logW = logW;
     int logn = 0;
     while ((1 << logn) < n) ++logn;
@@ -273,6 +286,8 @@ int setup_tma(zqd_job* J, int w_override) {
         const uint32_t box[3] = {(uint32_t)(E * W), (uint32_t)std::min(n, 256), 1};
         const int l2 = W * c >= 128 ? 128 : 0; // (promotion measured no faster on narrower rows)
         const int e = encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_maps[a]), J->psi_save.p, dims, st * c,
+                                    (uint64_t)n * st * c, box, l2) ||
+                      encode_map_3d(reinterpret_cast<CUtensorMap*>(J->nd_maps_phi[a]), J->phi.p, dims, st * c,
                                     (uint64_t)n * st * c, box, l2);
         if (e) return fail(ZQD_ERR_DEVICE, "cuTensorMapEncodeTiled failed for the tile pass");
     }

@@ -974,16 +974,19 @@ __global__ void __launch_bounds__(512)
 // of tile j + 1 fills the other, and tile j leaves through a TMA store.  The radix passes run in
 // place in the stage buffer (every thread reads its inputs, a barrier, then the writes), so a
 // tile needs no second line buffer; the first and last radix-8 passes stay in registers.
+// TM_KOBS (the momentum observables of phi after its forward transform along axis 0) stores
+// nothing: its sums run over the CTA's tiles and are written once, at column blockIdx.x.
 constexpr int NDT_STAGES = 2;
 constexpr long long NDT_WAIT_CYCLES = 4000000000LL; // ~2 s: a TMA load that has not landed by then has failed
 
 struct NdTma {
     int axis;
-    uint32_t mode;  // TM_FWD, TM_KPHASE, TM_INV
+    uint32_t mode;  // TM_FWD, TM_KPHASE, TM_INV, or TM_FWD | TM_KOBS (momentum sums, no store)
     int logW;       // lines per tile
     int logtiles;   // tiles per state
     int logO;       // outer lines (planes of the tensor map) per state
     unsigned nitems; // tiles of all states
+    unsigned ncols;  // TM_KOBS: columns of the partial-sum region (written whole)
 };
 
 template <typename T> __host__ __device__ inline size_t ndt_stage_bytes(int W, int n) { return (size_t)W * n * sizeof(cx<T>); }
@@ -1094,7 +1097,8 @@ __device__ __forceinline__ void ndt_fft(cx<T> (&v)[8], cx<T>* buf, const IX& ix,
 // lines), [n] rows along the axis, [S * O] planes (outer index and state); box [E W, min(n, 256), 1]
 template <typename T, int D>
 __global__ void __launch_bounds__(512)
-    nd_tile_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map, const NdTma P) {
+    nd_tile_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map, const NdTma P,
+                       size_t part_base, const __grid_constant__ NdFin F) {
     if (*J.stopped) return;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char* base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
@@ -1134,11 +1138,17 @@ __global__ void __launch_bounds__(512)
     for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
     nd_stage_mid_tw<T>(J.tw, twm + n, logn);
     __syncthreads();
+    const bool kobs = P.mode & TM_KOBS;
+    double acc[D + 1]; // TM_KOBS: <k_j> sums and the kinetic energy's, over the CTA's tiles
+#pragma unroll
+    for (int a = 0; a <= D; ++a) acc[a] = 0.0;
     if (tid == 0 && blockIdx.x < P.nitems) issue(blockIdx.x, 0);
+    bool failed = false;
     int j = 0;
     for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
         const int st = j & 1;
         const unsigned kn = k + gridDim.x;
+        if (j > 0 && kobs) __syncthreads(); // every thread is done with tile j - 1's stage (not stored)
         if (tid == 0 && kn < P.nitems) {
             bulk_wait_read_all(); // the store of tile j - 1 has read the other stage
             issue(kn, st ^ 1);
@@ -1149,6 +1159,7 @@ __global__ void __launch_bounds__(512)
                 atomicExch(J.err, 1);
                 if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, NDT_WAIT_CYCLES);
             }
+            failed = true;
             break;
         }
         cx<T>* buf = stage0 + (size_t)st * W * n;
@@ -1180,6 +1191,28 @@ __global__ void __launch_bounds__(512)
                 v[r] = tmul<-1>(v[r], mktab<T>(f.x, f.y));
             }
         }
+        if (kobs) { // Wavefunction.mom / ekin (wavepacket.zig:224-232, 258-268), per-axis tables
+            const size_t gl = gbase + g;
+            double Kl = 0, kl[D];
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                kl[a] = 0;
+                if (a != P.axis) {
+                    const double4 e = J.axis[a * n + axis_index<D>(gl, a, logn)];
+                    Kl += e.z;
+                    kl[a] = e.y;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const double4 a0 = J.axis[P.axis * n + i + (r << logm)];
+                const double w = (double)v[r].x * (double)v[r].x + (double)v[r].y * (double)v[r].y;
+#pragma unroll
+                for (int a = 0; a < D; ++a) acc[a] += w * (a == P.axis ? a0.y : kl[a]);
+                acc[D] += w * (Kl + a0.z);
+            }
+            continue; // no store
+        }
         if (P.mode & TM_INV) ndt_fft<T, 1>(v, buf, ix, logn, twm);
         __syncthreads(); // every thread's last-pass reads are done
 #pragma unroll
@@ -1192,6 +1225,15 @@ __global__ void __launch_bounds__(512)
         }
     }
     if (tid == 0) bulk_wait_all();
+    if (!kobs || failed) return;
+    block_partials<D + 1>(acc, Slots<D, 1>::mom, J.part, J.nparts, part_base + blockIdx.x);
+    for (size_t col = blockIdx.x + gridDim.x; col < P.ncols; col += gridDim.x) // columns no CTA owns
+        for (int a = tid; a <= D; a += blockDim.x) {
+            const size_t o = ((size_t)(Slots<D, 1>::mom + a) * J.nparts + part_base + col) * 2;
+            J.part[o] = 0.0;
+            J.part[o + 1] = 0.0;
+        }
+    if (F.enabled && nd_last_cta(&F.book->counter, gridDim.x)) nd_finalize_cta(J, F);
 }
 
 // ------------------------------------------------------------ row pass, TMA-staged and persistent
