@@ -257,7 +257,8 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.txt")
 
 def read_traffic(kernel, precision):
     """DRAM bytes per launch from profiles/traffic.txt: an ncu capture of the same kernel on the same
-    workload, tabulated by `python bench.py --traffic-table <ncu csv>` (not measured by this run)."""
+    workload, tabulated by `python bench.py --traffic-table <ncu csv> <label>` (the capture's
+    command heads that file; this run does not measure it)."""
     if not os.path.exists(TRAFFIC_FILE):
         return None
     for line in open(TRAFFIC_FILE):
@@ -268,8 +269,10 @@ def read_traffic(kernel, precision):
 
 
 def traffic_table(csv_path, label):
-    """Rows "kernel label bytes_per_launch" from an ncu --csv log with dram__bytes_read.sum and
-    dram__bytes_write.sum: per kernel the mean over its captured launches of read + write bytes."""
+    """Rows "kernel precision[_label] dram_bytes_per_launch" from an ncu --csv capture with
+    gpu__time_duration.sum, dram__bytes_read.sum and dram__bytes_write.sum: per kernel and
+    precision, the mean read + write bytes of the launches of its dominant grid (the grid with the
+    most device time, e.g. the bench's batched launch rather than the autotuner's candidates)."""
     import csv
 
     per = {}
@@ -277,18 +280,30 @@ def traffic_table(csv_path, label):
         lines = [ln for ln in f if ln.startswith('"')]
     for row in csv.DictReader(lines):
         metric = row.get("Metric Name", "")
-        if metric not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
-            continue
-        name = row["Kernel Name"].split("<")[0].split("(")[0].replace("void ", "").replace("zqd::", "").strip()
-        unit = row.get("Metric Unit", "byte").lower()
-        scale = {"byte": 1, "kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9}.get(unit, 1)
-        v = float(row["Metric Value"].replace(",", "")) * scale
-        key = (name, row["ID"])
-        per[key] = per.get(key, 0.0) + v
-    by_kernel = {}
-    for (name, _), v in per.items():
-        by_kernel.setdefault(name, []).append(v)
-    return [f"{k} {label} {statistics.mean(v):.4g}" for k, v in sorted(by_kernel.items())]
+        full = row["Kernel Name"]
+        name = full.split("<")[0].split("(")[0].replace("void ", "").replace("zqd::", "").strip()
+        prec = "fp32" if "<float" in full else "fp64" if "<double" in full else "-"
+        rec = per.setdefault(row["ID"], {"key": (name, prec, row.get("Grid Size", "")), "bytes": 0.0, "ns": 0.0})
+        unit = row.get("Metric Unit", "").lower()
+        v = float(row["Metric Value"].replace(",", ""))
+        if metric in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            rec["bytes"] += v * {"byte": 1, "kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9}.get(unit, 1)
+        elif metric == "gpu__time_duration.sum":
+            rec["ns"] += v * {"ns": 1, "nsecond": 1, "us": 1e3, "usecond": 1e3, "ms": 1e6, "msecond": 1e6}.get(unit, 1)
+    groups = {}
+    for rec in per.values():
+        g = groups.setdefault(rec["key"], {"bytes": [], "ns": 0.0})
+        g["bytes"].append(rec["bytes"])
+        g["ns"] += rec["ns"]
+    best = {}
+    for (name, prec, grid), g in groups.items():
+        if (name, prec) not in best or g["ns"] > best[(name, prec)][1]["ns"]:
+            best[(name, prec)] = (grid, g)
+    out = []
+    for (name, prec), (grid, g) in sorted(best.items()):
+        tag = prec + ("_" + label if label else "")
+        out.append(f"{name} {tag} {statistics.mean(g['bytes']):.4g}  # grid {grid}, {len(g['bytes'])} launches")
+    return out
 
 
 def measured_peak():
