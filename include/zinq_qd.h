@@ -486,6 +486,11 @@ void zqd_testing_fail_device_allocations(uint64_t after, uint64_t count);
    the CTAs that left that way, *wall_ms the host time until the kernel had ended. */
 int zqd_testing_service_idle(zqd_precision precision, uint32_t nstate, uint32_t ctas, double idle_us,
                              uint32_t* idle_exits, double* wall_ms);
+/* The next `launches` launches of the 2-D / 3-D TMA-staged axis passes issue no first tile load in
+   any CTA and bound their mbarrier waits by wait_us: every CTA's first wait runs out, the kernel
+   records it in the job's error word and returns, and the run fails with ZQD_ERR_DEVICE (the
+   context stays usable).  Tests the failure path of the waits without a device fault. */
+int zqd_testing_tma_withhold_load(uint32_t launches, double wait_us);
 
 /* ------------------------------------------------------------------ device */
 int zqd_device_count(void);

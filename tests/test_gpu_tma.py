@@ -94,3 +94,18 @@ def test_tma_runs_are_bitwise_reproducible():
         again = qd.run(opt)
         np.testing.assert_array_equal(first.observables[0].wavefunction, again.observables[0].wavefunction)
         np.testing.assert_array_equal(first.observables[0].history["population"], again.observables[0].history["population"])
+
+
+def test_a_tma_wait_that_runs_out_fails_the_run_and_leaves_the_device_usable():
+    # every CTA of the next TMA-staged launch withholds its first tile load, so its mbarrier wait
+    # runs out of a 100 us budget (nothing completes that phase; no load is left in flight)
+    from zinq_b200 import _abi
+
+    opt = copy.deepcopy(CASES["2d_64sq_3states_pop"])
+    opt["iterations"] = 5
+    _abi.check(_abi.load().zqd_testing_tma_withhold_load(1, 100.0))
+    with pytest.raises(_abi.ZqdError) as err:
+        qd.run(opt)
+    assert err.value.status == -8 and "TMA" in str(err.value)
+    # the armed launch is used up: the next run is whole and matches the oracle
+    compare(CASES["2d_64sq_3states_pop"])

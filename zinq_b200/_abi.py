@@ -179,6 +179,7 @@ SIGNATURES = [
     ("zqd_server_stats_get", C.c_int, [VP, C.POINTER(ZqdServerStats)]),
     ("zqd_server_destroy", None, [VP]),
     ("zqd_testing_fail_device_allocations", None, [C.c_uint64, C.c_uint64]),
+    ("zqd_testing_tma_withhold_load", C.c_int, [C.c_uint32, C.c_double]),
     ("zqd_testing_service_idle", C.c_int, [C.c_int, C.c_uint32, C.c_uint32, C.c_double, C.POINTER(C.c_uint32),
                                            C.POINTER(C.c_double)]),
     ("zqd_autotune", C.c_int, [C.POINTER(ZqdTuneEntry)]),

@@ -28,6 +28,10 @@ const char* last_error();
 // allocate in their own stream.
 cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st = nullptr);
 void dev_free(void* p, cudaStream_t st = nullptr);
+// The mbarrier wait budget (SM cycles) of the next launch of an N-D TMA-staged pass, and whether
+// that launch withholds each CTA's first load (zqd_testing_tma_withhold_load); the default budget
+// and false unless a test armed it.
+long long tma_wait_budget(long long default_cycles, bool* withhold);
 // device memory this process can still allocate: free HBM plus the blocks the pool keeps for reuse
 size_t device_free_bytes();
 

@@ -85,6 +85,14 @@ NdJob<T> describe(zqd_job* J) {
 inline bool row_narrow(unsigned threads) { return S > 1 && threads <= 256; }
 
 using RowTmaKernel = void (*)(NdJob<T>, CUtensorMap, CUtensorMap, NdRowTma, size_t, NdFin);
+// the momentum-copy form of the TMA row kernel (one state: with several it holds too many registers
+// for the per-block kernel's speed, and those launches take that kernel), or null
+inline RowTmaKernel row_tma_phi(int d) {
+    if constexpr (S == 1)
+        return d == 2 ? nd_row_tma_kernel<T, 2, S, true> : nd_row_tma_kernel<T, 3, S, true>;
+    else
+        return nullptr;
+}
 // the 512-thread plain form of the TMA row kernel (one or two states), or null
 inline RowTmaKernel row_tma_wide(int d) {
     if constexpr (S <= 2)
@@ -110,12 +118,15 @@ struct Launch {
             P.obs = obs;
             P.logL = J->nd_row_tma_logL;
             P.nitems = (unsigned)(J->N / J->n >> P.logL);
+            bool withhold = false;
+            P.wait_cycles = tma_wait_budget(NDT_WAIT_CYCLES, &withhold);
+            P.withhold = withhold;
             const size_t smem = ndr_smem_bytes<T>(S, 1 << P.logL, J->n);
             const unsigned nt = (unsigned)((S * J->n << P.logL) / 8), nb = (unsigned)J->nd_row_tma_ctas;
             const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_row_map);
             const CUtensorMap* mphi = reinterpret_cast<const CUtensorMap*>(J->nd_row_map_phi);
-            auto kern = (mode & RM_PHI) ? (D.d == 2 ? nd_row_tma_kernel<T, 2, S, true> : nd_row_tma_kernel<T, 3, S, true>)
-                                        : (D.d == 2 ? nd_row_tma_kernel<T, 2, S, false> : nd_row_tma_kernel<T, 3, S, false>);
+            RowTmaKernel kern = D.d == 2 ? nd_row_tma_kernel<T, 2, S, false> : nd_row_tma_kernel<T, 3, S, false>;
+            if (mode & RM_PHI) kern = row_tma_phi(D.d); // only where nd_row_tma_phi (one state)
             if (nt > (unsigned)NDR_THREADS) kern = row_tma_wide(D.d);
             kern<<<nb, nt, smem, J->stream>>>(d, *map, *mphi, P, region, f);
             ZQD_CUDA(cudaGetLastError());
@@ -166,6 +177,9 @@ struct Launch {
         // server's cap) and fits the region
         const unsigned grid = (mode & TM_KOBS) ? (unsigned)std::min<size_t>((size_t)J->nd_tma_ctas_full, P.ncols)
                                                : (unsigned)J->nd_tma_ctas;
+        bool withhold = false;
+        P.wait_cycles = tma_wait_budget(NDT_WAIT_CYCLES, &withhold);
+        P.withhold = withhold;
         if (D.d == 2) nd_tile_tma_kernel<T, 2><<<grid, threads, smem, J->stream>>>(d, *map, P, region, f);
         else nd_tile_tma_kernel<T, 3><<<grid, threads, smem, J->stream>>>(d, *map, P, region, f);
         ZQD_CUDA(cudaGetLastError());
@@ -314,12 +328,11 @@ int choose_row_tma(zqd_job* J, int l_override) {
     int dev = 0, sms = 148;
     ZQD_CUDA(cudaGetDevice(&dev));
     ZQD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>, nd_row_tma_kernel<T, 2, S, true>,
-                   nd_row_tma_kernel<T, 3, S, true>})
+    for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     for (int dd : {2, 3})
-        if (RowTmaKernel f = row_tma_wide(dd))
-            ZQD_CUDA(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
+        for (RowTmaKernel f : {row_tma_wide(dd), row_tma_phi(dd)})
+            if (f) ZQD_CUDA(cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     auto threads_of = [&](int L) { return (size_t)S * L * n / 8; };
     auto fits = [&](int L) {
         const size_t t = threads_of(L);
@@ -357,7 +370,7 @@ int choose_row_tma(zqd_job* J, int l_override) {
     J->nd_row_tma_logL = logL;
     // the momentum-copy form holds the end-of-step state in registers besides the sweep's: with one
     // state it keeps up with the per-block kernel, with several it does not (one CTA per SM)
-    J->nd_row_tma_phi = S == 1 && threads_of(L) <= (size_t)NDR_THREADS;
+    J->nd_row_tma_phi = row_tma_phi(d) && threads_of(L) <= (size_t)NDR_THREADS;
     J->nd_row_tma = true;
     return ZQD_OK;
 }

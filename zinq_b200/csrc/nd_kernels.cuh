@@ -978,6 +978,7 @@ __global__ void __launch_bounds__(512)
 // nothing: its sums run over the CTA's tiles and are written once, at column blockIdx.x.
 constexpr int NDT_STAGES = 2;
 constexpr long long NDT_WAIT_CYCLES = 4000000000LL; // ~2 s: a TMA load that has not landed by then has failed
+// (the default budget of the waits; a test of the failure path passes a short one)
 
 struct NdTma {
     int axis;
@@ -987,6 +988,8 @@ struct NdTma {
     int logO;       // outer lines (planes of the tensor map) per state
     unsigned nitems; // tiles of all states
     unsigned ncols;  // TM_KOBS: columns of the partial-sum region (written whole)
+    long long wait_cycles; // budget of each mbarrier wait
+    int withhold;    // testing: each CTA's first load is not issued, so its wait runs out
 };
 
 template <typename T> __host__ __device__ inline size_t ndt_stage_bytes(int W, int n) { return (size_t)W * n * sizeof(cx<T>); }
@@ -1142,7 +1145,7 @@ __global__ void __launch_bounds__(512)
     double acc[D + 1]; // TM_KOBS: <k_j> sums and the kinetic energy's, over the CTA's tiles
 #pragma unroll
     for (int a = 0; a <= D; ++a) acc[a] = 0.0;
-    if (tid == 0 && blockIdx.x < P.nitems) issue(blockIdx.x, 0);
+    if (tid == 0 && blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     bool failed = false;
     int j = 0;
     for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
@@ -1153,11 +1156,11 @@ __global__ void __launch_bounds__(512)
             bulk_wait_read_all(); // the store of tile j - 1 has read the other stage
             issue(kn, st ^ 1);
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, NDT_WAIT_CYCLES);
+        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, P.wait_cycles);
         if (!__syncthreads_and(ok)) { // the load never landed: record it, let the prefetch land, stop
             if (tid == 0) {
                 atomicExch(J.err, 1);
-                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, NDT_WAIT_CYCLES);
+                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, P.wait_cycles);
             }
             failed = true;
             break;
@@ -1251,6 +1254,8 @@ struct NdRowTma {
     uint32_t mode, obs;
     int logL;        // rows per block
     unsigned nitems; // blocks, and columns of the partial-sum region
+    long long wait_cycles; // budget of each mbarrier wait
+    int withhold;    // testing: each CTA's first load is not issued, so its wait runs out
 };
 
 template <typename T> __host__ __device__ inline size_t ndr_stage_bytes(int S, int L, int n) {
@@ -1331,7 +1336,7 @@ __global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? 2 : 1)
     const IxRow<T> ix{logn};
     int g, i;
     ix.item(tid, logm, g, i);
-    if (tid == 0 && blockIdx.x < P.nitems) issue(blockIdx.x, 0);
+    if (tid == 0 && blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     bool failed = false;
     int j = 0;
     for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
@@ -1342,11 +1347,11 @@ __global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? 2 : 1)
             bulk_wait_read_all(); // the store of block j - 1 has read the other stage
             issue(kn, st ^ 1);
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, NDT_WAIT_CYCLES);
+        const bool ok = mbar_wait_bounded(&bars[st], (unsigned)(j >> 1) & 1u, P.wait_cycles);
         if (!__syncthreads_and(ok)) {
             if (tid == 0) {
                 atomicExch(J.err, 1);
-                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, NDT_WAIT_CYCLES);
+                if (kn < P.nitems) mbar_wait_bounded(&bars[st ^ 1], (unsigned)((j + 1) >> 1) & 1u, P.wait_cycles);
             }
             failed = true;
             break;

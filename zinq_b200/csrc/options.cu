@@ -438,7 +438,32 @@ extern "C" void zqd_potential_init(zqd_potential* p, zqd_potential_kind kind) {
     }
 }
 
+namespace zqd {
+// Host-side arming of the TMA-wait failure path (zqd_testing_tma_withhold_load): the next
+// g_tma_withhold launches of the N-D TMA-staged passes issue no first load and wait at most
+// g_tma_wait_cycles.
+static std::atomic<long long> g_tma_withhold{0}, g_tma_wait_cycles{0};
+
+long long tma_wait_budget(long long default_cycles, bool* withhold) {
+    *withhold = false;
+    if (g_tma_withhold.load(std::memory_order_relaxed) <= 0) return default_cycles;
+    if (g_tma_withhold.fetch_sub(1) <= 0) return default_cycles;
+    *withhold = true;
+    return g_tma_wait_cycles.load();
+}
+} // namespace zqd
+
 extern "C" void zqd_testing_fail_device_allocations(uint64_t after, uint64_t count) {
     zqd::g_alloc_fail.store((long long)count);
     zqd::g_alloc_skip.store(count ? (long long)after : -1);
+}
+
+extern "C" int zqd_testing_tma_withhold_load(uint32_t launches, double wait_us) {
+    if (!(wait_us > 0)) return zqd::fail(ZQD_ERR_INVALID_INPUT, "WAIT BUDGET MUST BE POSITIVE");
+    int dev = 0, khz = 0;
+    ZQD_CUDA(cudaGetDevice(&dev));
+    ZQD_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+    zqd::g_tma_wait_cycles.store((long long)(wait_us * 1e-3 * (double)khz));
+    zqd::g_tma_withhold.store((long long)launches);
+    return ZQD_OK;
 }
