@@ -659,7 +659,8 @@ def main():
     ap.add_argument("--profile-case", choices=["fp64", "fp32"], default=None,
                     help="run a small case of the bench workload (1 job x 200 steps) twice and exit; for ncu captures")
     ap.add_argument("--nd-case", nargs=3, metavar=("WORKLOAD", "PRECISION", "STEPS"), default=None,
-                    help="run one 2-D/3-D workload (c3 | c3pop | c4 | c4itp | wide) for STEPS steps twice and exit; "
+                    help="run one 2-D/3-D workload (c3 | c3pop | c3pop1 | c3pop2 | c4 | c4itp | wide) for STEPS steps "
+                         "twice and exit; "
                          "for ncu captures")
     ap.add_argument("--table", action="store_true",
                     help="print per-configuration CPU (oracle) and GPU rates as one JSON line and exit")
@@ -684,12 +685,15 @@ def main():
         from zinq_b200 import quantum_dynamics as qd
 
         case, prec, steps = args.nd_case[0], args.nd_case[1], int(args.nd_case[2])
-        def c3pop():  # the 512^2 three-state grid recording populations only (the serving stream's largest jobs)
+        def c3pop(nstate=3):  # the 512^2 grid recording populations only (the serving stream's largest jobs)
             o = coupled_harmonic_2d(iters=steps)
             o["write"] = {"population": "P"}
+            m = o["potential"]["custom"]["matrix"]
+            o["potential"]["custom"]["matrix"] = [row[:nstate] for row in m[:nstate]]
             return o
 
-        opt = {"c3": lambda: coupled_harmonic_2d(iters=steps), "c3pop": c3pop, "c4": lambda: anharmonic_3d(steps, False),
+        opt = {"c3": lambda: coupled_harmonic_2d(iters=steps), "c3pop": c3pop, "c3pop1": lambda: c3pop(1),
+               "c3pop2": lambda: c3pop(2), "c4": lambda: anharmonic_3d(steps, False),
                "c4itp": lambda: anharmonic_3d(steps, True), "wide": lambda: wide_grid_2d(steps)}[case]()
         job = qd.Job(opt, prec)
         for _ in range(2):

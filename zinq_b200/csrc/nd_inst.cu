@@ -126,6 +126,9 @@ struct Launch {
             const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(J->nd_row_map);
             const CUtensorMap* mphi = reinterpret_cast<const CUtensorMap*>(J->nd_row_map_phi);
             RowTmaKernel kern = D.d == 2 ? nd_row_tma_kernel<T, 2, S, false> : nd_row_tma_kernel<T, 3, S, false>;
+            if (!(obs & ~(uint32_t)(WM_POP | WM_NORM)) && nt <= (unsigned)NDR_THREADS) // populations and norm only
+                kern = D.d == 2 ? nd_row_tma_kernel<T, 2, S, false, NDR_THREADS, true>
+                                : nd_row_tma_kernel<T, 3, S, false, NDR_THREADS, true>;
             if (mode & RM_PHI) kern = row_tma_phi(D.d); // only where nd_row_tma_phi (one state)
             if (nt > (unsigned)NDR_THREADS) kern = row_tma_wide(D.d);
             kern<<<nb, nt, smem, J->stream>>>(d, *map, *mphi, P, region, f);
@@ -328,7 +331,8 @@ int choose_row_tma(zqd_job* J, int l_override) {
     int dev = 0, sms = 148;
     ZQD_CUDA(cudaGetDevice(&dev));
     ZQD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>})
+    for (auto f : {nd_row_tma_kernel<T, 2, S, false>, nd_row_tma_kernel<T, 3, S, false>,
+                   nd_row_tma_kernel<T, 2, S, false, NDR_THREADS, true>, nd_row_tma_kernel<T, 3, S, false, NDR_THREADS, true>})
         ZQD_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget));
     for (int dd : {2, 3})
         for (RowTmaKernel f : {row_tma_wide(dd), row_tma_phi(dd)})

@@ -663,11 +663,14 @@ __device__ __forceinline__ void nd_observe(const NdJob<T>& J, const cx<T> (&x)[S
 // points in batches of four and loads the global inputs of the whole batch first (its
 // loads would otherwise wait one after the other); several states keep one point at a
 // time within the registers.  Returns after a barrier.
-// bx(line, x): where point x of line s L + l sits in buf (and phi_src)
-template <typename T, int D, int S, int NV, typename BX>
+// bx(line, x): where point x of line s L + l sits in buf (and phi_src).  OBSMAX: the observables
+// this instantiation can record (a compile-time bound on obs, so that a narrower form keeps fewer
+// accumulators and loads in registers).
+template <typename T, int D, int S, int NV, typename BX, uint32_t OBSMAX = ~0u>
 __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T>* phi_src, const BX& bx, int L, size_t row0,
-                                             uint32_t mode, uint32_t obs, double (&acc)[NV], bool wfn = true) {
+                                             uint32_t mode, uint32_t obs_in, double (&acc)[NV], bool wfn = true) {
     using SL = Slots<D, S>;
+    const uint32_t obs = obs_in & OBSMAX;
     constexpr int SB = S == 1 ? 4 : 1;
     using Aux = NdAux<T, S, (SB > 1)>;
     const int logn = J.logn, pts = L << logn, nt = blockDim.x;
@@ -1280,8 +1283,10 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
 // states on long lines.
 constexpr int NDR_THREADS = 256, NDR_THREADS_WIDE = 512;
 
-template <typename T, int D, int S, bool PHI, int MAXT = NDR_THREADS>
-__global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? 2 : 1)
+// POP: the form for steps that record only the populations and the norm (the other observables'
+// code and accumulators compiled out), three CTAs per SM (80 registers) for one or two states.
+template <typename T, int D, int S, bool PHI, int MAXT = NDR_THREADS, bool POP = false>
+__global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? (POP && S <= 2 ? 3 : 2) : 1)
     nd_row_tma_kernel(const __grid_constant__ NdJob<T> J, const __grid_constant__ CUtensorMap map,
                       const __grid_constant__ CUtensorMap map_phi, const NdRowTma P, size_t part_base,
                       const __grid_constant__ NdFin F) {
@@ -1368,16 +1373,19 @@ __global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? 2 : 1)
 #pragma unroll
             for (int r = 0; r < 8; ++r) buf[ix.at(g, i + (r << logm))] = v[r];
             __syncthreads();
+            constexpr uint32_t OBSMAX = POP ? (uint32_t)(WM_POP | WM_NORM) : ~0u;
             if (PHI) { // end of step i, the copy, then the start of step i+1
-                nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, mode & ~(uint32_t)RM_RSTART, P.obs, acc);
+                nd_row_sweep<T, D, S, SL::count, IxRow<T>, OBSMAX>(J, buf, (cx<T>*)nullptr, ix, L, row0,
+                                                                   mode & ~(uint32_t)RM_RSTART, P.obs, acc);
 #pragma unroll
                 for (int r = 0; r < 8; ++r) w[r] = buf[ix.at(g, i + (r << logm))];
                 if (mode & RM_RSTART) {
                     __syncthreads();
-                    nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, RM_RSTART, 0u, acc, false);
+                    nd_row_sweep<T, D, S, SL::count, IxRow<T>, OBSMAX>(J, buf, (cx<T>*)nullptr, ix, L, row0, RM_RSTART, 0u,
+                                                                       acc, false);
                 }
             } else {
-                nd_row_sweep<T, D, S>(J, buf, (cx<T>*)nullptr, ix, L, row0, mode, P.obs, acc);
+                nd_row_sweep<T, D, S, SL::count, IxRow<T>, OBSMAX>(J, buf, (cx<T>*)nullptr, ix, L, row0, mode, P.obs, acc);
             }
             if (mode & (RM_FWD | RM_STORE))
 #pragma unroll
