@@ -260,6 +260,18 @@ int zqd_job_run(zqd_job* job);                           /* every solve, device-
 int zqd_job_result(zqd_job* job, zqd_result** out);      /* device -> host copy of observables */
 int zqd_job_info(const zqd_job* job, uint32_t* ndim, uint32_t* nstate, uint64_t* npoint_total,
                  uint32_t* cluster_ctas, size_t* device_bytes);
+/* Launch shapes of a 2-D or 3-D job's axis passes (no counterpart in the reference: the reference
+   has no device passes; for tests and tuning).  tma_row_*: the TMA-staged persistent row pass (rows
+   per block, CTAs, threads), all 0 when the per-block kernel takes every row launch; tma_tile_*: the
+   TMA-staged persistent tile pass (lines per tile, CTAs, threads), all 0 when the per-block kernel
+   runs; rows_per_cta, tile_lines: the per-block kernels' shapes (the launches the TMA-staged forms do
+   not take).  ZQD_ERR_UNSUPPORTED for a 1-D job. */
+typedef struct {
+    uint32_t tma_row_block, tma_row_ctas, tma_row_threads;
+    uint32_t tma_tile_lines, tma_tile_ctas, tma_tile_threads;
+    uint32_t rows_per_cta, tile_lines;
+} zqd_nd_shape;
+int zqd_job_nd_shape(const zqd_job* job, zqd_nd_shape* out);
 /* device time (ms, CUDA events on the job's stream) of the last zqd_job_run (or of every
    zqd_job_step call of the current step-wise run) */
 double zqd_job_device_ms(const zqd_job* job);

@@ -109,3 +109,26 @@ def test_a_tma_wait_that_runs_out_fails_the_run_and_leaves_the_device_usable():
     assert err.value.status == -8 and "TMA" in str(err.value)
     # the armed launch is used up: the next run is whole and matches the oracle
     compare(CASES["2d_64sq_3states_pop"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_the_workloads_take_the_tma_staged_passes(precision):
+    # the 2-D 512^2 three-state grid (total energy; populations only), the 3-D 128^3 well and the 2-D
+    # 2048^2 two-state grid: both passes run in their TMA-staged persistent forms, in whole warps
+    pop_only = coupled_harmonic_2d(npoint=512, iters=10)
+    pop_only["write"] = {"population": "P"}
+    wide = {"grid": {"bounds": [[-20, 20], [-20, 20]], "npoint": 2048},
+            "initial_conditions": {"position": [-2, 0], "momentum": [1, 0], "gamma": [1, 1], "state": 0,
+                                   "adiabatic": False},
+            "potential": {"custom": {"ndim": 2, "matrix": [["0.5*(r1^2+r2^2)", "0.01*exp(-r1^2)"],
+                                                           ["0.01*exp(-r1^2)", "0.5*(r1^2+r2^2)+0.1"]]}},
+            "mass": [1, 1], "iterations": 10, "time_step": 0.05, "write": {"population": "P"}}
+    for opt in (coupled_harmonic_2d(npoint=512, iters=10), pop_only, anharmonic_3d(npoint=128, iters=10), wide):
+        job = qd.Job(opt, precision)
+        try:
+            sh = job.nd_shape()
+        finally:
+            job.close()
+        assert sh["tma_row_block"] > 0 and sh["tma_tile_lines"] > 0, sh
+        assert sh["tma_row_threads"] % 32 == 0 and sh["tma_tile_threads"] % 32 == 0, sh
+        assert sh["tma_row_ctas"] > 0 and sh["tma_tile_ctas"] > 0, sh

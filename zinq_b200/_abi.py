@@ -115,6 +115,12 @@ class ZqdTuneEntry(C.Structure):
                 ("candidates", C.c_uint32), ("tma_row_block", C.c_int32), ("tma_tile_lines", C.c_int32)]
 
 
+class ZqdNdShape(C.Structure):
+    _fields_ = [("tma_row_block", C.c_uint32), ("tma_row_ctas", C.c_uint32), ("tma_row_threads", C.c_uint32),
+                ("tma_tile_lines", C.c_uint32), ("tma_tile_ctas", C.c_uint32), ("tma_tile_threads", C.c_uint32),
+                ("rows_per_cta", C.c_uint32), ("tile_lines", C.c_uint32)]
+
+
 class ZqdEvent(C.Structure):
     _fields_ = [("ticket", C.c_uint64), ("kind", C.c_int), ("status", C.c_int), ("solve", C.c_uint32),
                 ("first_row", C.c_uint32), ("nrows", C.c_uint32), ("width", C.c_uint32), ("solve_finished", C.c_int),
@@ -147,6 +153,7 @@ SIGNATURES = [
     ("zqd_job_result", C.c_int, [VP, C.POINTER(VP)]),
     ("zqd_job_info", C.c_int, [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                C.POINTER(C.c_uint32), C.POINTER(C.c_size_t)]),
+    ("zqd_job_nd_shape", C.c_int, [VP, C.POINTER(ZqdNdShape)]),
     ("zqd_job_device_ms", C.c_double, [VP]),
     ("zqd_job_destroy", None, [VP]),
     ("zqd_job_step", C.c_int, [VP, C.c_uint32]),

@@ -859,6 +859,25 @@ extern "C" int zqd_job_info(const zqd_job* J, uint32_t* ndim, uint32_t* nstate, 
     return ZQD_OK;
 }
 
+extern "C" int zqd_job_nd_shape(const zqd_job* J, zqd_nd_shape* out) {
+    if (!J || !out) return fail(ZQD_ERR_INVALID_INPUT, "NULL ARGUMENT");
+    if (J->d < 2) return fail(ZQD_ERR_UNSUPPORTED, "NOT A 2-D OR 3-D JOB");
+    *out = zqd_nd_shape{};
+    if (J->nd_row_tma) {
+        out->tma_row_block = 1u << J->nd_row_tma_logL;
+        out->tma_row_ctas = (uint32_t)J->nd_row_tma_ctas;
+        out->tma_row_threads = (uint32_t)((size_t)J->S * J->n * out->tma_row_block / 8);
+    }
+    if (J->nd_tma) {
+        out->tma_tile_lines = 1u << J->nd_tma_logW;
+        out->tma_tile_ctas = (uint32_t)J->nd_tma_ctas;
+        out->tma_tile_threads = (uint32_t)((size_t)J->n * out->tma_tile_lines / 8);
+    }
+    out->rows_per_cta = (uint32_t)J->nd_rows;
+    out->tile_lines = (uint32_t)J->nd_tile;
+    return ZQD_OK;
+}
+
 extern "C" double zqd_job_device_ms(const zqd_job* J) { return J ? (double)J->last_ms : 0.0; }
 
 extern "C" void zqd_job_destroy(zqd_job* J) { delete J; }

@@ -309,6 +309,13 @@ class Job:
         return {"ndim": d.value, "nstate": s.value, "npoint_total": n.value, "cluster_ctas": c.value,
                 "device_bytes": b.value}
 
+    def nd_shape(self):
+        """zqd_job_nd_shape: the 2-D / 3-D axis passes' launch shapes (TMA-staged forms, 0 where the
+        per-block kernels run, and the per-block shapes)."""
+        sh = _abi.ZqdNdShape()
+        check(self._L.zqd_job_nd_shape(self._h, C.byref(sh)))
+        return {name: getattr(sh, name) for name, _ in sh._fields_}
+
     def run(self) -> float:
         check(self._L.zqd_job_run(self._h))
         return self._L.zqd_job_device_ms(self._h)
