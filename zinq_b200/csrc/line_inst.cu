@@ -13,8 +13,9 @@
 
 namespace zqd {
 
-template <int C, int LRM> static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
-    auto kern = line_solve_kernel<ZQD_T, ZQD_S, C, LRM>;
+template <int C, int LRM, int MAXT = LineMaxThreads<ZQD_T>::value>
+static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
+    auto kern = line_solve_kernel<ZQD_T, ZQD_S, C, LRM, MAXT>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(once, [&] {
@@ -51,7 +52,9 @@ int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
     case 2: return launch_one<2, 2>(J, dj, nj);
     case 4: return launch_one<4, 2>(J, dj, nj);
     case 8: return launch_one<8, 2>(J, dj, nj);
-    case 16: return launch_one<16, 2>(J, dj, nj);
+    case 16: // FP32 CTAs of at most 256 threads: the form compiled for 256 (no register spills)
+        if (LineMaxThreads<ZQD_T>::value > 256 && J->threads <= 256) return launch_one<16, 2, 256>(J, dj, nj);
+        return launch_one<16, 2>(J, dj, nj);
     default: return fail(ZQD_ERR_UNSUPPORTED, "CLUSTER SIZE MUST BE 1, 2, 4, 8 OR 16");
     }
 }
