@@ -40,6 +40,14 @@ static int launch_one(const LaunchShape* J, const void* d_jobs, int njobs) {
     return ZQD_OK;
 }
 
+// A radix-4 launch of C-CTA clusters: FP32 CTAs of at most 256 threads take the form compiled for
+// 256 threads (up to 255 registers, no spills; the FP32 kernel is otherwise compiled for 512-thread
+// CTAs and 128 registers)
+template <int C> static int launch_r4(const LaunchShape* J, const void* dj, int nj) {
+    if (LineMaxThreads<ZQD_T>::value > 256 && J->threads <= 256) return launch_one<C, 2, 256>(J, dj, nj);
+    return launch_one<C, 2>(J, dj, nj);
+}
+
 // Radix-4 kernels for every cluster size; radix 8 only with 16 CTAs, the one shape whose CTAs can
 // hold more points than radix-4 threads allow (the longest lines)
 int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
@@ -48,19 +56,19 @@ int ZQD_LAUNCH(const LaunchShape* J, const void* dj, int nj) {
         return fail(ZQD_ERR_UNSUPPORTED, "RADIX-8 LINE PASSES ARE BUILT FOR CLUSTERS OF 16 ONLY");
     }
     switch (J->C) {
-    case 1: return launch_one<1, 2>(J, dj, nj);
-    case 2: return launch_one<2, 2>(J, dj, nj);
-    case 4: return launch_one<4, 2>(J, dj, nj);
-    case 8: return launch_one<8, 2>(J, dj, nj);
-    case 16: // FP32 CTAs of at most 256 threads: the form compiled for 256 (no register spills)
-        if (LineMaxThreads<ZQD_T>::value > 256 && J->threads <= 256) return launch_one<16, 2, 256>(J, dj, nj);
-        return launch_one<16, 2>(J, dj, nj);
+    case 1: return launch_r4<1>(J, dj, nj);
+    case 2: return launch_r4<2>(J, dj, nj);
+    case 4: return launch_r4<4>(J, dj, nj);
+    case 8: return launch_r4<8>(J, dj, nj);
+    case 16: return launch_r4<16>(J, dj, nj);
     default: return fail(ZQD_ERR_UNSUPPORTED, "CLUSTER SIZE MUST BE 1, 2, 4, 8 OR 16");
     }
 }
 
 // The persistent service kernel (single-CTA jobs, radix-4 local passes): grid CTAs of `threads`
 // threads with `smem` bytes of dynamic shared memory each, on stream st.
+// (always the form compiled for LineMaxThreads: its many small CTAs share SMs, which fewer
+// registers per thread allow)
 int ZQD_SERVICE(const void* svc, unsigned grid, int threads, size_t smem, cudaStream_t st) {
     auto kern = line_service_kernel<ZQD_T, ZQD_S, 2>;
     static std::once_flag once;

@@ -937,8 +937,8 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
 }
 
 // One cluster of C CTAs per job of the array: a group of jobs in one launch.
-// MAXT: the CTA size the kernel is compiled for (LineMaxThreads by default; FP32 CTAs of at most 256
-// threads also have a 256-thread form, which leaves a thread 255 registers instead of 128)
+// MAXT: the CTA size the kernel is compiled for (LineMaxThreads by default; FP32 launches of at
+// most 256 threads per CTA take a 256-thread form, which leaves a thread 255 registers instead of 128)
 template <typename T, int S, int C, int LRM, int MAXT = LineMaxThreads<T>::value>
 __global__ void __launch_bounds__(MAXT, 1) line_solve_kernel(const LineJob<T>* __restrict__ jobs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
