@@ -275,9 +275,7 @@ int setup_tma(zqd_job* J, int w_override) {
     };
     const size_t lines = J->N / (size_t)n; // lines of one state along any axis
     int W = 0;
-    const char* ew = getenv("ZQD_TMA_W");
     if (w_override > 0) W = w_override;
-    else if (ew && atoi(ew) > 0) W = atoi(ew);
     if (W) {
         if (!fits(W) || lines % (size_t)W) return fail(ZQD_ERR_UNSUPPORTED, "TMA TILE SHAPE OUTSIDE THE KERNEL'S LIMITS");
     } else {
@@ -356,9 +354,7 @@ int choose_row_tma(zqd_job* J, int l_override) {
         return ZQD_OK;
     };
     int L = 0;
-    const char* el = getenv("ZQD_TMA_ROWS");
     if (l_override > 0) L = l_override;
-    else if (el && atoi(el) > 0) L = atoi(el);
     if (L) {
         if (!fits(L)) return fail(ZQD_ERR_UNSUPPORTED, "TMA ROW-BLOCK SHAPE OUTSIDE THE KERNEL'S LIMITS");
     } else { // the largest block of at most 256 threads (measured: fewer, larger CTAs win), else the wide form
