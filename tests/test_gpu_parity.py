@@ -101,6 +101,15 @@ def test_cluster_sizes_agree_with_oracle(cluster, monkeypatch):
     compare(opt)
 
 
+@pytest.mark.parametrize("cluster", ["1", "2", "4", "8", "16"])
+def test_cluster_sizes_agree_with_oracle_fp32(cluster, monkeypatch):
+    # FP32 CTAs of at most 256 threads run the kernel form compiled for 256 threads (clusters of 2 to
+    # 16 here); one-CTA lines of 1024 points keep the 512-thread form
+    monkeypatch.setenv("ZQD_LINE_CLUSTER", cluster)
+    opt = tully("tully_1", True, npoint=1024, iters=400)
+    compare(opt, precision="fp32", pop_tol=FP32_POP_TOL, obs_tol=1e-4)
+
+
 def test_custom_expression_potential_matches_builtin():
     # example/input/quantum_dynamics_custom_real.json writes Tully 1 as expressions
     expr = {"custom": {"ndim": 1, "matrix": [
