@@ -75,6 +75,7 @@ NdJob<T> describe(zqd_job* J) {
     while ((1 << D.logtile) < J->nd_tile) ++D.logtile;
     D.stopped = J->flags.as<int>();
     D.err = J->flags.as<int>() + 2;
+    D.nsum = J->book.as<NdBook>()->scal; // where nd_reduce_kernel leaves the norm's sum (device address)
     D.pot = J->pot.dev;
     return D;
 }
@@ -218,8 +219,8 @@ struct Launch {
         return ZQD_OK;
     }
     // scalar sums of slots [0, nv) over partial blocks [b0, b1) into scal()
-    int reduce(size_t b0, size_t b1, int nv) {
-        nd_reduce_kernel<<<1, 32 * nv, 0, J->stream>>>(D.part, D.nparts, b0, b1, nv, D.stopped, scal());
+    int reduce(size_t b0, size_t b1, int nv, bool clear = false) {
+        nd_reduce_kernel<<<1, 32 * nv, 0, J->stream>>>(D.part, D.nparts, b0, b1, nv, D.stopped, scal(), clear ? 1 : 0);
         ZQD_CUDA(cudaGetLastError());
         return ZQD_OK;
     }
@@ -612,12 +613,29 @@ struct Seq {
             if (needk && (rc = Lc.kobs(false, f))) return rc;
             return ZQD_OK;
         }
-        if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE, 0, Lc.R0))) return rc;
-        if (o.imag_nstate && (rc = itp_ops(s))) return rc; // every i, the initial state included
+        // Imaginary time, first state (nothing to orthogonalise against), no absorbing potential, after
+        // step 0: the pass that closes step i also sums |psi|^2, and the next pass divides by the norm
+        // as it loads psi, in place of the norm and normalisation kernels (quantum_dynamics.zig:898-906
+        // with no earlier states); without a time-dependent potential that pass also records the
+        // step's observables and opens step i+1.
+        const bool fuse = o.imag_nstate && s == 0 && i > 0 && !o.has_cap;
+        if (i > 0 && (rc = Lc.row(RM_INV | RM_REND | RM_STORE | (fuse ? (uint32_t)RM_NORM : 0u), 0, Lc.R0))) return rc;
+        if (fuse) { // the norm's sum into scal[0], taken out of R0 (the observables row sums R0 too)
+            if ((rc = Lc.reduce(Lc.R0, Lc.R0 + Lc.nrow_blocks, 1, true))) return rc;
+        } else if (o.imag_nstate && (rc = itp_ops(s))) {
+            return rc; // every i, the initial state included
+        }
         if (o.pot_td && (rc = Lc.table((double)i * o.time_step, 0))) return rc;
         // R0 holds the end-of-step sums of the row pass that closed step i (none at i = 0)
         const NdFin f = fin(s, 0, i > 0 ? Lc.R0 : Lc.R1, Lc.R1 + Lc.nrow_blocks, needk, mask, row, i);
-        if ((rc = Lc.row(RM_OBS | (needk ? RM_PHI : 0u), obs, Lc.R1, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
+        if (fuse && !o.pot_td && i < iters) { // normalise, observe, and open step i+1 in one pass
+            const uint32_t mode = RM_SCALE | RM_OBS | RM_RSTART | RM_FWD | RM_STORE | (needk ? (uint32_t)RM_PHI : 0u);
+            if ((rc = Lc.row(mode, obs, Lc.R1, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
+            if (needk && (rc = Lc.kobs(false, f))) return rc;
+            return ZQD_OK;
+        }
+        const uint32_t omode = RM_OBS | (needk ? (uint32_t)RM_PHI : 0u) | (fuse ? (uint32_t)(RM_SCALE | RM_STORE) : 0u);
+        if ((rc = Lc.row(omode, obs, Lc.R1, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
         if (needk && (rc = Lc.kobs(false, f))) return rc;
         if (i < iters) {
             if (o.pot_td && (rc = Lc.table(((double)i + 0.5) * o.time_step, 1))) return rc;

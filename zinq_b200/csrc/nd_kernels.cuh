@@ -64,6 +64,7 @@ template <typename T> struct NdJob {
     const double2* kphase; // [D][n] exp(Complex(0, -k^2 / (2 m_j)) * dt) of axis j
     const double4* axis;   // [D][n] per-axis grid values: coordinate r, wavenumber k, 0.5 k^2 / m_j
     double* part;     // per-CTA partial sums, slot-major: [NDV][nparts][2]
+    const double* nsum; // RM_SCALE: the reduced sum of |psi|^2 the load divides by (sqrt of dr times it)
     size_t nparts;
     int rows_per_cta; // row pass: rows of the last axis per CTA
     int tile, logtile; // tile pass: lines per CTA (a power of two) and its log2
@@ -81,6 +82,8 @@ enum : uint32_t {
     RM_RSTART = 1u << 4, // accumAbsorbed (if tracking) then R: start of the next step
     RM_FWD = 1u << 5,    // forward FFT along the last axis
     RM_STORE = 1u << 6,  // write psi back
+    RM_NORM = 1u << 7,   // after RM_REND: sum |psi|^2 into the norm slot (imaginary time: the renormalisation's norm)
+    RM_SCALE = 1u << 8,  // on load: psi /= sqrt(dr * *nsum), as the normalisation kernel does (imaginary time)
 };
 // tile-pass modes
 enum : uint32_t {
@@ -266,13 +269,22 @@ __device__ __forceinline__ double warp_sum_partials(const double* __restrict__ p
 }
 
 // scalars for the imaginary-time kernels: out[v] = sum of slot v over [b0, b1), v < nv (one warp per slot)
-static __global__ void nd_reduce_kernel(const double* __restrict__ part, size_t P, size_t b0, size_t b1, int nv,
-                                        const int* stopped, double* __restrict__ out) {
+// clear: the summed columns are zeroed afterwards (a sum taken out of a region the step's
+// observables row also sums)
+static __global__ void nd_reduce_kernel(double* __restrict__ part, size_t P, size_t b0, size_t b1, int nv,
+                                        const int* stopped, double* __restrict__ out, int clear) {
     if (*stopped) return;
     const int w = threadIdx.x >> 5;
     if (w >= nv) return;
     const double v = warp_sum_partials(part, P, b0, b1, w);
     if ((threadIdx.x & 31) == 0) out[w] = v;
+    if (clear) {
+        __syncwarp();
+        for (size_t b = b0 + (threadIdx.x & 31); b < b1; b += 32) {
+            part[((size_t)w * P + b) * 2] = 0.0;
+            part[((size_t)w * P + b) * 2 + 1] = 0.0;
+        }
+    }
 }
 
 // Per-solve bookkeeping on the device.
@@ -675,6 +687,8 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
     using Aux = NdAux<T, S, (SB > 1)>;
     const int logn = J.logn, pts = L << logn, nt = blockDim.x;
     const T inv_n = (T)(1.0 / (double)J.N);
+    // RM_SCALE: the normalisation kernel's factors sqrt(dr * sum) and its square
+    const double nsq = (mode & RM_SCALE) ? sqrt(*J.nsum * J.dr) : 1.0, nden = nsq * nsq;
     const bool obsv = mode & RM_OBS, adia = J.adiabatic && S > 1;
     NdNeed nd;
     nd.R = mode & (RM_REND | RM_RSTART);
@@ -700,9 +714,17 @@ __device__ __forceinline__ void nd_row_sweep(const NdJob<T>& J, cx<T>* buf, cx<T
             if (mode & RM_INV)
 #pragma unroll
                 for (int s = 0; s < S; ++s) v[s] = scale<T>(v[s], inv_n);
+            if (mode & RM_SCALE) // normalize (wavepacket.zig:282-284) with the norm of the previous pass
+#pragma unroll
+                for (int s = 0; s < S; ++s)
+                    v[s] = mk<T>((T)((double)v[s].x * nsq / nden), (T)((double)v[s].y * nsq / nden));
             if (mode & RM_REND) {
                 if (J.track) nd_absorbed<T, S, SL::abs>(J, v, g, a[b], acc);
                 a[b].R.apply(v);
+                if (mode & RM_NORM)
+#pragma unroll
+                    for (int s = 0; s < S; ++s)
+                        acc[SL::norm] += (double)v[s].x * (double)v[s].x + (double)v[s].y * (double)v[s].y;
             }
             if (obsv) nd_observe<T, D, S>(J, v, g, obs, a[b], acc);
             if (wout) { // History.append of the wavefunction (quantum_dynamics.zig:176-180), toAdia first (:919-927)
