@@ -129,8 +129,10 @@ def nd_bytes_moved(opt, c):
     """Bytes the N-D kernels themselves read and write in one step (each array once per pass):
     the row pass reads and writes psi and reads the upper triangle of R (16-byte entries in both
     forms: FP32 keeps an FP64-accurate hi + lo pair), the autocorrelation reference, the CAP weight
-    and the eigenvectors where they are used (imaginary time and stop_norm split it into two or
-    three launches, and imaginary time renormalises); every tile pass (one in 2-D, three in 3-D) reads
+    and the eigenvectors where they are used (stop_norm, a time-dependent potential and imaginary
+    time with earlier states split it into three launches, and imaginary time renormalises; one
+    relaxed state defers its renormalisation into the next step's passes and moves what real time
+    moves); every tile pass (one in 2-D, three in 3-D) reads
     and writes psi; a step that records momentum observables also writes phi and runs the momentum
     tile passes over it."""
     d = len(opt["grid"]["bounds"])
@@ -149,9 +151,7 @@ def nd_bytes_moved(opt, c):
         b += N * S * (S + 1) // 2 * 8
     cap = bool(opt.get("absorbing_potential"))
     if opt.get("imaginary") and (opt["imaginary"].get("nstate", 1) == 1) and not cap:
-        # one relaxed state: the step closes in one row pass (summing the norm) and the next pass
-        # renormalises on load, records the observables and opens the next step
-        b += 2 * N * S * c + nsym * 16 * N
+        pass  # the renormalisation rides on the step's own passes
     elif opt.get("imaginary") or opt.get("absorbing_potential", {}).get("stop_norm"):
         # the row pass runs in three launches (end of step, observables, start of the next step)
         b += 3 * N * S * c + nsym * 16 * N

@@ -90,8 +90,17 @@ def stepped(opt, chunk, precision="fp64"):
     return res, rows
 
 
+def itp_2d():
+    # the first solve defers each step's renormalisation into the next step's passes; the second
+    # (orthogonalised against the first) renormalises in the step
+    opt = coupled_2d(60)
+    opt["imaginary"] = {"nstate": 2}
+    opt["write"] = {"population": "P", "total_energy": "E", "acf": "A", "norm": "N"}
+    return opt
+
+
 CASES = {"tully_cap_stop": tully_cap, "itp_three_solves": harmonic_itp, "time_dependent": td_1d,
-         "2d_acf": coupled_2d, "2d_cap_stop": cap_2d}
+         "2d_acf": coupled_2d, "2d_cap_stop": cap_2d, "2d_itp_two_solves": itp_2d}
 
 
 @pytest.mark.parametrize("case", sorted(CASES))

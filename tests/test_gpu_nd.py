@@ -103,6 +103,47 @@ def test_2d_long_lines_one_row_per_block():
     compare(opt)
 
 
+ALL_OBS = {"population": "P", "position": "X", "momentum": "K", "potential_energy": "V", "kinetic_energy": "T",
+           "total_energy": "E", "norm": "N", "acf": "A"}
+
+
+def itp_2d(write, nstate=1, npoint=64, iters=80, adiabatic=False):
+    opt = coupled_harmonic_2d(npoint=npoint, iters=iters)
+    opt["imaginary"] = {"nstate": nstate}
+    opt["write"] = write
+    opt["adiabatic"] = adiabatic
+    return opt
+
+
+@pytest.mark.parametrize("what", ["every_observable", "populations", "nothing", "adiabatic_populations"])
+def test_2d_imaginary_time_deferred_renormalisation(what):
+    # one relaxed state: the step's renormalisation is deferred into the next step's first pass and
+    # the observables row is scaled by its factor (squared for the quadratic sums); every recorded
+    # series and the final state against the oracle, which normalises before it observes
+    write = {"every_observable": ALL_OBS, "populations": {"population": "P"}, "nothing": {},
+             "adiabatic_populations": {"population": "P", "norm": "N"}}[what]
+    compare(itp_2d(write, adiabatic=what == "adiabatic_populations"))
+
+
+def test_2d_imaginary_time_deferred_renormalisation_fp32():
+    opt = itp_2d({"population": "P", "total_energy": "E", "norm": "N"})
+    gpu = qd.run(opt, precision="fp32").observables[0]
+    ref = qd_ref.run(opt)[0]
+    assert float(np.max(np.abs(gpu.history["population"] - ref.history["pop"]))) <= FP32_POP_TOL
+    assert float(np.max(np.abs(gpu.history["norm"] - ref.history["norm"]))) <= 1e-6
+
+
+def test_2d_imaginary_time_with_wavefunction_history(tmp_path):
+    # a recorded wavefunction history keeps the renormalisation in the step (the history holds
+    # normalised states): the other fused form of the step
+    opt = itp_2d({"wavefunction": str(tmp_path / "w.mat"), "population": "P", "norm": "N"}, npoint=32, iters=40)
+    gpu, ref, _ = compare(opt)
+    w = gpu.observables[0].history["wavefunction"]
+    r = ref[0].history["wfn"]
+    assert w.shape[0] == 41
+    assert float(np.max(np.abs(w.reshape(r.shape) - r))) <= 1e-10
+
+
 def test_3d_imaginary_time_two_states():
     compare(anharmonic_3d(npoint=16, iters=150, write={"total_energy": "E", "norm": "N"}, imaginary=2))
 

@@ -190,12 +190,13 @@ struct Launch {
         return ZQD_OK;
     }
     int ptile(int axis, uint32_t mode) { return J->nd_tma ? tile_tma(axis, mode) : tile(axis, mode, 0); }
-    // forward along axes d-2..1, forward + kinetic phase + inverse along axis 0, inverse along 1..d-2
-    int step_tiles() {
+    // forward along axes d-2..1, forward + kinetic phase + inverse along axis 0, inverse along 1..d-2;
+    // `first`: mode bits of the first of these launches only (TM_SCALE)
+    int step_tiles(uint32_t first = 0) {
         int rc;
-        for (int a = D.d - 2; a >= 1; --a)
-            if ((rc = ptile(a, TM_FWD))) return rc;
-        if ((rc = ptile(0, TM_FWD | TM_KPHASE | TM_INV))) return rc;
+        for (int a = D.d - 2; a >= 1; --a, first = 0)
+            if ((rc = ptile(a, TM_FWD | first))) return rc;
+        if ((rc = ptile(0, TM_FWD | TM_KPHASE | TM_INV | first))) return rc;
         for (int a = 1; a <= D.d - 2; ++a)
             if ((rc = ptile(a, TM_INV))) return rc;
         return ZQD_OK;
@@ -543,6 +544,18 @@ struct Seq {
     }
     double* hist(int s) const { return J->hist.as<double>() + (size_t)s * (iters + 1) * HC; }
     int* rows_out(int s) const { return J->rows.as<int>() + s; }
+    // Imaginary time, first state, no absorbing potential, no time-dependent potential and no
+    // wavefunction history: the renormalisation of step i (quantum_dynamics.zig:898-906 with no
+    // earlier states) is deferred.  Propagation is linear, the norm, populations, energies and
+    // positions are quadratic in psi and the autocorrelation is linear, so the step closes and the
+    // next one opens in a single row pass over the unnormalised psi, as in real time; its finalize
+    // scales the observables row by the renormalisation factor (squared) and keeps the sum of
+    // |psi|^2, and the first tile pass of step i+1 (or the final observables' pass) multiplies psi
+    // by that factor as it loads it.
+    bool deferred(int s) const {
+        const Opts& o = J->o;
+        return o.imag_nstate && s == 0 && !o.has_cap && !o.pot_td && !J->wfn_hist.p;
+    }
     // this solve's wavefunction history entry of step i (write.wavefunction), or null
     cx<T>* whist(int s, int i) const {
         return J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + ((size_t)s * (iters + 1) + i) * S * J->N : nullptr;
@@ -603,13 +616,16 @@ struct Seq {
         const bool needk = mask & (WM_MOM | WM_EKIN | WM_ETOT);
         const uint32_t obs = mask | ((o.has_cap && o.cap_has_stop) ? (uint32_t)WM_NORM : 0u);
         double* row = hist(s) + (size_t)i * HC;
-        if (i > 0 && (rc = Lc.step_tiles())) return rc;
-        if (!split) {
+        const bool defer = deferred(s);
+        if (i > 0 && (rc = Lc.step_tiles(defer ? (uint32_t)TM_SCALE : 0u))) return rc;
+        if (!split || defer) {
             uint32_t mode = RM_OBS | RM_STORE | (needk ? RM_PHI : 0u);
             if (i > 0) mode |= RM_INV | RM_REND;
             if (i < iters) mode |= RM_RSTART | RM_FWD;
-            const NdFin f = fin(s, 0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, row, i);
-            if ((rc = Lc.row(mode, obs, Lc.R0, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
+            NdFin f = fin(s, 0, Lc.R0, Lc.R0 + Lc.nrow_blocks, needk, mask, row, i);
+            if (defer) f.nsum_out = Lc.scal();
+            const uint32_t o2 = obs | (defer ? (uint32_t)WM_NORM : 0u);
+            if ((rc = Lc.row(mode, o2, Lc.R0, false, needk ? NdFin{} : f, whist(s, i)))) return rc;
             if (needk && (rc = Lc.kobs(false, f))) return rc;
             return ZQD_OK;
         }
@@ -649,7 +665,9 @@ struct Seq {
         int rc;
         // final Observables.init(..., log = true) (quantum_dynamics.zig:949)
         const uint32_t all = WM_ALL_OBS | (acf ? (uint32_t)WM_ACF : 0u);
-        if ((rc = Lc.row(RM_OBS | RM_PHI, all, Lc.R1, true))) return rc;
+        // a deferred renormalisation (the last step's) is applied here, and psi stored normalised
+        const uint32_t scale = deferred(s) ? (uint32_t)(RM_SCALE | RM_STORE) : 0u;
+        if ((rc = Lc.row(RM_OBS | RM_PHI | scale, all, Lc.R1, true))) return rc;
         if ((rc = Lc.kobs(true, fin(s, 1, Lc.R1, Lc.R1 + Lc.nrow_blocks, true, all, J->fin.as<double>() + (size_t)s * HC, 0))))
             return rc;
         if (s + 1 < J->nsolve) // orthw.append (quantum_dynamics.zig:586-591)

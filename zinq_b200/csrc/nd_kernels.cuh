@@ -92,7 +92,19 @@ enum : uint32_t {
     TM_INV = 1u << 2,
     TM_KOBS = 1u << 3,   // after the forward FFT along axis 0: momentum observables, no store
     TM_PHI = 1u << 4,    // operate on phi instead of psi
+    TM_SCALE = 1u << 5,  // on load: psi *= nd_norm_factor(*nsum, dr) (imaginary time, renormalisation deferred)
 };
+
+// The renormalisation factor of psi whose sum of |psi|^2 is `sum`: 1 / sqrt(dr * sum), formed as
+// Wavefunction.normalize's division by the real sqrt(norm) is (wavepacket.zig:282-284): sq / sq^2.
+__host__ __device__ inline double nd_norm_factor(double sum, double dr) {
+    const double sq = sqrt(sum * dr);
+    return sq / (sq * sq);
+}
+// psi times an FP64 factor, rounded once to the state's precision
+template <typename T> __device__ __forceinline__ cx<T> nd_scaled(cx<T> v, double f) {
+    return mk<T>((T)((double)v.x * f), (T)((double)v.y * f));
+}
 
 template <typename T> __host__ __device__ inline int tile_ldp(int n) { return padded_len<T>(n) | 1; }
 // dynamic shared memory: nbuf line buffers of `lines` lines, then the twiddle table on a 16-byte boundary
@@ -304,6 +316,11 @@ struct NdFin {
     double* row;
     int* rows_out;
     NdBook* book;
+    // kind 0, renormalisation deferred (imaginary time): the launch summed the unnormalised psi.
+    // The row is scaled as if psi had been normalised first (every sum by the factor squared, the
+    // autocorrelation by the factor), and the raw sum of |psi|^2 goes to *nsum_out, where the next
+    // step's first pass (TM_SCALE) or the final observables' pass (RM_SCALE) takes it from.
+    double* nsum_out;
     size_t x0, x1, k0, k1;
     double stop_norm;
     uint32_t mask;
@@ -339,6 +356,12 @@ template <typename T> __device__ void nd_finalize_cta(const NdJob<T>& J, const N
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
+    if (F.nsum_out) {
+        const double f = nd_norm_factor(out[sl.norm()], J.dr);
+        *F.nsum_out = out[sl.norm()];
+        for (int v = 0; v < sl.count(); ++v)
+            out[v] *= (v == sl.acf() || v == sl.acf() + 1) ? f : f * f;
+    }
     NdBook* book = F.book;
     if (F.kind == 2) {
         for (int s = 0; s < J.S; ++s) book->carry[s] = out[sl.absn() + s];
@@ -902,6 +925,7 @@ __global__ void __launch_bounds__(512)
     const size_t outer = (size_t)blockIdx.x >> ltpo, inner0 = ((size_t)blockIdx.x & ((1u << ltpo) - 1)) << logt;
     const size_t c0 = ((outer << logn) << lstride) + inner0;
     cx<T>* data = ((mode & TM_PHI) ? J.phi : J.psi) + (size_t)blockIdx.y * J.N;
+    const double nf = (mode & TM_SCALE) ? nd_norm_factor(*J.nsum, J.dr) : 1.0;
     // element t of line g sits at data[c0 + (t << lstride) + g]; consecutive threads take consecutive lines
     cx<T> v[ND_IPT][8];
 #pragma unroll
@@ -912,6 +936,9 @@ __global__ void __launch_bounds__(512)
             nd_item<true>(it, logt, logm, g, i);
 #pragma unroll
             for (int r = 0; r < 8; ++r) v[k][r] = data[c0 + ((size_t)(i + (r << logm)) << lstride) + g];
+            if (mode & TM_SCALE)
+#pragma unroll
+                for (int r = 0; r < 8; ++r) v[k][r] = nd_scaled<T>(v[k][r], nf);
         }
     }
     __syncthreads(); // twiddles staged
@@ -1167,6 +1194,7 @@ __global__ void __launch_bounds__(512)
     nd_stage_mid_tw<T>(J.tw, twm + n, logn);
     __syncthreads();
     const bool kobs = P.mode & TM_KOBS;
+    const double nf = (P.mode & TM_SCALE) ? nd_norm_factor(*J.nsum, J.dr) : 1.0;
     double acc[D + 1]; // TM_KOBS: <k_j> sums and the kinetic energy's, over the CTA's tiles
 #pragma unroll
     for (int a = 0; a <= D; ++a) acc[a] = 0.0;
@@ -1198,6 +1226,9 @@ __global__ void __launch_bounds__(512)
         cx<T> v[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) v[r] = buf[ix.at(g, i + (r << logm))];
+        if (P.mode & TM_SCALE)
+#pragma unroll
+            for (int r = 0; r < 8; ++r) v[r] = nd_scaled<T>(v[r], nf);
         if (P.mode & TM_FWD) ndt_fft<T, -1>(v, buf, ix, logn, twm);
         if (P.mode & TM_KPHASE) {
             // exp(Complex(0, -K) * dt), K = sum_j k_j^2 / (2 m_j) (quantum_dynamics.zig:397-399), as the
