@@ -244,8 +244,6 @@ static int choose_line_shape(zqd_job* J) {
             if (J->n % C) continue;
             const int m = J->n / C;
             if (m < 8 || m / C < 1) continue;
-            const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m, rg) : line_smem_bytes<double>(J->S, C, m, rg);
-            if (smem > budget) continue;
             // radix 4 doubles the threads of a CTA (more warps to hide latency) where the limit allows
             int lrmax = 2;
             const int tmax = J->fp32 ? LineMaxThreads<float>::value : LineMaxThreads<double>::value;
@@ -254,6 +252,9 @@ static int choose_line_shape(zqd_job* J) {
             else if (forced_lr == 2 && lrmax != 2) continue;
             if (lrmax == 3 && C != 16) continue; // radix 8 is built for 16-CTA clusters only
             if (std::max(32, ((m >> lrmax) + 31) / 32 * 32) > tmax) continue;
+            const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m, rg, lrmax)
+                                        : line_smem_bytes<double>(J->S, C, m, rg, lrmax);
+            if (smem > budget) continue;
             // one thread per butterfly of every state (passes without state-mixing hooks split
             // the states over the threads), within the kernel's thread limit
             const int threads = std::min(tmax, std::max(32, ((m >> lrmax) * J->S + 31) / 32 * 32));

@@ -23,9 +23,18 @@ namespace zqd {
 // dynamic shared memory of one CTA
 // r_global: the R table is read from global memory (L2) instead of being staged, for the
 // largest lines whose R slice does not fit next to the wavefunction buffers
-template <typename T> __host__ __device__ inline size_t line_smem_bytes(int S, int C, int m, bool r_global = false) {
+// lrm: log2 of the largest local radix; the inverse transform's pass schedule needs a twiddle table
+// of its own when m is not a power of 2^lrm
+__host__ __device__ inline bool line_two_schedules(int m, int lrm) {
+    int logm = 0;
+    while ((1 << logm) < m) ++logm;
+    return logm % lrm != 0;
+}
+template <typename T>
+__host__ __device__ inline size_t line_smem_bytes(int S, int C, int m, bool r_global, int lrm) {
     const size_t ld = (size_t)padded_len<T>(m), nsym = r_global ? 0 : (size_t)S * (S + 1) / 2;
-    return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 2 : 1) + nsym + 1) * (size_t)m * sizeof(Tab<T>);
+    const size_t ntw = line_two_schedules(m, lrm) ? 2 : 1;
+    return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 1 : 0) + ntw + nsym + 1) * (size_t)m * sizeof(Tab<T>);
 }
 
 // reduction slots of a step
@@ -420,7 +429,21 @@ __device__ __noinline__ void line_initial_state(const LineCtx<T>& X, double lo, 
 template <typename T> struct LineMaxThreads { static constexpr int value = 512; };
 template <> struct LineMaxThreads<double> { static constexpr int value = 256; };
 
-enum PassKind : int { FWD_FIRST = 1, FWD_LAST = 2, INV_FIRST = 4, INV_LAST = 8 };
+// FUSE_NEXT (with INV_LAST): the pass also runs the next step's forward first pass on the same
+// points (the last inverse pass leaves point i + r m/R with the thread of butterfly i, which is
+// where the forward first pass takes it from)
+enum PassKind : int { FWD_FIRST = 1, FWD_LAST = 2, INV_FIRST = 4, INV_LAST = 8, FUSE_NEXT = 16 };
+
+// log2 of the radix of local pass `idx` of an m = 2^logm point transform: 2^lrm (8, or 4 with twice
+// the threads and only the radix-4/2 code compiled, which keeps the kernel's instruction footprint
+// small), except for one smaller remainder pass: the forward transform's first, the inverse's last.
+// The inverse's last pass and the forward's first pass then have the same radix and the same
+// points per butterfly, and the passes with state-mixing hooks (R) have the most butterflies.
+__host__ __device__ __forceinline__ int local_passes(int logm, int lrm) { return (logm + lrm - 1) / lrm; }
+__host__ __device__ __forceinline__ int local_pass_lr(int logm, int lrm, int idx, bool inverse) {
+    const int np = local_passes(logm, lrm);
+    return idx == (inverse ? np - 1 : 0) ? logm - (np - 1) * lrm : lrm;
+}
 
 // All state of one CTA's solve.  Every member function is force-inlined into
 // the kernel, so the members stay in registers (no closure objects, no stack).
@@ -433,7 +456,8 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     cx<T>* bufA;
     cx<T>* bufB;
     cx<T>* cur; // holds psi between steps
-    const Tab<T>* twm; // local-pass twiddles, pass by pass (see the staging in the kernel)
+    const Tab<T>* twm; // local-pass twiddles of the forward schedule, pass by pass (see the staging in the kernel)
+    const Tab<T>* twi; // ... of the inverse schedule (twm when the two schedules are the same)
     const Tab<T>* twp; // the current pass's table: W at [(r - 1) p + kk]
     const Tab<T>* twc;
     const Tab<T>* Rs;
@@ -603,64 +627,96 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             const int o0 = ((i - kk) << LR) + kk;
             if constexpr (KIND & FWD_LAST) fwd_last<R>(o0, p, v);
             if constexpr (KIND & INV_LAST) inv_last<R>(o0, p, v);
+            if constexpr (KIND & FUSE_NEXT) { // last pass: o0 = i, p = mr; the next step's first pass (p = 1)
+                fwd_first<R>(i, mr, v);
 #pragma unroll
-            for (int s = 0; s < S; ++s)
+                for (int s = 0; s < S; ++s) dft<R, -1, T>(v[s]);
 #pragma unroll
-                for (int r = 0; r < R; ++r) out[s * ldp + padx<T>(o0 + r * p)] = v[s][r];
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) out[s * ldp + padx<T>((i << LR) + r)] = v[s][r];
+            } else {
+#pragma unroll
+                for (int s = 0; s < S; ++s)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) out[s * ldp + padx<T>(o0 + r * p)] = v[s][r];
+            }
         }
         __syncthreads();
     }
 
-    // local m-point transform ping-ponging between a (input) and b; returns the result buffer
-    template <int SIGN> __device__ __forceinline__ cx<T>* local_fft(cx<T>* a, cx<T>* b, const cx<T>* xbuf) {
+    // one local pass of radix R, its kind from its place in the schedule.  The remainder radix
+    // (below 2^LRM) is only ever the forward's first or the inverse's last pass.
+    template <int R, int SIGN>
+    __device__ __forceinline__ void pass_at(bool first, bool last, bool fuse_next, cx<T>* in, cx<T>* out, int p,
+                                            const cx<T>* xbuf) {
         constexpr int KF = SIGN < 0 ? FWD_FIRST : INV_FIRST, KL = SIGN < 0 ? FWD_LAST : INV_LAST;
-        int p = 1, rem = logm, tbase = 0;
-        bool first = true;
+        constexpr bool REM = R < (1 << LRM);
+        if (first && last) {
+            pass<R, SIGN, KF | KL>(in, out, p, xbuf);
+        } else if constexpr (REM && SIGN < 0) {
+            pass<R, SIGN, KF>(in, out, p, xbuf);
+        } else if constexpr (REM && SIGN > 0) {
+            if (fuse_next) pass<R, SIGN, KL | FUSE_NEXT>(in, out, p, xbuf);
+            else pass<R, SIGN, KL>(in, out, p, xbuf);
+        } else {
+            if (first) pass<R, SIGN, KF>(in, out, p, xbuf);
+            else if (!last) pass<R, SIGN, 0>(in, out, p, xbuf);
+            else if constexpr (SIGN > 0) {
+                if (fuse_next) pass<R, SIGN, KL | FUSE_NEXT>(in, out, p, xbuf);
+                else pass<R, SIGN, KL>(in, out, p, xbuf);
+            } else {
+                pass<R, SIGN, KL>(in, out, p, xbuf);
+            }
+        }
+    }
+
+    // local m-point transform ping-ponging between a (input) and b; returns the result buffer.
+    // start: passes already run (1: the first pass ran as part of the previous step's last pass);
+    // fuse_next (inverse only): the last pass also runs the next step's forward first pass
+    template <int SIGN>
+    __device__ __forceinline__ cx<T>* local_fft(cx<T>* a, cx<T>* b, const cx<T>* xbuf, int start = 0,
+                                                bool fuse_next = false) {
+        const int np = local_passes(logm, LRM);
+        const Tab<T>* tw = SIGN < 0 ? twm : twi;
+        int p = 1, tbase = 0;
         cx<T>* in = a;
         cx<T>* out = b;
-        while (rem > 0) {
-            // largest radix 2^LRM (8, or 4 with twice the threads and only the radix-4/2 code compiled,
-            // which keeps the kernel's instruction footprint small), smaller at the end
-            const int LR = rem >= LRM ? LRM : rem;
-            const bool last = rem == LR;
-            twp = twm + tbase;
-            if (LRM == 3 && LR == 3) {
-                if constexpr (LRM == 3) {
-                    if (first && last) pass<8, SIGN, KF | KL>(in, out, p, xbuf);
-                    else if (first) pass<8, SIGN, KF>(in, out, p, xbuf);
-                    else if (last) pass<8, SIGN, KL>(in, out, p, xbuf);
-                    else pass<8, SIGN, 0>(in, out, p, xbuf);
+        for (int idx = 0; idx < np; ++idx) {
+            const int LR = local_pass_lr(logm, LRM, idx, SIGN > 0);
+            if (idx >= start) {
+                const bool first = idx == 0, last = idx == np - 1;
+                twp = tw + tbase;
+                if (LR == 3) {
+                    if constexpr (LRM == 3) pass_at<8, SIGN>(first, last, fuse_next, in, out, p, xbuf);
+                } else if (LR == 2) {
+                    pass_at<4, SIGN>(first, last, fuse_next, in, out, p, xbuf);
+                } else {
+                    pass_at<2, SIGN>(first, last, fuse_next, in, out, p, xbuf);
                 }
-            } else if (LR == 2) {
-                if (first && last) pass<4, SIGN, KF | KL>(in, out, p, xbuf);
-                else if (first) pass<4, SIGN, KF>(in, out, p, xbuf);
-                else if (last) pass<4, SIGN, KL>(in, out, p, xbuf);
-                else pass<4, SIGN, 0>(in, out, p, xbuf);
-            } else {
-                if (first) pass<2, SIGN, KF | KL>(in, out, p, xbuf);
-                else pass<2, SIGN, KL>(in, out, p, xbuf);
+                // the inverse's first pass read other CTAs' exchange buffers: none may be
+                // overwritten before every CTA of the cluster has finished that gather.  The
+                // gathered values were consumed (butterflies, stored locally) before the arrive,
+                // so the barrier publishes nothing and its arrive can be relaxed (no fence)
+                if (C > 1 && SIGN > 0 && first) cluster_barrier_relaxed();
+                cx<T>* t = in;
+                in = out;
+                out = t;
             }
-            // the inverse's first pass read other CTAs' exchange buffers: none may be
-            // overwritten before every CTA of the cluster has finished that gather.  The
-            // gathered values were consumed (butterflies, stored locally) before the arrive,
-            // so the barrier publishes nothing and its arrive can be relaxed (no fence)
-            if (C > 1 && SIGN > 0 && first) cluster_barrier_relaxed();
-            cx<T>* t = in;
-            in = out;
-            out = t;
             tbase += ((1 << LR) - 1) * p;
             p <<= LR;
-            rem -= LR;
-            first = false;
         }
         return in;
     }
+    // the last inverse pass can take the next step's forward first pass: at least two passes
+    __device__ __forceinline__ bool can_fuse_steps() const { return local_passes(logm, LRM) >= 2; }
 
     __device__ __forceinline__ cx<T>* other(const cx<T>* b) const { return b == bufA ? bufB : bufA; }
 
-    // forward transform of cur; returns the buffer the inverse starts from
-    __device__ __forceinline__ cx<T>* forward() {
-        cx<T>* res = local_fft<-1>(cur, other(cur), nullptr);
+    // forward transform of cur (start = 1: its first pass already ran); returns the buffer the
+    // inverse starts from
+    __device__ __forceinline__ cx<T>* forward(int start = 0) {
+        cx<T>* res = local_fft<-1>(cur, other(cur), nullptr, start);
         if constexpr (C > 1) { // C-point DFTs across the cluster, kinetic phase in between
             cx<T>* xb = other(res);
             cg::cluster_group cl = cg::this_cluster();
@@ -686,10 +742,11 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
         }
         return res;
     }
-    // inverse transform (from forward's buffer) into cur
-    __device__ __forceinline__ void inverse(cx<T>* kb) {
-        if constexpr (C > 1) cur = local_fft<1>(kb, other(kb), kb); // first pass gathers remote kb, writes the other buffer
-        else cur = local_fft<1>(kb, other(kb), nullptr);
+    // inverse transform (from forward's buffer) into cur; fuse_next: cur then holds the next step's
+    // forward first pass instead of psi
+    __device__ __forceinline__ void inverse(cx<T>* kb, bool fuse_next = false) {
+        if constexpr (C > 1) cur = local_fft<1>(kb, other(kb), kb, 0, fuse_next); // first pass gathers remote kb
+        else cur = local_fft<1>(kb, other(kb), nullptr, 0, fuse_next);
     }
 
     __device__ __forceinline__ void zero_acc() {
@@ -786,10 +843,13 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
     X.bufA = reinterpret_cast<cx<T>*>(smem_raw);
     X.bufB = X.bufA + S * X.ldp;
     Tab<T>* twm = reinterpret_cast<Tab<T>*>(X.bufB + S * X.ldp);
-    Tab<T>* twc = twm + X.m;
+    const bool two = line_two_schedules(X.m, LRM);
+    Tab<T>* twi = two ? twm + X.m : twm;
+    Tab<T>* twc = twi + X.m;
     Tab<T>* Rs = J.r_global ? J.R + X.base : twc + (C > 1 ? X.m : 0);
     Tab<T>* eks = twc + (C > 1 ? X.m : 0) + (J.r_global ? 0 : NSYM * X.m);
     X.twm = twm;
+    X.twi = twi;
     X.twc = twc;
     X.Rs = Rs;
     X.rstride = J.r_global ? J.n : J.m;
@@ -815,18 +875,18 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
     // [(r - 1) p + kk], r = 1..R-1, kk < p.  A warp's twiddle reads are then contiguous
     // (reading W_m^t at stride m/(p R) put up to 16 of them in the same banks); the tables
     // take sum (R - 1) p = m - 1 entries.
-    {
-        int p = 1, logp = 0, rem = X.logm, tbase = 0;
-        while (rem > 0) {
-            const int LR = rem >= LRM ? LRM : rem, R = 1 << LR, tshift = X.logm - logp - LR;
+    for (int dir = 0; dir < (two ? 2 : 1); ++dir) {
+        Tab<T>* tw = dir ? twi : twm;
+        int p = 1, logp = 0, tbase = 0;
+        for (int idx = 0; idx < local_passes(X.logm, LRM); ++idx) {
+            const int LR = local_pass_lr(X.logm, LRM, idx, dir == 1), R = 1 << LR, tshift = X.logm - logp - LR;
             for (int e = threadIdx.x; e < (R - 1) * p; e += blockDim.x) {
                 const int r = e / p + 1, kk = e - (r - 1) * p;
-                twm[tbase + e] = J.tw[((r * kk) << tshift) * C];
+                tw[tbase + e] = J.tw[((r * kk) << tshift) * C];
             }
             tbase += (R - 1) * p;
             p <<= LR;
             logp += LR;
-            rem -= LR;
         }
     }
     if (!J.r_global)
@@ -853,6 +913,13 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
     const int iters = J.iters;
     int rows = J.i1 + 1;
     bool ended = J.i1 >= iters;
+    // Step i's last inverse pass also runs step i+1's forward first pass (the applyR that ends step
+    // i and the one that begins step i+1 act on the same grid points, quantum_dynamics.zig:417-427)
+    // wherever nothing needs the end-of-step wavefunction in between: no momentum round trip, no
+    // wavefunction history, no stop test, no absorbed-population tracking (its sums belong to the
+    // next row), no imaginary time or time-dependent update, and not the launch's last step.
+    const bool fusable = X.can_fuse_steps() && !J.itp && !J.td && !J.wfn_hist && !J.has_stop && !J.track;
+    bool pre = false; // cur holds step i's forward first pass (run by step i-1's last pass)
     for (int i = J.i0; i <= J.i1; ++i) {
         const bool logstep = J.log && ((i % J.log_interval == 0) || (i == iters));
         X.set_flags(J.wmask | (logstep ? (uint32_t)WM_ALL_OBS : 0u));
@@ -864,7 +931,9 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
                 line_ham_update<T, S, C>(ctx, ((double)i - 0.5) * J.tstep, true, Rs, X.rstride, X.lo, X.span);
             }
             X.prop = true;
-            X.inverse(X.forward());
+            const bool fuse = fusable && i < J.i1 && !(X.f.mom || X.f.ekin);
+            X.inverse(X.forward(pre ? 1 : 0), fuse);
+            pre = fuse;
             ctx.psi = X.cur;
         }
         if (J.itp) { // quantum_dynamics.zig:898-906
