@@ -255,6 +255,10 @@ static int choose_line_shape(zqd_job* J) {
             const size_t smem = J->fp32 ? line_smem_bytes<float>(J->S, C, m, rg, lrmax)
                                         : line_smem_bytes<double>(J->S, C, m, rg, lrmax);
             if (smem > budget) continue;
+            // the eigenvectors staged beside the tables where they fit (several states)
+            const size_t smem_u = J->fp32 ? line_smem_bytes<float>(J->S, C, m, rg, lrmax, true)
+                                          : line_smem_bytes<double>(J->S, C, m, rg, lrmax, true);
+            const bool u_smem = J->S > 1 && smem_u <= budget;
             // one thread per butterfly of every state (passes without state-mixing hooks split
             // the states over the threads), within the kernel's thread limit
             const int threads = std::min(tmax, std::max(32, ((m >> lrmax) * J->S + 31) / 32 * 32));
@@ -264,9 +268,10 @@ static int choose_line_shape(zqd_job* J) {
             J->q = m / C;
             J->E = 8 * J->S;
             J->threads = threads;
-            J->smem = smem;
+            J->smem = u_smem ? smem_u : smem;
             J->r_global = rg;
             J->lrmax = lrmax;
+            J->u_smem = u_smem;
             return ZQD_OK;
         }
     }
@@ -445,6 +450,7 @@ template <typename T> static LineJob<T> line_job_desc(const zqd_job* J, int s) {
     L.psi_init = J->psi_init.as<cx<T>>();
     L.r_global = J->r_global ? 1 : 0;
     L.lrmax = J->lrmax;
+    L.u_smem = J->u_smem ? 1 : 0;
     L.sign_track = needs_sign_tracking(o, J->S, J->nsolve) ? 1 : 0;
     L.sgn = J->sgn.as<double>();
     L.wfn_hist = J->wfn_hist.p ? J->wfn_hist.as<cx<T>>() + (size_t)s * ((size_t)o.iterations + 1) * J->S * J->n : nullptr;
@@ -966,7 +972,7 @@ extern "C" int zqd_batch_create(const zqd_options* const* opts, uint32_t njobs, 
         for (uint32_t k = i + 1; k < njobs; ++k) {
             zqd_job* b = B->jobs[k].get();
             if (!done[k] && b->d == 1 && b->nsolve == 1 && b->fp32 == a->fp32 && b->S == a->S && b->C == a->C &&
-                b->r_global == a->r_global && b->lrmax == a->lrmax) {
+                b->r_global == a->r_global && b->lrmax == a->lrmax && b->u_smem == a->u_smem) {
                 g->members.push_back(b);
                 done[k] = true;
             }
@@ -1021,7 +1027,7 @@ int zqd::run_line_group(const std::vector<zqd_job*>& jobs, cudaStream_t st, floa
     const zqd_job* a = jobs[0];
     for (const zqd_job* J : jobs)
         if (J->d != 1 || J->nsolve != 1 || J->fp32 != a->fp32 || J->S != a->S || J->C != a->C || J->r_global != a->r_global ||
-            J->lrmax != a->lrmax)
+            J->lrmax != a->lrmax || J->u_smem != a->u_smem)
             return fail(ZQD_ERR_INVALID_INPUT, "JOBS OF ONE GROUP MUST SHARE PRECISION, STATES AND CLUSTER SHAPE");
     LaunchShape sh{a->S, a->C, a->E, 0, 0, st};
     sh.lrmax = a->lrmax;
@@ -1075,7 +1081,7 @@ int zqd::step_line_group(const std::vector<zqd_job*>& jobs, uint32_t nsteps, cud
     const zqd_job* a = jobs[0];
     for (const zqd_job* J : jobs)
         if (J->d != 1 || J->nsolve != 1 || J->fp32 != a->fp32 || J->S != a->S || J->C != a->C || J->r_global != a->r_global ||
-            J->lrmax != a->lrmax)
+            J->lrmax != a->lrmax || J->u_smem != a->u_smem)
             return fail(ZQD_ERR_INVALID_INPUT, "JOBS OF ONE GROUP MUST SHARE PRECISION, STATES AND CLUSTER SHAPE");
     LaunchShape sh{a->S, a->C, a->E, 0, 0, st};
     sh.lrmax = a->lrmax;

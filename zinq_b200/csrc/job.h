@@ -88,6 +88,7 @@ struct zqd_job {
     bool fp32 = false;
     bool r_global = false; // 1-D: R read from global memory (the largest lines)
     int lrmax = 3;         // 1-D: log2 of the largest local radix
+    bool u_smem = false;   // 1-D: the shape stages the eigenvectors in shared memory
     int nsolve = 1, hc = 0;
     zqd::PotStore pot;
     cudaStream_t stream = nullptr;

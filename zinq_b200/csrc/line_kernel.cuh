@@ -76,6 +76,7 @@ template <typename T> struct LineJob {
     const cx<T>* psi_init; // [S][n] permuted initial wavefunction replacing the Gaussian, or null
     int r_global;          // R read from global memory instead of shared memory
     int lrmax;             // log2 of the largest local radix (threads per CTA = m >> lrmax)
+    int u_smem;            // the shape reserved shared memory for the eigenvectors of the CTA's points
     cx<T>* wfn_hist;       // [step][S][n] permuted wavefunction history of this solve, or null
     // time-dependent potentials whose eigenvector signs are observed (the adiabatic wavefunction
     // history, or the toDia of a later imaginary-time solve): after every update the 1-D

@@ -30,11 +30,13 @@ __host__ __device__ inline bool line_two_schedules(int m, int lrm) {
     while ((1 << logm) < m) ++logm;
     return logm % lrm != 0;
 }
+// u_smem: room for the S x S eigenvectors of the CTA's points (FP64) after the tables
 template <typename T>
-__host__ __device__ inline size_t line_smem_bytes(int S, int C, int m, bool r_global, int lrm) {
+__host__ __device__ inline size_t line_smem_bytes(int S, int C, int m, bool r_global, int lrm, bool u_smem = false) {
     const size_t ld = (size_t)padded_len<T>(m), nsym = r_global ? 0 : (size_t)S * (S + 1) / 2;
     const size_t ntw = line_two_schedules(m, lrm) ? 2 : 1;
-    return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 1 : 0) + ntw + nsym + 1) * (size_t)m * sizeof(Tab<T>);
+    return 2 * (size_t)S * ld * sizeof(cx<T>) + ((C > 1 ? 1 : 0) + ntw + nsym + 1) * (size_t)m * sizeof(Tab<T>) +
+           (u_smem ? (size_t)S * S * m * sizeof(double) : 0);
 }
 
 // reduction slots of a step
@@ -108,9 +110,10 @@ __device__ __forceinline__ void absorbed_point(Acc* acc, const cx<T>* x, double 
 }
 
 // position-space observables of one point (wavepacket.zig:235-352, Observables.init :321-345)
+// U: the eigenvectors of the CTA's points, component e of point j at U[e * us + j]
 template <typename T, int S>
 __device__ __forceinline__ void observe_point(Acc* acc, const cx<T>* x, double r, const LineJob<T>& J, size_t gidx,
-                                              const ObsFlags& f) {
+                                              const ObsFlags& f, const double* __restrict__ U, int us, int j) {
     double m2 = 0;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -147,7 +150,7 @@ __device__ __forceinline__ void observe_point(Acc* acc, const cx<T>* x, double r
             double are = 0, aim = 0;
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-                const double u = J.U[(size_t)(k * S + i) * J.n + gidx];
+                const double u = U[(size_t)(k * S + i) * us + j];
                 are += (double)x[k].x * u;
                 aim += (double)x[k].y * u;
             }
@@ -464,7 +467,8 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
     int rstride; // component stride of Rs: m when staged in shared memory, n when read from global
     const Tab<T>* eks;
     const double* capw; // this CTA's slice of the global tables
-    const double* Ug;
+    const double* Ug; // the eigenvectors of the CTA's points: component e of point j at Ug[e * ustride + j]
+    int ustride;
     const double* Vg;
     const cx<T>* psi0;
     int m, n, logm, q, ldp, cta;
@@ -487,7 +491,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             cx<T> x[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) x[s] = v[s][r];
-            if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
+            if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, ustride, j, f.adia);
             apply_r_point<T, S>(x, Rs, rstride, j);
 #pragma unroll
             for (int s = 0; s < S; ++s) v[s][r] = x[s];
@@ -540,9 +544,9 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
 #pragma unroll
             for (int s = 0; s < S; ++s) x[s] = scale<T>(v[s][r], inv_n);
             if (prop) {
-                if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, n, j, f.adia);
+                if (f.track) absorbed_point<T, S>(acc, x, capw[j], Ug, ustride, j, f.adia);
                 apply_r_point<T, S>(x, Rs, rstride, j);
-                if (fuse_obs) observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f);
+                if (fuse_obs) observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f, Ug, ustride, j);
             }
 #pragma unroll
             for (int s = 0; s < S; ++s) v[s][r] = x[s];
@@ -759,7 +763,7 @@ template <typename T, int S, int C, int LRM> struct LineSolver {
             cx<T> x[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) x[s] = cur[s * ldp + padx<T>(j)];
-            observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f);
+            observe_point<T, S>(acc, x, grid_r<C>(lo, span, n, cta, j), *J, base + j, f, Ug, ustride, j);
         }
     }
     // momentum-space round trip (quantum_dynamics.zig:347-363): psi <- IFFT(FFT(psi)) as in the reference
@@ -856,6 +860,7 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
     X.eks = eks;
     X.capw = J.capw ? J.capw + X.base : nullptr;
     X.Ug = J.U ? J.U + X.base : nullptr;
+    X.ustride = J.n;
     X.Vg = J.V + X.base;
     X.psi0 = J.psi0 ? J.psi0 + X.base : nullptr;
     X.cur = X.bufA;
@@ -894,6 +899,17 @@ __device__ __forceinline__ void line_solve_run(LineJob<T>& J, RedSmem& rs, unsig
             const int c = e / m, j = e - c * m;
             Rs[e] = J.R[(size_t)c * n + X.base + j];
         }
+    // the eigenvectors (adiabatic populations, absorbed populations) after the tables, where the
+    // shape reserved room for them and they do not change during the solve
+    if (J.u_smem && J.U && !J.td) {
+        double* Us = reinterpret_cast<double*>(eks + m);
+        for (int e = threadIdx.x; e < S * S * m; e += blockDim.x) {
+            const int c = e / m, j = e - c * m;
+            Us[e] = J.U[(size_t)c * n + X.base + j];
+        }
+        X.Ug = Us;
+        X.ustride = m;
+    }
     __syncthreads();
 
     LineCtx<T> ctx{&J, X.cur, nullptr, &rs, m, n, X.logm, X.q, X.ldp, cta, X.base};
