@@ -1189,6 +1189,8 @@ __global__ void __launch_bounds__(512)
 #pragma unroll
         for (int s = 0; s < NDT_STAGES; ++s) mbar_init(&bars[s], 1);
         fence_barrier_init();
+        // the first load overlaps the twiddle staging (the stages and the twiddles do not overlap)
+        if (blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     }
     for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
     nd_stage_mid_tw<T>(J.tw, twm + n, logn);
@@ -1198,7 +1200,6 @@ __global__ void __launch_bounds__(512)
     double acc[D + 1]; // TM_KOBS: <k_j> sums and the kinetic energy's, over the CTA's tiles
 #pragma unroll
     for (int a = 0; a <= D; ++a) acc[a] = 0.0;
-    if (tid == 0 && blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     bool failed = false;
     int j = 0;
     for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
@@ -1372,6 +1373,8 @@ __global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? (POP && S 
 #pragma unroll
         for (int s = 0; s < NDT_STAGES; ++s) mbar_init(&bars[s], 1);
         fence_barrier_init();
+        // the first load overlaps the twiddle staging (the stages and the twiddles do not overlap)
+        if (blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     }
     for (int t = tid; t < n; t += blockDim.x) twm[t] = J.tw[t];
     nd_stage_mid_tw<T>(J.tw, twm + n, logn);
@@ -1394,7 +1397,6 @@ __global__ void __launch_bounds__(MAXT, MAXT == NDR_THREADS && !PHI ? (POP && S 
     const IxRow<T> ix{logn};
     int g, i;
     ix.item(tid, logm, g, i);
-    if (tid == 0 && blockIdx.x < P.nitems && !P.withhold) issue(blockIdx.x, 0);
     bool failed = false;
     int j = 0;
     for (unsigned k = blockIdx.x; k < P.nitems; k += gridDim.x, ++j) {
