@@ -335,7 +335,11 @@ def nd_legs(qd, torch, flush, reps=2):
     for name, opt in cases:
         leg = {"units_per_run": nd_units(opt)}
         pops = {}
+        d, n = len(opt["grid"]["bounds"]), opt["grid"]["npoint"]
+        S = len(opt["potential"]["custom"]["matrix"])
         for prec in ("fp32", "fp64"):
+            # the library's autotuner for the (dims, points, states, precision) key, outside the timing
+            tuned = qd.autotune(d, n, S, prec)
             job = qd.Job(opt, prec)
             job.run()  # captures the run's graph; warm-up
             ts = []
@@ -356,7 +360,10 @@ def nd_legs(qd, torch, flush, reps=2):
                                       "moved": {"bytes_per_step": bmoved, "achieved": moved, "frac": moved / peak,
                                                 "note": "the bytes the kernels read and write per step "
                                                         "(bench.nd_bytes_moved); DRAM traffic is lower where the "
-                                                        "working set stays in the 126 MB L2"}}}
+                                                        "working set stays in the 126 MB L2"}},
+                         "autotune": {k: tuned[k] for k in ("us_per_step", "default_us_per_step", "candidates",
+                                                            "tma_row_block", "tma_tile_lines", "rows_per_cta",
+                                                            "tile_lines")}}
             h = job.result(want_wavefunction=False).observables[0].history
             if "population" in h:
                 pops[prec] = h["population"]
@@ -437,10 +444,18 @@ def serving_leg(qd):
     opts, arrivals = qd.serving_stream(SERVE_JOBS, seed=7, rate_per_s=SERVE_RATE, max_steps=SERVE_MAX_STEPS)
     units = sum(o["grid"]["npoint"] ** len(o["grid"]["bounds"]) * len(o["potential"]["custom"]["matrix"]) * o["iterations"]
                 for o in opts)
+    # the autotuner over the stream's 2-D keys (the 1-D jobs take the single-CTA service kernel or the
+    # cluster shapes of their line length), outside the timing; served and plain runs share the table
+    keys2d = sorted({(o["grid"]["npoint"], len(o["potential"]["custom"]["matrix"])) for o in opts
+                     if len(o["grid"]["bounds"]) == 2})
+    for n, S in keys2d:
+        for prec in ("fp32", "fp64"):
+            qd.autotune(2, n, S, prec)
     w_opts, w_arr = qd.serving_stream(60, seed=8, rate_per_s=2000.0, max_steps=200)
     qd.serve_stream(w_opts, w_arr, "fp32")  # warm-up: module loading, memory pool
     qd.serve_stream(w_opts, w_arr, "fp64")
     out = {"jobs": SERVE_JOBS, "arrival_rate_per_s": SERVE_RATE, "steps": f"100..{SERVE_MAX_STEPS}",
+           "autotuned_2d_keys": len(keys2d) * 2,
            "workload": "seeded stream: 1-D 256..16384 pts or 2-D 64^2..512^2, 1-3 states, harmonic or tanh-crossing",
            "units": units}
     pops, forms = {}, {}
