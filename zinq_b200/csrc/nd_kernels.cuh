@@ -348,7 +348,23 @@ template <typename T> __device__ void nd_finalize_cta(const NdJob<T>& J, const N
     __shared__ double out[NDV];
     const NdSlots sl{J.d, J.S};
     const int nw = blockDim.x >> 5;
-    for (int v = threadIdx.x >> 5; v < sl.count(); v += nw) {
+    const uint32_t mask = F.mask;
+    const bool c_pos = mask & WM_POS, c_mom = mask & WM_MOM, c_pop = mask & WM_POP;
+    const bool c_ekin = (mask & WM_EKIN) || (mask & WM_ETOT), c_epot = (mask & WM_EPOT) || (mask & WM_ETOT);
+    const bool c_norm = (mask & WM_NORM) || F.has_stop, c_acf = mask & WM_ACF;
+    // only the slots this finalize uses are summed (the others are zero or unrecorded): the norm, the
+    // recorded observables and, with CAP tracking, the absorbed sums; the rest read as 0
+    int list[NDV], nl = 0;
+    for (int v = 0; v < sl.count(); ++v) {
+        const bool need = v == sl.norm() || (c_pos && v >= sl.pos() && v < sl.pos() + J.d) ||
+                          (c_epot && v == sl.epot()) || (c_acf && (v == sl.acf() || v == sl.acf() + 1)) ||
+                          (c_mom && v >= sl.mom() && v < sl.mom() + J.d) || (c_ekin && v == sl.ekin()) ||
+                          (c_pop && v >= sl.pop() && v < sl.pop() + J.S) || (J.track && v >= sl.abs());
+        if (need) list[nl++] = v;
+        else if (threadIdx.x == 0) out[v] = 0.0;
+    }
+    for (int k = threadIdx.x >> 5; k < nl; k += nw) {
+        const int v = list[k];
         const bool kslot = v >= sl.mom() && v <= sl.ekin();
         const double x = kslot ? (F.k1 > F.k0 ? warp_sum_partials(J.part, J.nparts, F.k0, F.k1, v) : 0.0)
                                : warp_sum_partials(J.part, J.nparts, F.x0, F.x1, v);
@@ -367,12 +383,8 @@ template <typename T> __device__ void nd_finalize_cta(const NdJob<T>& J, const N
         for (int s = 0; s < J.S; ++s) book->carry[s] = out[sl.absn() + s];
         return;
     }
-    const uint32_t mask = F.mask;
     double* row = F.row;
     const RowLayout L{J.d, J.S};
-    const bool c_pos = mask & WM_POS, c_mom = mask & WM_MOM, c_pop = mask & WM_POP;
-    const bool c_ekin = (mask & WM_EKIN) || (mask & WM_ETOT), c_epot = (mask & WM_EPOT) || (mask & WM_ETOT);
-    const bool c_norm = (mask & WM_NORM) || F.has_stop, c_acf = mask & WM_ACF;
     if (F.kind == 0)
         for (int s = 0; s < J.S; ++s) { // accumAbsorbed adds sum * dr twice per step (quantum_dynamics.zig:497)
             book->pop_abs[s] += book->carry[s] * J.dr;
