@@ -37,7 +37,7 @@ struct GapArgs {
     double lo[3], span[3];
     unsigned long long* out;
 };
-template <int S> __global__ void min_gap_kernel(GapArgs a) {
+template <int S> __global__ void min_gap_kernel(const __grid_constant__ GapArgs a) {
     double best = INFINITY;
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < a.N; g += (size_t)gridDim.x * blockDim.x) {
         double r[3];
@@ -105,7 +105,7 @@ static int resolve_auto_precision(zqd_job* J) {
 
 // Hamiltonian.init/update at t = 0 (wavepacket.zig:96-143) and Propagator.init/update
 // (quantum_dynamics.zig:387-468) for every grid point, written in the cluster-permuted layout.
-template <typename T, int S> __global__ void line_tables_kernel(LineTablesArgs<T> a) {
+template <typename T, int S> __global__ void line_tables_kernel(const __grid_constant__ LineTablesArgs<T> a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     const int c = p / a.m, j = p - c * a.m;

@@ -1560,7 +1560,7 @@ __device__ __forceinline__ void nd_table_point(const NdJob<T>& J, size_t g, doub
         }
 }
 
-template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double t, int with_R) {
+template <typename T, int S> __global__ void nd_table_kernel(const __grid_constant__ NdJob<T> J, double t, int with_R) {
     if (*J.stopped) return;
     const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (g >= J.N) return;
@@ -1572,7 +1572,8 @@ template <typename T, int S> __global__ void nd_table_kernel(NdJob<T> J, double 
 // eigenvector j the partial sums of sum_k U_new[k][j] U_prev[k][j] over the grid (the global
 // alignment with the previous update, wavepacket.zig:157-167), grid-stride over <= 1024 blocks of
 // at most 16 warps.  nd_sign_flip_kernel applies the decision after the sums are reduced.
-template <typename T, int S> __global__ void nd_table_sign_kernel(NdJob<T> J, double t, int with_R, size_t part_base) {
+template <typename T, int S>
+__global__ void nd_table_sign_kernel(const __grid_constant__ NdJob<T> J, double t, int with_R, size_t part_base) {
     if (*J.stopped) return;
     double acc[S];
 #pragma unroll

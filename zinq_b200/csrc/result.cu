@@ -283,7 +283,8 @@ template <int S> __global__ void eigh_batch_kernel(const double* V, double* W, d
 // potential_plot.run (src/potential_plot.zig:48-106): V(r, t) at every point of Grid.init's grid
 // (wavepacket.zig:55-74), or with `adiabatic` the eigenvalues on the diagonal and zeros elsewhere
 template <int S>
-static __global__ void potential_plot_kernel(PotDev pot, int d, int n, size_t N, double3 lo, double3 span, double t,
+static __global__ void potential_plot_kernel(const __grid_constant__ PotDev pot, int d, int n, size_t N, double3 lo,
+                                             double3 span, double t,
                                              int adiabatic, double* __restrict__ U, double* __restrict__ R) {
     const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (g >= N) return;
