@@ -1631,7 +1631,8 @@ template <typename T> __global__ void nd_gauss_kernel(const __grid_constant__ Nd
 
 // psi /= sqrt(norm) (Complex.div by (s, 0), wavepacket.zig:282-284); optionally toDia and the acf reference
 template <typename T, int S>
-__global__ void nd_normalize_kernel(NdJob<T> J, const double* __restrict__ sum, int to_dia, int save_psi0) {
+__global__ void nd_normalize_kernel(const __grid_constant__ NdJob<T> J, const double* __restrict__ sum, int to_dia,
+                                    int save_psi0) {
     if (*J.stopped) return;
     const double sq = sqrt(sum[0] * J.dr), den = sq * sq;
     for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < J.N; g += (size_t)gridDim.x * blockDim.x) {
@@ -1685,7 +1686,8 @@ template <typename T> __global__ void nd_dot_kernel(const __grid_constant__ NdJo
 }
 
 // psi -= <phi_o|psi> dr phi_o (quantum_dynamics.zig:898-904)
-template <typename T> __global__ void nd_orth_apply_kernel(NdJob<T> J, int o, const double* __restrict__ sum) {
+template <typename T>
+__global__ void nd_orth_apply_kernel(const __grid_constant__ NdJob<T> J, int o, const double* __restrict__ sum) {
     if (*J.stopped) return;
     const double ore = sum[0] * J.dr, oim = sum[1] * J.dr;
     const cx<T>* ph = J.orth + (size_t)o * J.S * J.N;
